@@ -1,0 +1,329 @@
+#!/usr/bin/env python
+"""Benchmark of the matrix-free Q2 A11 apply (MatMult_MFStokes_A11 hot path).
+
+Default workload: the FP64 A11 MatMult on the 96^3-element deformed mesh
+(Q2, 7,189,057 nodes = 21,567,171 velocity dofs; interior lattice nodes
+perturbed by U[-0.2h,0.2h]; per-element log-normal viscosity, sigma 2
+decades, correlation length 0.1, seeded synthetic fields; free-slip walls).
+A step is one apply of A11 to one velocity vector (every element, Dirichlet
+columns/rows handled in the kernel).  Inputs (709 MB of algorithmic FP64
+traffic per apply) exceed the 126 MB L2, so no L2 flush is needed between
+steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank applies its own replica of the mesh (independent
+operators, no collective on the data path) and `value` is the total dof
+throughput of all ranks, timed as the max over ranks.  `--impl reference`
+times the reference's own CPU implementation of the same apply
+(MFStokesWrapper_A11_AVX compiled from the pTatin3d sources into
+oracle/_ref, all host threads) on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "A11 MF apply GDoF/s (FP64, 96^3 Q2 deformed mesh)"
+UNIT = "GDoF/s"
+
+
+def workload(m=96, seed=4):
+    from ptatin3d_b200 import mesh as M
+    c = M.perturb_interior(M.uniform_coords(m, m, m), m, m, m, frac=0.2, seed=seed)
+    eta = M.lognormal_grf_eta(m, m, m, seed=seed, sigma_decades=2.0, corr_len=0.1)
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(-1.0, 1.0, size=c.size)
+    return dict(m=m, coords=c, eta=eta, x=x, bits=M.FREE_SLIP)
+
+
+def algorithmic_bytes(m, elem_bytes=8):
+    """x read + y write + coords read + 27 eta per element (connectivity and
+    Dirichlet mask are index arithmetic)."""
+    nn = (2 * m + 1) ** 3
+    return elem_bytes * (3 * nn + 3 * nn + 3 * nn + 27 * m ** 3)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        return dist.get_rank(), world, local
+    return 0, 1, 0
+
+
+def reduce_max(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_apply(wl, steps, warmup, threads=None):
+    """Time the reference's own A11 kernel (AVX backend, OpenMP) on the host."""
+    from oracle.oracle import Reference, build
+    if not Reference.available():
+        build()
+    F = Reference()
+    m = wl["m"]
+    F.setup((m, m, m), wl["coords"], wl["eta"])
+    n = threads or os.cpu_count()
+    F.set_threads(n)
+    x = wl["x"]
+    y = np.zeros_like(x)
+    for _ in range(warmup):
+        F.a11_raw(x, "avx", out=y)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        F.a11_raw(x, "avx", out=y)
+    dt = (time.perf_counter() - t0) / steps
+    return dt, n
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = workload()
+    dt, n = cpu_reference_apply(wl, args.steps, args.warmup)
+    ndof = wl["x"].size
+    v = ndof / dt / 1e9
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "A11 MatMult, Q2 96^3 deformed mesh, log-normal eta", "elements": wl["m"] ** 3,
+                       "dofs": ndof},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": n, "kind": "reference",
+                             "sample": f"{args.steps} full applies of MFStokesWrapper_A11_AVX (OpenMP {n} threads)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    import ctypes as C
+
+    import torch
+
+    from ptatin3d_b200 import PREC_F32, PREC_F64, launch_count
+    from ptatin3d_b200._lib import BC_MATMULT, check, lib
+    from ptatin3d_b200.operators import MatA11MF, mesh_desc_whole
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    wl = workload()
+    m = wl["m"]
+    ndof = wl["x"].size
+    desc = mesh_desc_whole(m, m, m, wl["bits"])
+    op = MatA11MF(desc, PREC_F64, device=local)
+    op.set_coefficients(wl["coords"], wl["eta"])
+    L = lib()
+    check(L.p3d_op_set_bc_mode(op.h, BC_MATMULT))
+    x = torch.tensor(wl["x"], dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(x)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    xp, yp = C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())
+
+    def step():
+        check(L.p3d_a11_apply(op.h, xp, yp, sp))
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    n0 = launch_count()
+    with ClockSampler(local) as clk:
+        barrier(world)
+        torch.cuda.synchronize()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for e0, e1 in evs:
+            e0.record(stream)
+            step()
+            e1.record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    launches = launch_count() - n0
+    total_ms = t_start.elapsed_time(t_end)
+    kern_ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    step_ms = reduce_max(total_ms / args.steps, world)
+    value = world * ndof / (step_ms * 1e-3) / 1e9
+
+    # FP32 operator on the same mesh (the mixed-precision smoother's apply)
+    op32 = MatA11MF(desc, PREC_F32, device=local)
+    op32.set_coefficients(wl["coords"], wl["eta"])
+    check(L.p3d_op_set_bc_mode(op32.h, BC_MATMULT))
+    x32, y32 = x.float(), torch.zeros(ndof, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        check(L.p3d_a11_apply(op32.h, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), sp))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        check(L.p3d_a11_apply(op32.h, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), sp))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    f32_ms = e0.elapsed_time(e1) / args.steps
+    del op32, x32, y32
+
+    # end to end through the reference-facing host-buffer call (x in, y out each step)
+    xh = torch.tensor(wl["x"], dtype=torch.float64).pin_memory()
+    yh = torch.zeros(ndof, dtype=torch.float64).pin_memory()
+    xhp, yhp = C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr())
+    for _ in range(2):
+        check(L.p3d_a11_apply_host(op.h, xhp, yhp))
+    barrier(world)
+    t0 = time.perf_counter()
+    ne2e = max(3, args.steps // 2)
+    for _ in range(ne2e):
+        check(L.p3d_a11_apply_host(op.h, xhp, yhp))
+    e2e_s = reduce_max((time.perf_counter() - t0) / ne2e, world)
+    e2e_value = world * ndof / e2e_s / 1e9
+
+    peak, peak_kind = load_peaks()
+    ab = algorithmic_bytes(m)
+    achieved = ab / (kern_ms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get("a11_f64_general_96", None)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            sub = dict(wl)
+            dt, n = cpu_reference_apply(sub, steps=2, warmup=1)
+            cpu = {"value": ndof / dt / 1e9, "unit": UNIT, "cores": n, "kind": "reference",
+                   "sample": "2 full 96^3 applies of the reference MFStokesWrapper_A11_AVX (oracle/_ref), OpenMP"}
+        except Exception as exc:  # the baseline is reported, not required
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "A11 MatMult, Q2 96^3 deformed mesh (interior nodes +-0.2h), log-normal eta "
+                                       "(sigma 2 decades, corr 0.1), free-slip walls",
+                           "elements": m ** 3, "dofs": ndof, "geometry_path": "general" if op.geometry_mode == 1 else "affine",
+                           "l2": "inputs > L2 (709 MB/apply), no flush", "parallelism": f"replicas x{world}"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "algorithmic_bytes": ab, "kernel_ms": kern_ms},
+                "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof},
+                "gpu_launches": launches,
+                "clocks": clk.summary(),
+                "fp32_apply": {"ms": f32_ms, "GDoF/s": ndof / (f32_ms * 1e-3) / 1e9,
+                               "hbm_frac": algorithmic_bytes(m, 4) / (f32_ms * 1e-3) / 1e9 / peak}}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,138 @@
+/*
+ * p3d_b200 -- B200-native matrix-free Q2-P1disc Stokes operators for pTatin3d.
+ *
+ * Plain C ABI: every entry point takes plain pointers and sizes, returns an
+ * int status (P3D_OK == 0, never exits), and does not expose CUDA or torch
+ * types beyond an opaque stream handle (a cudaStream_t passed as void*; NULL
+ * means the default stream).
+ *
+ * Reference interfaces replaced (paths relative to the pTatin3d tree):
+ *   - the A11 SpMVOp callback triple {SpMVOp_MatMult, SpMVOp_SetUp,
+ *     SpMVOp_Destroy} of struct _p_MatA11MF       include/stokes_operators.h:47-62
+ *   - MFStokesWrapper_A11_CUDA / _Tensor / _AVX     src/stokes_operators_cuda.cu:457-532,
+ *                                                   src/stokes_operators_tensor.c:181-288,
+ *                                                   src/stokes_operators_avx.c:206-315
+ *   - MatGetDiagonal_MFStokes_A11 / MFStokesWrapper_diagA11
+ *                                                   src/stokes_operators.c:1060-1099,
+ *                                                   src/stokes_operators_mf.c:67-131
+ *   - MatMult_MFStokes_A12 / A21 (MFStokesWrapper_A12/_A21)
+ *                                                   src/stokes_operators.c:1284-1486,
+ *                                                   src/stokes_operators_mf.c:788-933
+ *   - MatMult_MFStokes_A (fused A11+A12+A21)        src/stokes_operators.c:884-967,
+ *                                                   src/stokes_operators_mf.c:707-786
+ *   - BCListInsertLocalZero / BCListInsertDirichlet_MatMult /
+ *     BCListInsertValueIntoDirichletSlot            src/dmda_bcs.c:409-611
+ *   - PCMG interpolation/restriction Mats (DMCreateInterpolation on the Q2
+ *     node lattice)                                 src/ptatin_driver_linear_ts.c:850,986-990
+ *
+ * Data layout (identical to the reference's ghosted local arrays):
+ *   velocity / coordinates : node-lexicographic (x fastest) on the ghosted
+ *                            node lattice gx*gy*gz, 3 interleaved components
+ *   viscosity              : eta[e*27 + q], e lexicographic over the local
+ *                            elements (x fastest), q = qi + 3qj + 9qk
+ *   pressure (P1disc)      : p[e*4 + i], basis [1, xh, yh, zh]
+ */
+#ifndef P3D_B200_H
+#define P3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ----------------------------------------------------------- status ---- */
+#define P3D_OK 0
+#define P3D_ERR_ARG 1     /* bad argument / size mismatch                  */
+#define P3D_ERR_CUDA 2    /* a CUDA runtime call failed (message retained) */
+#define P3D_ERR_STATE 3   /* call out of order (e.g. apply before setup)   */
+#define P3D_ERR_NOMEM 4   /* device allocation failed                      */
+#define P3D_ERR_NOCONV 5  /* a solve hit its iteration limit               */
+#define P3D_ERR_BREAKDOWN 6 /* a solve produced a non-finite residual      */
+#define P3D_ERR_TIMEOUT 7 /* a bounded wait ran out                        */
+
+/* ---------------------------------------------------------- meshes ---- */
+/* Dirichlet bits: bit (3*face + component), faces in this order.  A bit is
+ * honoured only on faces flagged in `global_faces` (faces of the local block
+ * that lie on the global domain boundary). */
+enum { P3D_FACE_IMIN = 0, P3D_FACE_IMAX, P3D_FACE_JMIN, P3D_FACE_JMAX, P3D_FACE_KMIN, P3D_FACE_KMAX };
+#define P3D_BC_BIT(face, comp) (1u << (3u * (unsigned)(face) + (unsigned)(comp)))
+
+typedef struct p3d_mesh_desc {
+  int32_t mx, my, mz;        /* local (owned) elements per direction              */
+  int32_t gx, gy, gz;        /* ghosted node-lattice extent of the local arrays   */
+  int32_t ox, oy, oz;        /* lattice index of the first node of element (0,0,0) */
+  uint32_t dirichlet;        /* P3D_BC_BIT mask                                   */
+  uint32_t global_faces;     /* bit f set: local face f lies on the global boundary */
+} p3d_mesh_desc;
+
+/* Fill a desc for one process owning a whole mx*my*mz mesh (no ghosts). */
+int p3d_mesh_desc_whole(int32_t mx, int32_t my, int32_t mz, uint32_t dirichlet, p3d_mesh_desc *out);
+
+/* --------------------------------------------------- device operator --- */
+typedef struct p3d_op p3d_op; /* opaque: one mesh + coefficients resident in HBM */
+
+#define P3D_PREC_F64 64
+#define P3D_PREC_F32 32
+
+#define P3D_GEOM_AUTO 0    /* affine fast path when every element is a parallelepiped */
+#define P3D_GEOM_GENERAL 1 /* per-quadrature-point Jacobian from the coordinates      */
+#define P3D_GEOM_AFFINE 2  /* force the per-element Jacobian (caller asserts affinity) */
+
+#define P3D_BC_NONE 0      /* raw element apply: y += sum_e A_e x  (SpMVOp contract)   */
+#define P3D_BC_MATMULT 1   /* MatMult contract: Dirichlet columns zeroed, rows y_k = x_k */
+
+/* Create an operator on device `device` for the mesh; precision P3D_PREC_*. */
+int p3d_op_create(const p3d_mesh_desc *mesh, int precision, int device, p3d_op **op);
+int p3d_op_destroy(p3d_op *op);
+/* Upload geometry and coefficients (host arrays, FP64).  coords: 3*gx*gy*gz,
+ * eta: 27*mx*my*mz.  Re-callable whenever the reference's Mat state changes
+ * (src/stokes_operators_cuda.cu:413-421). geom_mode: P3D_GEOM_*. */
+int p3d_op_set_coefficients(p3d_op *op, const double *coords, const double *eta, int geom_mode);
+/* Same, from device arrays already in HBM (FP64). */
+int p3d_op_set_coefficients_device(p3d_op *op, const double *coords_dev, const double *eta_dev, int geom_mode);
+int p3d_op_set_bc_mode(p3d_op *op, int bc_mode);
+/* Which geometry path setup selected (P3D_GEOM_GENERAL or P3D_GEOM_AFFINE). */
+int p3d_op_geometry_mode(const p3d_op *op, int *mode);
+/* Sizes: velocity dofs 3*gx*gy*gz, pressure dofs 4*mx*my*mz. */
+int p3d_op_sizes(const p3d_op *op, int64_t *n_velocity, int64_t *n_pressure);
+
+/* Device-pointer applies, asynchronous on `stream`.  Element type is the
+ * operator's precision (double* for F64, float* for F32).  All ADD into y
+ * (the caller zeroes y, as MatMult_MFStokes_A11 does at
+ * src/stokes_operators.c:1181); with P3D_BC_MATMULT the Dirichlet rows are
+ * overwritten with x instead. */
+int p3d_a11_apply(p3d_op *op, const void *x, void *y, void *stream);
+int p3d_a11_diagonal(p3d_op *op, void *d, void *stream);           /* d += diag(A11); Dirichlet slots = 1 with MATMULT */
+int p3d_a12_apply(p3d_op *op, const void *p, void *yu, void *stream);  /* yu += A12 p; Dirichlet rows 0 with MATMULT */
+int p3d_a21_apply(p3d_op *op, const void *u, void *yp, void *stream);  /* yp += A21 u; Dirichlet columns zeroed with MATMULT */
+int p3d_stokes_apply(p3d_op *op, const void *u, const void *p, void *yu, void *yp, void *stream); /* [A11 A12; A21 0] */
+
+/* Host-buffer apply with the reference CUDA backend's synchronous contract
+ * (src/stokes_operators_cuda.cu:457-532): copies x in, applies into a zeroed
+ * device y, copies y out (y = A11 x, overwriting y as the reference backend's
+ * CopyFrom_A11_CUDA does; its caller has zeroed Yu, so this equals the
+ * SpMVOp "+=" contract), and returns when y is complete. */
+int p3d_a11_apply_host(p3d_op *op, const double *x_host, double *y_host);
+
+/* --------------------------------------- multigrid transfer (DMDA) ---- */
+/* Trilinear prolongation on the node lattice, coarse (cnx,cny,cnz) nodes ->
+ * fine (2c-1) nodes, `ndof` interleaved components; xf = P xc (overwrite).
+ * Restriction is the transpose: xc = P^T xf (overwrite).  `prec` selects
+ * double or float element type. */
+int p3d_mg_prolong(int prec, int cnx, int cny, int cnz, int ndof, const void *xc, void *xf, void *stream);
+int p3d_mg_restrict(int prec, int cnx, int cny, int cnz, int ndof, const void *xf, void *xc, void *stream);
+
+/* -------------------------------------------------------- diagnostics --- */
+/* Last error message of the calling thread (static storage, never NULL). */
+const char *p3d_last_error(void);
+/* Number of kernels this library launched since load (all devices). */
+int64_t p3d_kernel_launch_count(void);
+/* Library version string. */
+const char *p3d_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* P3D_B200_H */

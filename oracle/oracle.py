@@ -1,0 +1,183 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Two independent checkers, both plain CPU code:
+  * ``Restatement`` -- oracle/liboracle.so, the C restatement in q2_oracle.c;
+  * ``Reference``   -- oracle/_ref/libp3dref.so, the reference's own element
+    kernels (stokes_operators_{tensor,avx,mf}.c, element_utils_q2.c) compiled
+    unmodified against oracle/shim by ``make -C oracle ref``.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module.  The product (ptatin3d_b200) never imports it.
+
+MatMult conventions applied here follow src/stokes_operators.c:1142-1205
+(A11), :1284-1350 (A12), :1424-1486 (A21), :1060-1099 (diagonal).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libp3dref.so")
+
+_dp = C.POINTER(C.c_double)
+_u8 = C.POINTER(C.c_uint8)
+
+
+def build(ref_dir: str | None = None, quiet: bool = True) -> None:
+    """Compile liboracle.so, and oracle/_ref when the pTatin3d tree is present."""
+    out = subprocess.DEVNULL if quiet else None
+    subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=out)
+    ref_dir = ref_dir or os.environ.get("P3D_REFERENCE_DIR", "/root/reference")
+    if os.path.isdir(os.path.join(ref_dir, "src")):
+        subprocess.run(["make", "-C", HERE, "ref", f"REF_DIR={ref_dir}"], check=True, stdout=out)
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+class Restatement:
+    def __init__(self):
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.o_a11_apply.argtypes = [C.c_int] * 3 + [_dp] * 4
+        L.o_a21_apply.argtypes = [C.c_int] * 3 + [_dp] * 3
+        L.o_a11_diag.argtypes = [C.c_int] * 3 + [_dp] * 3
+        L.o_a12_apply.argtypes = [C.c_int] * 3 + [_dp] * 3
+        L.o_schur_mass.argtypes = [C.c_int] * 3 + [_dp] * 3
+        L.o_a11_element_matrix.argtypes = [_dp] * 3
+        L.o_prolong.argtypes = [C.c_int] * 4 + [_dp] * 2
+        L.o_restrict.argtypes = [C.c_int] * 4 + [_dp] * 2
+        self.L = L
+
+    # raw element operators (y += ...), SpMVOp contract
+    def a11_raw(self, dims, coords, eta, x):
+        y = np.zeros_like(x)
+        self.L.o_a11_apply(*dims, _p(coords), _p(eta), _p(np.ascontiguousarray(x, dtype=np.float64)), _p(y))
+        return y
+
+    def diag_raw(self, dims, coords, eta):
+        nn = coords.size
+        y = np.zeros(nn)
+        self.L.o_a11_diag(*dims, _p(coords), _p(eta), _p(y))
+        return y
+
+    def a12_raw(self, dims, coords, p):
+        y = np.zeros(coords.size)
+        self.L.o_a12_apply(*dims, _p(coords), _p(np.ascontiguousarray(p, dtype=np.float64)), _p(y))
+        return y
+
+    def a21_raw(self, dims, coords, u):
+        nel = dims[0] * dims[1] * dims[2]
+        y = np.zeros(4 * nel)
+        self.L.o_a21_apply(*dims, _p(coords), _p(np.ascontiguousarray(u, dtype=np.float64)), _p(y))
+        return y
+
+    def schur_mass(self, dims, coords, eta):
+        nel = dims[0] * dims[1] * dims[2]
+        S = np.zeros(16 * nel)
+        self.L.o_schur_mass(*dims, _p(coords), _p(eta), _p(S))
+        return S.reshape(nel, 4, 4)
+
+    def element_matrix(self, elcoords, eta_e):
+        K = np.zeros(81 * 81)
+        self.L.o_a11_element_matrix(_p(np.ascontiguousarray(elcoords, dtype=np.float64)), _p(np.ascontiguousarray(eta_e, dtype=np.float64)), _p(K))
+        return K.reshape(81, 81)
+
+    def prolong(self, cn, ndof, xc):
+        fn = [2 * c - 1 for c in cn]
+        xf = np.zeros(fn[0] * fn[1] * fn[2] * ndof)
+        self.L.o_prolong(*cn, ndof, _p(np.ascontiguousarray(xc, dtype=np.float64)), _p(xf))
+        return xf
+
+    def restrict(self, cn, ndof, xf):
+        xc = np.zeros(cn[0] * cn[1] * cn[2] * ndof)
+        self.L.o_restrict(*cn, ndof, _p(np.ascontiguousarray(xf, dtype=np.float64)), _p(xc))
+        return xc
+
+
+class Reference:
+    """The reference's own kernels; one mesh at a time (module-global state in the driver)."""
+
+    VARIANTS = {"tensor": 0, "avx": 1, "ref": 2}
+
+    def __init__(self):
+        if not os.path.exists(REF_LIB):
+            build()
+        if not os.path.exists(REF_LIB):
+            raise FileNotFoundError("oracle/_ref/libp3dref.so not built (pTatin3d sources absent)")
+        L = C.CDLL(REF_LIB)
+        L.ref_setup.argtypes = [C.c_int] * 3 + [_dp] * 2
+        L.ref_a11.argtypes = [C.c_int, _dp, _dp]
+        L.ref_diag.argtypes = [_dp]
+        L.ref_a12.argtypes = [_dp, _dp]
+        L.ref_a21.argtypes = [_dp, _dp]
+        L.ref_set_threads.argtypes = [C.c_int]
+        self.L = L
+        self.dims = None
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_LIB)
+
+    def setup(self, dims, coords, eta):
+        self.dims = tuple(dims)
+        self._coords = np.ascontiguousarray(coords, dtype=np.float64)
+        self._eta = np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)
+        rc = self.L.ref_setup(*self.dims, _p(self._coords), _p(self._eta))
+        assert rc == 0
+
+    def set_threads(self, n):
+        self.L.ref_set_threads(int(n))
+
+    def a11_raw(self, x, variant="tensor", out=None):
+        y = np.zeros_like(x) if out is None else out
+        rc = self.L.ref_a11(self.VARIANTS[variant], _p(np.ascontiguousarray(x, dtype=np.float64)), _p(y))
+        assert rc == 0
+        return y
+
+    def diag_raw(self):
+        y = np.zeros(self._coords.size)
+        assert self.L.ref_diag(_p(y)) == 0
+        return y
+
+    def a12_raw(self, p):
+        y = np.zeros(self._coords.size)
+        assert self.L.ref_a12(_p(np.ascontiguousarray(p, dtype=np.float64)), _p(y)) == 0
+        return y
+
+    def a21_raw(self, u):
+        y = np.zeros(4 * self.dims[0] * self.dims[1] * self.dims[2])
+        assert self.L.ref_a21(_p(np.ascontiguousarray(u, dtype=np.float64)), _p(y)) == 0
+        return y
+
+
+# --------------------------------------------------- MatMult conventions ---
+def matmult_a11(raw, x, mask):
+    """MatMult_MFStokes_A11: zero Dirichlet columns, apply, y_k = x_k on Dirichlet rows."""
+    xl = np.where(mask.astype(bool), 0.0, x)
+    y = raw(xl)
+    y[mask.astype(bool)] = x[mask.astype(bool)]
+    return y
+
+
+def matmult_a12(raw, p, mask):
+    y = raw(p)
+    y[mask.astype(bool)] = 0.0
+    return y
+
+
+def matmult_a21(raw, u, mask):
+    return raw(np.where(mask.astype(bool), 0.0, u))
+
+
+def get_diagonal(raw_diag, mask):
+    d = raw_diag()
+    d[mask.astype(bool)] = 1.0
+    return d

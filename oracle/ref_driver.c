@@ -1,0 +1,241 @@
+/*
+ * Driver for the reference's own element kernels, compiled unmodified from
+ * the pTatin3d source tree against the PETSc stand-in headers in
+ * oracle/shim (see oracle/Makefile).  It supplies the few accessor functions
+ * those kernels call (DM coordinates, element connectivity, quadrature-point
+ * records, Gauss rule) over plain arrays for ONE process owning the whole
+ * mesh, and exports plain-C entry points:
+ *
+ *   ref_setup(mx,my,mz, coords[3*nn], eta[27*nel])
+ *   ref_a11(variant, x[3*nn], y[3*nn])   variant 0=tensor 1=avx 2=ref
+ *   ref_diag(y[3*nn]), ref_a12(p[4*nel], yu[3*nn]), ref_a21(u[3*nn], yp[4*nel])
+ *
+ * Each adds element contributions exactly as the reference's SpMVOp_MatMult
+ * callback does (the caller zeroes y and applies Dirichlet rows/columns).
+ *
+ * TEST INFRASTRUCTURE ONLY: built into oracle/_ref/libp3dref.so, used by
+ * tests/ and bench.py's CPU-baseline leg.  The product never links it.
+ */
+#include <omp.h>
+#include <stdarg.h>
+#include <sys/time.h>
+
+#include "petsc.h"
+#include "ptatin3d.h"
+#include "private/ptatin_impl.h"
+#include "ptatin3d_stokes.h"
+#include "stokes_operators.h"
+
+/* kernels provided by the reference objects */
+PetscErrorCode MFStokesWrapper_A11_Tensor(MatA11MF, Quadrature, DM, PetscScalar[], PetscScalar[]);
+PetscErrorCode MFStokesWrapper_A11_AVX(MatA11MF, Quadrature, DM, PetscScalar[], PetscScalar[]);
+PetscErrorCode MFStokesWrapper_A11(MatA11MF, Quadrature, DM, PetscScalar[], PetscScalar[]);
+PetscErrorCode MFStokesWrapper_diagA11(Quadrature, DM, PetscScalar[]);
+PetscErrorCode MFStokesWrapper_A12(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
+PetscErrorCode MFStokesWrapper_A21(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
+
+struct _p_shim_Vec {
+  PetscScalar *a;
+  long n;
+};
+struct _p_shim_DM {
+  int kind; /* 0 velocity (Q2 lattice, stencil 2), 1 pressure (P1disc, stencil 0) */
+  PetscInt M, N, P, dof, sw;
+  PetscInt nel, npe;
+  PetscInt *e;
+  struct _p_shim_Vec coords;
+};
+
+static struct _p_shim_DM g_dau, g_dap;
+static struct _p_Quadrature g_Q;
+static QPntVolCoefStokes *g_cells = NULL;
+
+/* ---------------------------------------------------------- accessors --- */
+PetscErrorCode PetscPrintf(MPI_Comm c, const char fmt[], ...) { (void)c; (void)fmt; return 0; }
+PetscErrorCode PetscTime(PetscLogDouble *t)
+{
+  struct timeval tv;
+  gettimeofday(&tv, NULL);
+  *t = tv.tv_sec + 1e-6 * tv.tv_usec;
+  return 0;
+}
+PetscErrorCode MPI_Comm_rank(MPI_Comm c, PetscMPIInt *r) { (void)c; *r = 0; return 0; }
+PetscErrorCode MPI_Comm_size(MPI_Comm c, PetscMPIInt *r) { (void)c; *r = 1; return 0; }
+PetscErrorCode MPI_Allreduce(const void *a, void *b, int n, MPI_Datatype t, MPI_Op o, MPI_Comm c)
+{
+  (void)o; (void)c;
+  memcpy(b, a, (size_t)n * (t == MPI_DOUBLE ? sizeof(double) : sizeof(int)));
+  return 0;
+}
+
+/* closed-form 3-point Gauss-Legendre rule on [a,b], ascending nodes */
+PetscErrorCode PetscDTGaussQuadrature(PetscInt npoints, PetscReal a, PetscReal b, PetscReal *x, PetscReal *w)
+{
+  if (npoints != 3) return PETSC_ERR_SUP;
+  const double s = sqrt(3.0 / 5.0);
+  const double xs[3] = {-s, 0.0, s}, ws[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+  for (int i = 0; i < 3; i++) {
+    x[i] = 0.5 * (b - a) * xs[i] + 0.5 * (b + a);
+    w[i] = 0.5 * (b - a) * ws[i];
+  }
+  return 0;
+}
+
+PetscErrorCode DMGetCoordinateDM(DM dm, DM *cdm) { *cdm = dm; return 0; }
+PetscErrorCode DMGetCoordinatesLocal(DM dm, Vec *c) { *c = &dm->coords; return 0; }
+PetscErrorCode VecGetArray(Vec v, PetscScalar **a) { *a = v->a; return 0; }
+PetscErrorCode VecRestoreArray(Vec v, PetscScalar **a) { (void)v; *a = NULL; return 0; }
+PetscErrorCode VecGetArrayRead(Vec v, const PetscScalar **a) { *a = v->a; return 0; }
+PetscErrorCode VecRestoreArrayRead(Vec v, const PetscScalar **a) { (void)v; *a = NULL; return 0; }
+PetscErrorCode PetscOptionsGetBool(void *o, const char p[], const char n[], PetscBool *v, PetscBool *s) { (void)o; (void)p; (void)n; (void)v; if (s) *s = PETSC_FALSE; return 0; }
+PetscErrorCode PetscOptionsGetInt(void *o, const char p[], const char n[], PetscInt *v, PetscBool *s) { (void)o; (void)p; (void)n; (void)v; if (s) *s = PETSC_FALSE; return 0; }
+PetscErrorCode PetscOptionsGetReal(void *o, const char p[], const char n[], PetscReal *v, PetscBool *s) { (void)o; (void)p; (void)n; (void)v; if (s) *s = PETSC_FALSE; return 0; }
+PetscErrorCode DMDAGetInfo(DM dm, PetscInt *dim, PetscInt *M, PetscInt *N, PetscInt *P, PetscInt *m, PetscInt *n,
+                           PetscInt *p, PetscInt *dof, PetscInt *sw, DMBoundaryType *bx, DMBoundaryType *by,
+                           DMBoundaryType *bz, DMDAStencilType *st)
+{
+  (void)bx; (void)by; (void)bz; (void)st;
+  if (dim) *dim = 3;
+  if (M) *M = dm->M;
+  if (N) *N = dm->N;
+  if (P) *P = dm->P;
+  if (m) *m = 1;
+  if (n) *n = 1;
+  if (p) *p = 1;
+  if (dof) *dof = dm->dof;
+  if (sw) *sw = dm->sw;
+  return 0;
+}
+PetscErrorCode DMDAGetGhostCorners(DM dm, PetscInt *x, PetscInt *y, PetscInt *z, PetscInt *m, PetscInt *n, PetscInt *p)
+{
+  if (x) *x = 0;
+  if (y) *y = 0;
+  if (z) *z = 0;
+  if (m) *m = dm->M;
+  if (n) *n = dm->N;
+  if (p) *p = dm->P;
+  return 0;
+}
+PetscErrorCode DMDAGetCorners(DM dm, PetscInt *x, PetscInt *y, PetscInt *z, PetscInt *m, PetscInt *n, PetscInt *p)
+{
+  return DMDAGetGhostCorners(dm, x, y, z, m, n, p);
+}
+
+PetscErrorCode DMDAGetElements_pTatinQ2P1(DM dm, PetscInt *nel, PetscInt *npe, const PetscInt **e)
+{
+  if (nel) *nel = dm->nel;
+  if (npe) *npe = dm->npe;
+  if (e) *e = dm->e;
+  return 0;
+}
+
+PetscErrorCode VolumeQuadratureGetAllCellData_Stokes(Quadrature Q, QPntVolCoefStokes *coeffs[])
+{
+  *coeffs = (QPntVolCoefStokes *)Q->shim_cells;
+  return 0;
+}
+PetscErrorCode VolumeQuadratureGetCellData_Stokes(Quadrature Q, QPntVolCoefStokes coeffs[], PetscInt cidx, QPntVolCoefStokes *cell[])
+{
+  *cell = &coeffs[cidx * Q->npoints];
+  return 0;
+}
+
+/* local dof indices of an element: 3 interleaved components per node */
+PetscErrorCode StokesVelocity_GetElementLocalIndices(PetscInt idx[], PetscInt elnid[])
+{
+  for (int n = 0; n < 27; n++)
+    for (int d = 0; d < 3; d++) idx[3 * n + d] = 3 * elnid[n] + d;
+  return 0;
+}
+PetscErrorCode StokesPressure_GetElementLocalIndices(PetscInt idx[], PetscInt elnid[])
+{
+  for (int n = 0; n < 4; n++) idx[n] = elnid[n];
+  return 0;
+}
+PetscErrorCode DMDASetValuesLocalStencil_AddValues_Stokes_Velocity(PetscScalar *F, PetscInt eqn[], PetscScalar Fe[])
+{
+  for (int k = 0; k < 81; k++) F[eqn[k]] += Fe[k];
+  return 0;
+}
+PetscErrorCode DMDASetValuesLocalStencil_AddValues_Stokes_Pressure(PetscScalar *F, PetscInt eqn[], PetscScalar Fe[])
+{
+  for (int k = 0; k < 4; k++) F[eqn[k]] += Fe[k];
+  return 0;
+}
+PetscErrorCode DMDAGetElementCoordinatesQ2_3D(PetscScalar elcoords[], PetscInt elnid[], PetscScalar LA_gcoords[])
+{
+  for (int n = 0; n < 27; n++)
+    for (int d = 0; d < 3; d++) elcoords[3 * n + d] = LA_gcoords[3 * elnid[n] + d];
+  return 0;
+}
+PetscErrorCode DMDAGetVectorElementFieldQ2_3D(PetscScalar elfield[], PetscInt elnid[], PetscScalar LA_gfield[])
+{
+  return DMDAGetElementCoordinatesQ2_3D(elfield, elnid, LA_gfield);
+}
+PetscErrorCode DMDAGetScalarElementField(PetscScalar elfield[], PetscInt npe, PetscInt elnid[], PetscScalar LA_gfield[])
+{
+  for (int n = 0; n < npe; n++) elfield[n] = LA_gfield[elnid[n]];
+  return 0;
+}
+
+/* ------------------------------------------------------------- entry --- */
+void ref_teardown(void)
+{
+  free(g_dau.e); g_dau.e = NULL;
+  free(g_dap.e); g_dap.e = NULL;
+  free(g_dau.coords.a); g_dau.coords.a = NULL;
+  free(g_cells); g_cells = NULL;
+}
+
+/* Build the one-process mesh: node lattice (2mx+1)x(2my+1)x(2mz+1), the
+ * lexicographic Q2 connectivity, the P1disc element-major pressure layout
+ * and the quadrature-point records (eta per QP; other fields zero). */
+int ref_setup(int mx, int my, int mz, const double *coords, const double *eta)
+{
+  ref_teardown();
+  int X = 2 * mx + 1, Y = 2 * my + 1, Z = 2 * mz + 1;
+  long nn = (long)X * Y * Z, nel = (long)mx * my * mz;
+  g_dau.kind = 0; g_dau.M = X; g_dau.N = Y; g_dau.P = Z; g_dau.dof = 3; g_dau.sw = 2;
+  g_dau.nel = (PetscInt)nel; g_dau.npe = 27;
+  g_dau.e = (PetscInt *)malloc(sizeof(PetscInt) * 27 * (nel + 1));
+  long cnt = 0;
+  for (int ek = 0; ek < mz; ek++)
+    for (int ej = 0; ej < my; ej++)
+      for (int ei = 0; ei < mx; ei++, cnt++)
+        for (int c = 0; c < 3; c++)
+          for (int b = 0; b < 3; b++)
+            for (int a = 0; a < 3; a++)
+              g_dau.e[27 * cnt + a + 3 * b + 9 * c] = (2 * ei + a) + X * ((2 * ej + b) + Y * (2 * ek + c));
+  g_dau.coords.n = 3 * nn;
+  g_dau.coords.a = (double *)malloc(sizeof(double) * 3 * nn);
+  memcpy(g_dau.coords.a, coords, sizeof(double) * 3 * nn);
+
+  g_dap.kind = 1; g_dap.M = mx; g_dap.N = my; g_dap.P = mz; g_dap.dof = 4; g_dap.sw = 0;
+  g_dap.nel = (PetscInt)nel; g_dap.npe = 4;
+  g_dap.e = (PetscInt *)malloc(sizeof(PetscInt) * 4 * (nel + 1));
+  for (long e = 0; e < nel; e++)
+    for (int d = 0; d < 4; d++) g_dap.e[4 * e + d] = (PetscInt)(4 * e + d);
+  g_dap.coords = g_dau.coords;
+
+  g_cells = (QPntVolCoefStokes *)calloc((size_t)nel * 27, sizeof(QPntVolCoefStokes));
+  for (long k = 0; k < nel * 27; k++) g_cells[k].eta = eta[k];
+  memset(&g_Q, 0, sizeof g_Q);
+  g_Q.dim = 3; g_Q.type = VOLUME_QUAD; g_Q.npoints = 27; g_Q.n_elements = (PetscInt)nel;
+  g_Q.shim_cells = g_cells;
+  return 0;
+}
+
+int ref_a11(int variant, double *x, double *y)
+{
+  switch (variant) {
+  case 0: return MFStokesWrapper_A11_Tensor(NULL, &g_Q, &g_dau, x, y);
+  case 1: return MFStokesWrapper_A11_AVX(NULL, &g_Q, &g_dau, x, y);
+  case 2: return MFStokesWrapper_A11(NULL, &g_Q, &g_dau, x, y);
+  default: return PETSC_ERR_SUP;
+  }
+}
+int ref_diag(double *y) { return MFStokesWrapper_diagA11(&g_Q, &g_dau, y); }
+int ref_a12(double *p, double *yu) { return MFStokesWrapper_A12(&g_Q, &g_dau, &g_dap, p, yu); }
+int ref_a21(double *u, double *yp) { return MFStokesWrapper_A21(&g_Q, &g_dau, &g_dap, u, yp); }
+int ref_set_threads(int n) { omp_set_num_threads(n); return 0; }
+int ref_max_threads(void) { return omp_get_max_threads(); }

@@ -1,0 +1,93 @@
+"""ctypes binding of the in-tree CUDA library ``libp3d_b200.so``.
+
+The library is the product: there is no CPU fallback.  Loading fails loudly
+when the shared object is missing, and every call that reports a nonzero
+status raises :class:`P3DError` with the library's message (the C ABI never
+exits the process, unlike the reference CUDA backend's CUDACHECK at
+src/stokes_operators_cuda.cu:46-57).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libp3d_b200.so")
+
+P3D_OK = 0
+P3D_ERR_ARG, P3D_ERR_CUDA, P3D_ERR_STATE, P3D_ERR_NOMEM, P3D_ERR_NOCONV, P3D_ERR_BREAKDOWN, P3D_ERR_TIMEOUT = range(1, 8)
+PREC_F64, PREC_F32 = 64, 32
+GEOM_AUTO, GEOM_GENERAL, GEOM_AFFINE = 0, 1, 2
+BC_NONE, BC_MATMULT = 0, 1
+FACE_IMIN, FACE_IMAX, FACE_JMIN, FACE_JMAX, FACE_KMIN, FACE_KMAX = range(6)
+
+
+def bc_bit(face: int, comp: int) -> int:
+    return 1 << (3 * face + comp)
+
+
+class P3DError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"p3d error {code}: {msg}")
+        self.code = code
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("mx", C.c_int32), ("my", C.c_int32), ("mz", C.c_int32),
+                ("gx", C.c_int32), ("gy", C.c_int32), ("gz", C.c_int32),
+                ("ox", C.c_int32), ("oy", C.c_int32), ("oz", C.c_int32),
+                ("dirichlet", C.c_uint32), ("global_faces", C.c_uint32)]
+
+
+_lib = None
+
+_SIGS = {
+    "p3d_last_error": ([], C.c_char_p),
+    "p3d_kernel_launch_count": ([], C.c_int64),
+    "p3d_version": ([], C.c_char_p),
+    "p3d_mesh_desc_whole": ([C.c_int32, C.c_int32, C.c_int32, C.c_uint32, C.POINTER(MeshDesc)], C.c_int),
+    "p3d_op_create": ([C.POINTER(MeshDesc), C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "p3d_op_destroy": ([C.c_void_p], C.c_int),
+    "p3d_op_set_coefficients": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "p3d_op_set_coefficients_device": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_int], C.c_int),
+    "p3d_op_set_bc_mode": ([C.c_void_p, C.c_int], C.c_int),
+    "p3d_op_geometry_mode": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "p3d_op_sizes": ([C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
+    "p3d_a11_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_a11_diagonal": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_a12_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_a21_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_stokes_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_a11_apply_host": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_mg_prolong": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_mg_restrict": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+}
+
+
+def lib():
+    """Load libp3d_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m ptatin3d_b200.build` "
+                          "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def check(rc: int):
+    if rc != P3D_OK:
+        raise P3DError(rc, lib().p3d_last_error().decode())
+
+
+def launch_count() -> int:
+    return int(lib().p3d_kernel_launch_count())

@@ -1,0 +1,112 @@
+// Geometric-multigrid transfer on the Q2 node lattice.
+//
+// PETSc's DMCreateInterpolation between two DMDAs whose node counts satisfy
+// Nf = 2 Nc - 1 (called at src/ptatin_driver_linear_ts.c:986-990 and handed to
+// PCMGSetInterpolation at :850) is the tensor-product linear interpolation on
+// the node lattice: a fine node with an even index coincides with a coarse
+// node, an odd index sits halfway between two.  Restriction is the transpose.
+// Both kernels are gathers (one thread per output node and component), so
+// they are deterministic and need no atomics.
+#include <cuda_runtime.h>
+
+#include "p3d_b200.h"
+#include "p3d_internal.h"
+
+namespace p3d {
+
+template <typename T>
+__global__ void prolong_kernel(int cnx, int cny, int cnz, int ndof, const T *__restrict__ xc, T *__restrict__ xf)
+{
+  const int fnx = 2 * cnx - 1, fny = 2 * cny - 1, fnz = 2 * cnz - 1;
+  const size_t total = (size_t)fnx * fny * fnz * ndof;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    int d = idx % ndof;
+    size_t node = idx / ndof;
+    int i = node % fnx, j = (node / fnx) % fny, k = node / ((size_t)fnx * fny);
+    int i0 = i >> 1, i1 = (i + 1) >> 1, j0 = j >> 1, j1 = (j + 1) >> 1, k0 = k >> 1, k1 = (k + 1) >> 1;
+    auto C = [&](int a, int b, int c) { return xc[((size_t)a + (size_t)cnx * ((size_t)b + (size_t)cny * c)) * ndof + d]; };
+    T v;
+    // the 2x2x2 average degenerates to copies along even directions
+    T s00 = C(i0, j0, k0) + C(i1, j0, k0), s10 = C(i0, j1, k0) + C(i1, j1, k0);
+    T s01 = C(i0, j0, k1) + C(i1, j0, k1), s11 = C(i0, j1, k1) + C(i1, j1, k1);
+    v = (T)0.125 * ((s00 + s10) + (s01 + s11));
+    xf[idx] = v;
+  }
+}
+
+template <typename T>
+__global__ void restrict_kernel(int cnx, int cny, int cnz, int ndof, const T *__restrict__ xf, T *__restrict__ xc)
+{
+  const int fnx = 2 * cnx - 1, fny = 2 * cny - 1, fnz = 2 * cnz - 1;
+  const size_t total = (size_t)cnx * cny * cnz * ndof;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    int d = idx % ndof;
+    size_t node = idx / ndof;
+    int I = node % cnx, J = (node / cnx) % cny, K = node / ((size_t)cnx * cny);
+    T acc = (T)0;
+    for (int c = -1; c <= 1; c++) {
+      int k = 2 * K + c;
+      if (k < 0 || k >= fnz) continue;
+      T wk = c == 0 ? (T)1 : (T)0.5;
+      for (int b = -1; b <= 1; b++) {
+        int j = 2 * J + b;
+        if (j < 0 || j >= fny) continue;
+        T wj = b == 0 ? (T)1 : (T)0.5;
+        for (int a = -1; a <= 1; a++) {
+          int i = 2 * I + a;
+          if (i < 0 || i >= fnx) continue;
+          T wi = a == 0 ? (T)1 : (T)0.5;
+          acc += wi * wj * wk * xf[((size_t)i + (size_t)fnx * ((size_t)j + (size_t)fny * k)) * ndof + d];
+        }
+      }
+    }
+    xc[idx] = acc;
+  }
+}
+
+static int tgrid(size_t n)
+{
+  size_t g = (n + 255) / 256;
+  if (g > 148 * 32) g = 148 * 32;
+  return g < 1 ? 1 : (int)g;
+}
+
+template <typename T> int mg_prolong(int cnx, int cny, int cnz, int ndof, const T *xc, T *xf, cudaStream_t st)
+{
+  size_t n = (size_t)(2 * cnx - 1) * (2 * cny - 1) * (2 * cnz - 1) * ndof;
+  prolong_kernel<T><<<tgrid(n), 256, 0, st>>>(cnx, cny, cnz, ndof, xc, xf);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "prolong launch");
+}
+template <typename T> int mg_restrict(int cnx, int cny, int cnz, int ndof, const T *xf, T *xc, cudaStream_t st)
+{
+  size_t n = (size_t)cnx * cny * cnz * ndof;
+  restrict_kernel<T><<<tgrid(n), 256, 0, st>>>(cnx, cny, cnz, ndof, xf, xc);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "restrict launch");
+}
+template int mg_prolong<double>(int, int, int, int, const double *, double *, cudaStream_t);
+template int mg_prolong<float>(int, int, int, int, const float *, float *, cudaStream_t);
+template int mg_restrict<double>(int, int, int, int, const double *, double *, cudaStream_t);
+template int mg_restrict<float>(int, int, int, int, const float *, float *, cudaStream_t);
+
+} // namespace p3d
+
+using namespace p3d;
+
+extern "C" {
+int p3d_mg_prolong(int prec, int cnx, int cny, int cnz, int ndof, const void *xc, void *xf, void *stream)
+{
+  if (cnx < 1 || cny < 1 || cnz < 1 || ndof < 1 || !xc || !xf) return set_error(P3D_ERR_ARG, "mg_prolong: bad args");
+  if (prec == P3D_PREC_F64) return mg_prolong<double>(cnx, cny, cnz, ndof, (const double *)xc, (double *)xf, (cudaStream_t)stream);
+  if (prec == P3D_PREC_F32) return mg_prolong<float>(cnx, cny, cnz, ndof, (const float *)xc, (float *)xf, (cudaStream_t)stream);
+  return set_error(P3D_ERR_ARG, "mg_prolong: precision must be 64 or 32");
+}
+int p3d_mg_restrict(int prec, int cnx, int cny, int cnz, int ndof, const void *xf, void *xc, void *stream)
+{
+  if (cnx < 1 || cny < 1 || cnz < 1 || ndof < 1 || !xc || !xf) return set_error(P3D_ERR_ARG, "mg_restrict: bad args");
+  if (prec == P3D_PREC_F64) return mg_restrict<double>(cnx, cny, cnz, ndof, (const double *)xf, (double *)xc, (cudaStream_t)stream);
+  if (prec == P3D_PREC_F32) return mg_restrict<float>(cnx, cny, cnz, ndof, (const float *)xf, (float *)xc, (cudaStream_t)stream);
+  return set_error(P3D_ERR_ARG, "mg_restrict: precision must be 64 or 32");
+}
+}

@@ -1,0 +1,36 @@
+// Internal (non-ABI) declarations shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "p3d_b200.h"
+
+namespace p3d {
+constexpr int NW_AFF = 4; // warp layers per CTA, affine A11 path (40 elements)
+constexpr int NW_GEN = 2; // warp layers per CTA, general-geometry paths (20 elements)
+
+int set_error(int code, const char *fmt, ...);
+int cuda_check(cudaError_t e, const char *what);
+void count_launch(int n);
+int dev_alloc(void **p, size_t bytes, const char *what);
+} // namespace p3d
+
+struct p3d_op {
+  p3d_mesh_desc m;
+  int prec = 64;
+  int device = 0;
+  int bc = 0;
+  int geom = 1;
+  bool have_coef = false;
+  void *coords = nullptr; // [3*gx*gy*gz] in operator precision
+  void *kgen = nullptr;   // general path: eta, brick order (NW_GEN)
+  void *kaff = nullptr;   // affine path: J^{-1} + eta*w*detJ, brick order (NW_AFF)
+  void *hx = nullptr, *hy = nullptr; // host-apply staging
+  cudaStream_t stream = nullptr;     // setup / host-apply stream
+};
+
+namespace p3d {
+template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st);
+template <typename T> int launch_diag(p3d_op *op, T *d, cudaStream_t st);
+template <typename T, bool DA11, bool DA12, bool DA21>
+int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st);
+} // namespace p3d

@@ -1,0 +1,442 @@
+// Operator objects and the C-ABI of libp3d_b200.so (see include/p3d_b200.h).
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "p3d_b200.h"
+#include "p3d_internal.h"
+#include "stokes_kernels.cuh"
+
+namespace p3d {
+
+// ------------------------------------------------------------- errors ----
+static thread_local char g_err[512] = "";
+std::atomic<long long> g_launches{0};
+
+int set_error(int code, const char *fmt, ...)
+{
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+int cuda_check(cudaError_t e, const char *what)
+{
+  if (e == cudaSuccess) return P3D_OK;
+  return set_error(P3D_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+void count_launch(int n) { g_launches += n; }
+
+static std::once_flag g_tables_once;
+static int upload_tables()
+{
+  static int rc = 0;
+  std::call_once(g_tables_once, [] {
+    double B[3][3], D[3][3];
+    const double s = std::sqrt(0.6), xs[3] = {-s, 0.0, s};
+    for (int q = 0; q < 3; q++) {
+      double x = xs[q];
+      B[q][0] = 0.5 * (x * x - x); B[q][1] = 1.0 - x * x; B[q][2] = 0.5 * (x * x + x);
+      D[q][0] = x - 0.5; D[q][1] = -2.0 * x; D[q][2] = x + 0.5;
+    }
+    rc = cuda_check(cudaMemcpyToSymbol(c_B, B, sizeof B), "cudaMemcpyToSymbol(B)");
+    if (!rc) rc = cuda_check(cudaMemcpyToSymbol(c_D, D, sizeof D), "cudaMemcpyToSymbol(D)");
+  });
+  return rc;
+}
+
+// brick counts for a layer height
+static void bricks(const p3d_mesh_desc &m, int nw, int &ntx, int &nty, int &ntz)
+{
+  ntx = (m.mx + TX - 1) / TX;
+  nty = (m.my + TY - 1) / TY;
+  ntz = (m.mz + nw - 1) / nw;
+}
+
+template <typename T> static TileArgs<T> tile_args(const p3d_op *op, int nw)
+{
+  TileArgs<T> a;
+  memset(&a, 0, sizeof a);
+  a.mx = op->m.mx; a.my = op->m.my; a.mz = op->m.mz;
+  a.gx = op->m.gx; a.gy = op->m.gy; a.gz = op->m.gz;
+  a.ox = op->m.ox; a.oy = op->m.oy; a.oz = op->m.oz;
+  bricks(op->m, nw, a.ntx, a.nty, a.ntz);
+  uint32_t dir = 0;
+  for (int f = 0; f < 6; f++)
+    if (op->m.global_faces & (1u << f)) dir |= op->m.dirichlet & (7u << (3 * f));
+  a.dir = dir;
+  a.bc = op->bc;
+  a.coords = reinterpret_cast<const T *>(op->coords);
+  return a;
+}
+
+template <typename K> static int prep_kernel(K kernel, size_t smem)
+{
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_check(e, "cudaFuncSetAttribute");
+  }
+  return P3D_OK;
+}
+
+template <typename T> static int nbricks_t(const TileArgs<T> &a) { return a.ntx * a.nty * a.ntz; }
+
+// ------------------------------------------------------------- launches ---
+template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st)
+{
+  if (op->geom == P3D_GEOM_AFFINE) {
+    TileArgs<T> a = tile_args<T>(op, NW_AFF);
+    a.x = x; a.y = y; a.kdat = reinterpret_cast<const T *>(op->kaff);
+    auto kern = a11_affine_kernel<T, NW_AFF>;
+    size_t smem = AffineSmem<T, NW_AFF>::BYTES;
+    int rc = prep_kernel(kern, smem);
+    if (rc) return rc;
+    if (nbricks_t(a) == 0) return P3D_OK;
+    kern<<<nbricks_t(a), 32 * NW_AFF, smem, st>>>(a);
+  } else {
+    TileArgs<T> a = tile_args<T>(op, NW_GEN);
+    a.x = x; a.y = y; a.kdat = reinterpret_cast<const T *>(op->kgen);
+    auto kern = stokes_general_kernel<T, NW_GEN, true, false, false>;
+    size_t smem = GeneralSmem<T, NW_GEN, true, false, false>::BYTES;
+    int rc = prep_kernel(kern, smem);
+    if (rc) return rc;
+    if (nbricks_t(a) == 0) return P3D_OK;
+    kern<<<nbricks_t(a), 32 * NW_GEN, smem, st>>>(a);
+  }
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "a11 launch");
+}
+
+template <typename T, bool DA11, bool DA12, bool DA21>
+int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st)
+{
+  TileArgs<T> a = tile_args<T>(op, NW_GEN);
+  a.x = u; a.y = yu; a.p = p; a.yp = yp; a.kdat = reinterpret_cast<const T *>(op->kgen);
+  auto kern = stokes_general_kernel<T, NW_GEN, DA11, DA12, DA21>;
+  size_t smem = GeneralSmem<T, NW_GEN, DA11, DA12, DA21>::BYTES;
+  int rc = prep_kernel(kern, smem);
+  if (rc) return rc;
+  if (nbricks_t(a) == 0) return P3D_OK;
+  kern<<<nbricks_t(a), 32 * NW_GEN, smem, st>>>(a);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "stokes launch");
+}
+
+template <typename T> int launch_diag(p3d_op *op, T *d, cudaStream_t st)
+{
+  TileArgs<T> a = tile_args<T>(op, NW_GEN);
+  a.y = d; a.kdat = reinterpret_cast<const T *>(op->kgen); a.diag = 1;
+  auto kern = diag_general_kernel<T, NW_GEN>;
+  size_t smem = GeneralSmem<T, NW_GEN, true, false, false>::BYTES;
+  int rc = prep_kernel(kern, smem);
+  if (rc) return rc;
+  if (nbricks_t(a) == 0) return P3D_OK;
+  kern<<<nbricks_t(a), 32 * NW_GEN, smem, st>>>(a);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "diag launch");
+}
+
+template int launch_a11<double>(p3d_op *, const double *, double *, cudaStream_t);
+template int launch_a11<float>(p3d_op *, const float *, float *, cudaStream_t);
+template int launch_diag<double>(p3d_op *, double *, cudaStream_t);
+template int launch_diag<float>(p3d_op *, float *, cudaStream_t);
+template int launch_general<double, true, true, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t);
+template int launch_general<float, true, true, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t);
+template int launch_general<double, false, true, false>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t);
+template int launch_general<double, false, false, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t);
+template int launch_general<float, false, true, false>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t);
+template int launch_general<float, false, false, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t);
+
+// --------------------------------------------------------------- setup ---
+static void free_dev(void *&p)
+{
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+int dev_alloc(void **p, size_t bytes, const char *what)
+{
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_error(P3D_ERR_NOMEM, "cudaMalloc(%zu) for %s: %s", bytes, what, cudaGetErrorString(e));
+  }
+  return P3D_OK;
+}
+
+template <typename T>
+__global__ void convert_kernel(size_t n, const double *__restrict__ src, T *__restrict__ dst)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (T)src[i];
+}
+
+static int grid_for(size_t n, int block = 256)
+{
+  size_t g = (n + block - 1) / block;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// coords/eta are device FP64 arrays
+int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geom_mode)
+{
+  const p3d_mesh_desc &m = op->m;
+  size_t nn = (size_t)m.gx * m.gy * m.gz, nel = (size_t)m.mx * m.my * m.mz;
+  size_t es = op->prec == P3D_PREC_F64 ? 8 : 4;
+  int rc;
+  cudaStream_t st = op->stream;
+  // coordinates in operator precision
+  if (!op->coords && (rc = dev_alloc(&op->coords, 3 * nn * es, "coords"))) return rc;
+  if (op->prec == P3D_PREC_F64)
+    rc = cuda_check(cudaMemcpyAsync(op->coords, coords, 3 * nn * 8, cudaMemcpyDeviceToDevice, st), "copy coords");
+  else {
+    convert_kernel<float><<<grid_for(3 * nn), 256, 0, st>>>(3 * nn, coords, (float *)op->coords);
+    count_launch(1);
+    rc = cuda_check(cudaGetLastError(), "convert coords");
+  }
+  if (rc) return rc;
+  // general-path eta in brick order
+  int ntx, nty, ntz;
+  bricks(m, NW_GEN, ntx, nty, ntz);
+  size_t ng = (size_t)ntx * nty * ntz * Brick<NW_GEN>::NE * 27;
+  free_dev(op->kgen);
+  if ((rc = dev_alloc(&op->kgen, ng * es, "eta (brick order)"))) return rc;
+  if (op->prec == P3D_PREC_F64)
+    pack_eta_kernel<double, NW_GEN><<<grid_for(ng), 256, 0, st>>>(m.mx, m.my, m.mz, ntx, nty, ntz, eta, (double *)op->kgen);
+  else
+    pack_eta_kernel<float, NW_GEN><<<grid_for(ng), 256, 0, st>>>(m.mx, m.my, m.mz, ntx, nty, ntz, eta, (float *)op->kgen);
+  count_launch(1);
+  if ((rc = cuda_check(cudaGetLastError(), "pack eta"))) return rc;
+  // affinity
+  int mode = geom_mode;
+  if (mode == P3D_GEOM_AUTO) {
+    unsigned long long *bad = nullptr, hbad = 0;
+    if ((rc = dev_alloc((void **)&bad, sizeof *bad, "affine flag"))) return rc;
+    cudaMemsetAsync(bad, 0, sizeof *bad, st);
+    affine_check_kernel<<<grid_for(nel), 256, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz, coords, 1e-13, bad);
+    count_launch(1);
+    rc = cuda_check(cudaMemcpyAsync(&hbad, bad, sizeof hbad, cudaMemcpyDeviceToHost, st), "affine flag");
+    if (!rc) rc = cuda_check(cudaStreamSynchronize(st), "affine sync");
+    cudaFree(bad);
+    if (rc) return rc;
+    mode = (hbad == 0 && nel > 0) ? P3D_GEOM_AFFINE : P3D_GEOM_GENERAL;
+  }
+  free_dev(op->kaff);
+  if (mode == P3D_GEOM_AFFINE) {
+    bricks(m, NW_AFF, ntx, nty, ntz);
+    size_t na = (size_t)ntx * nty * ntz * Brick<NW_AFF>::NE;
+    if ((rc = dev_alloc(&op->kaff, na * 36 * es, "affine geometry"))) return rc;
+    if (op->prec == P3D_PREC_F64)
+      pack_affine_kernel<double, NW_AFF><<<grid_for(na), 256, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz,
+                                                                      ntx, nty, ntz, coords, eta, (double *)op->kaff);
+    else
+      pack_affine_kernel<float, NW_AFF><<<grid_for(na), 256, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz,
+                                                                     ntx, nty, ntz, coords, eta, (float *)op->kaff);
+    count_launch(1);
+    if ((rc = cuda_check(cudaGetLastError(), "pack affine"))) return rc;
+  }
+  op->geom = mode;
+  op->have_coef = true;
+  return cuda_check(cudaStreamSynchronize(st), "setup sync");
+}
+
+} // namespace p3d
+
+using namespace p3d;
+
+// ============================================================== C ABI ====
+extern "C" {
+
+const char *p3d_last_error(void) { return g_err; }
+int64_t p3d_kernel_launch_count(void) { return (int64_t)g_launches.load(); }
+const char *p3d_version(void) { return "p3d_b200 0.1 (sm_100a)"; }
+
+int p3d_mesh_desc_whole(int32_t mx, int32_t my, int32_t mz, uint32_t dirichlet, p3d_mesh_desc *out)
+{
+  if (!out || mx < 1 || my < 1 || mz < 1) return set_error(P3D_ERR_ARG, "p3d_mesh_desc_whole: bad sizes");
+  out->mx = mx; out->my = my; out->mz = mz;
+  out->gx = 2 * mx + 1; out->gy = 2 * my + 1; out->gz = 2 * mz + 1;
+  out->ox = out->oy = out->oz = 0;
+  out->dirichlet = dirichlet;
+  out->global_faces = 0x3f;
+  return P3D_OK;
+}
+
+int p3d_op_create(const p3d_mesh_desc *mesh, int precision, int device, p3d_op **out)
+{
+  if (!mesh || !out) return set_error(P3D_ERR_ARG, "p3d_op_create: null argument");
+  *out = nullptr;
+  const p3d_mesh_desc &m = *mesh;
+  if (m.mx < 1 || m.my < 1 || m.mz < 1) return set_error(P3D_ERR_ARG, "p3d_op_create: empty mesh");
+  if (m.ox < 0 || m.oy < 0 || m.oz < 0 || m.ox + 2 * m.mx + 1 > m.gx || m.oy + 2 * m.my + 1 > m.gy ||
+      m.oz + 2 * m.mz + 1 > m.gz)
+    return set_error(P3D_ERR_ARG, "p3d_op_create: element block exceeds the ghosted lattice");
+  if (precision != P3D_PREC_F64 && precision != P3D_PREC_F32)
+    return set_error(P3D_ERR_ARG, "p3d_op_create: precision must be 64 or 32");
+  int ndev = 0;
+  if (int rc = cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount")) return rc;
+  if (device < 0 || device >= ndev) return set_error(P3D_ERR_ARG, "p3d_op_create: device %d of %d", device, ndev);
+  if (int rc = cuda_check(cudaSetDevice(device), "cudaSetDevice")) return rc;
+  if (int rc = upload_tables()) return rc;
+  p3d_op *op = new p3d_op();
+  op->m = m;
+  op->prec = precision;
+  op->device = device;
+  op->bc = P3D_BC_NONE;
+  op->geom = P3D_GEOM_GENERAL;
+  if (int rc = cuda_check(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking), "cudaStreamCreate")) {
+    delete op;
+    return rc;
+  }
+  *out = op;
+  return P3D_OK;
+}
+
+int p3d_op_destroy(p3d_op *op)
+{
+  if (!op) return P3D_OK;
+  cudaSetDevice(op->device);
+  free_dev(op->coords);
+  free_dev(op->kgen);
+  free_dev(op->kaff);
+  free_dev(op->hx);
+  free_dev(op->hy);
+  if (op->stream) cudaStreamDestroy(op->stream);
+  delete op;
+  return P3D_OK;
+}
+
+int p3d_op_set_coefficients_device(p3d_op *op, const double *coords, const double *eta, int geom_mode)
+{
+  if (!op || !coords || !eta) return set_error(P3D_ERR_ARG, "set_coefficients: null argument");
+  if (geom_mode < P3D_GEOM_AUTO || geom_mode > P3D_GEOM_AFFINE) return set_error(P3D_ERR_ARG, "bad geometry mode");
+  cudaSetDevice(op->device);
+  return op_setup_device(op, coords, eta, geom_mode);
+}
+
+int p3d_op_set_coefficients(p3d_op *op, const double *coords, const double *eta, int geom_mode)
+{
+  if (!op || !coords || !eta) return set_error(P3D_ERR_ARG, "set_coefficients: null argument");
+  cudaSetDevice(op->device);
+  const p3d_mesh_desc &m = op->m;
+  size_t nn = (size_t)m.gx * m.gy * m.gz, nel = (size_t)m.mx * m.my * m.mz;
+  void *dc = nullptr, *de = nullptr;
+  int rc = dev_alloc(&dc, 3 * nn * 8, "coords staging");
+  if (!rc) rc = dev_alloc(&de, 27 * nel * 8, "eta staging");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(dc, coords, 3 * nn * 8, cudaMemcpyHostToDevice, op->stream), "H2D coords");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(de, eta, 27 * nel * 8, cudaMemcpyHostToDevice, op->stream), "H2D eta");
+  if (!rc) rc = p3d_op_set_coefficients_device(op, (const double *)dc, (const double *)de, geom_mode);
+  cudaStreamSynchronize(op->stream);
+  if (dc) cudaFree(dc);
+  if (de) cudaFree(de);
+  return rc;
+}
+
+int p3d_op_set_bc_mode(p3d_op *op, int bc_mode)
+{
+  if (!op || (bc_mode != P3D_BC_NONE && bc_mode != P3D_BC_MATMULT)) return set_error(P3D_ERR_ARG, "bad bc mode");
+  op->bc = bc_mode;
+  return P3D_OK;
+}
+
+int p3d_op_geometry_mode(const p3d_op *op, int *mode)
+{
+  if (!op || !mode) return set_error(P3D_ERR_ARG, "null argument");
+  *mode = op->geom;
+  return P3D_OK;
+}
+
+int p3d_op_sizes(const p3d_op *op, int64_t *nv, int64_t *np)
+{
+  if (!op) return set_error(P3D_ERR_ARG, "null argument");
+  if (nv) *nv = 3LL * op->m.gx * op->m.gy * op->m.gz;
+  if (np) *np = 4LL * op->m.mx * op->m.my * op->m.mz;
+  return P3D_OK;
+}
+
+#define P3D_REQUIRE_SETUP(op)                                                                                    \
+  do {                                                                                                           \
+    if (!(op)) return set_error(P3D_ERR_ARG, "null operator");                                                   \
+    if (!(op)->have_coef) return set_error(P3D_ERR_STATE, "operator coefficients not set");                      \
+  } while (0)
+
+int p3d_a11_apply(p3d_op *op, const void *x, void *y, void *stream)
+{
+  P3D_REQUIRE_SETUP(op);
+  if (!x || !y) return set_error(P3D_ERR_ARG, "a11_apply: null vector");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (op->prec == P3D_PREC_F64) return launch_a11<double>(op, (const double *)x, (double *)y, st);
+  return launch_a11<float>(op, (const float *)x, (float *)y, st);
+}
+
+int p3d_a11_diagonal(p3d_op *op, void *d, void *stream)
+{
+  P3D_REQUIRE_SETUP(op);
+  if (!d) return set_error(P3D_ERR_ARG, "a11_diagonal: null vector");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (op->prec == P3D_PREC_F64) return launch_diag<double>(op, (double *)d, st);
+  return launch_diag<float>(op, (float *)d, st);
+}
+
+int p3d_a12_apply(p3d_op *op, const void *p, void *yu, void *stream)
+{
+  P3D_REQUIRE_SETUP(op);
+  if (!p || !yu) return set_error(P3D_ERR_ARG, "a12_apply: null vector");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (op->prec == P3D_PREC_F64)
+    return launch_general<double, false, true, false>(op, nullptr, (const double *)p, (double *)yu, nullptr, st);
+  return launch_general<float, false, true, false>(op, nullptr, (const float *)p, (float *)yu, nullptr, st);
+}
+
+int p3d_a21_apply(p3d_op *op, const void *u, void *yp, void *stream)
+{
+  P3D_REQUIRE_SETUP(op);
+  if (!u || !yp) return set_error(P3D_ERR_ARG, "a21_apply: null vector");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (op->prec == P3D_PREC_F64)
+    return launch_general<double, false, false, true>(op, (const double *)u, nullptr, nullptr, (double *)yp, st);
+  return launch_general<float, false, false, true>(op, (const float *)u, nullptr, nullptr, (float *)yp, st);
+}
+
+int p3d_stokes_apply(p3d_op *op, const void *u, const void *p, void *yu, void *yp, void *stream)
+{
+  P3D_REQUIRE_SETUP(op);
+  if (!u || !p || !yu || !yp) return set_error(P3D_ERR_ARG, "stokes_apply: null vector");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (op->prec == P3D_PREC_F64)
+    return launch_general<double, true, true, true>(op, (const double *)u, (const double *)p, (double *)yu,
+                                                    (double *)yp, st);
+  return launch_general<float, true, true, true>(op, (const float *)u, (const float *)p, (float *)yu, (float *)yp, st);
+}
+
+int p3d_a11_apply_host(p3d_op *op, const double *xh, double *yh)
+{
+  P3D_REQUIRE_SETUP(op);
+  if (!xh || !yh) return set_error(P3D_ERR_ARG, "a11_apply_host: null vector");
+  if (op->prec != P3D_PREC_F64) return set_error(P3D_ERR_ARG, "a11_apply_host: FP64 operators only");
+  cudaSetDevice(op->device);
+  size_t n = 3ull * op->m.gx * op->m.gy * op->m.gz;
+  int rc;
+  if (!op->hx && (rc = dev_alloc(&op->hx, n * 8, "host-apply x"))) return rc;
+  if (!op->hy && (rc = dev_alloc(&op->hy, n * 8, "host-apply y"))) return rc;
+  cudaStream_t st = op->stream;
+  if ((rc = cuda_check(cudaMemcpyAsync(op->hx, xh, n * 8, cudaMemcpyHostToDevice, st), "H2D x"))) return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(op->hy, 0, n * 8, st), "zero y"))) return rc;
+  if ((rc = launch_a11<double>(op, (const double *)op->hx, (double *)op->hy, st))) return rc;
+  if ((rc = cuda_check(cudaMemcpyAsync(yh, op->hy, n * 8, cudaMemcpyDeviceToHost, st), "D2H y"))) return rc;
+  return cuda_check(cudaStreamSynchronize(st), "host apply sync");
+}
+
+} // extern "C"

@@ -1,0 +1,458 @@
+// Element kernels built on the brick decomposition of q2_tile.cuh.
+//
+//   a11_affine_kernel      y += A11 x, per-element constant Jacobian
+//   stokes_general_kernel  any of {A11, A12, A21} with per-Gauss-point geometry
+//   diag_general_kernel    d += diag(A11)
+//   setup kernels          brick packing of eta, affinity test, affine packing
+#pragma once
+#include "q2_tile.cuh"
+
+namespace p3d {
+
+__host__ __device__ constexpr int align16(int n_elems, int elem_bytes)
+{
+  return ((n_elems * elem_bytes + 15) / 16) * 16 / elem_bytes;
+}
+
+// lane -> element slot/component inside the warp's 5x2 layer
+struct LaneMap {
+  int slot, a, b, c, f, base;
+  bool active; // lane < 30
+};
+__device__ __forceinline__ LaneMap lane_map()
+{
+  LaneMap m;
+  int lane = threadIdx.x & 31;
+  int s = lane / 3;
+  m.active = lane < 30;
+  if (!m.active) s = 9; // idle lanes mirror slot 9 and never write
+  m.f = m.active ? lane - 3 * s : lane - 30;
+  m.base = 3 * s;
+  m.a = s % TX;
+  m.b = s / TX;
+  m.c = threadIdx.x >> 5;
+  m.slot = m.a + TX * (m.b + TY * m.c);
+  return m;
+}
+
+template <int NW> __device__ __forceinline__ int brick_node(int a, int b, int c, int n)
+{
+  using BK = Brick<NW>;
+  return (2 * a + n % 3) + BK::NX * ((2 * b + (n / 3) % 3) + BK::NY * (2 * c + n / 9));
+}
+
+// 3x3 inverse: M[3d+l] = dx_l/dxi_d  ->  Mi[3k+d] = dxi_d/dx_k, returns det
+template <typename T> __device__ __forceinline__ T inv3(const T M[9], T Mi[9])
+{
+  T c00 = M[4] * M[8] - M[5] * M[7];
+  T c01 = -(M[3] * M[8] - M[5] * M[6]);
+  T c02 = M[3] * M[7] - M[4] * M[6];
+  T c10 = -(M[1] * M[8] - M[2] * M[7]);
+  T c11 = M[0] * M[8] - M[2] * M[6];
+  T c12 = -(M[0] * M[7] - M[1] * M[6]);
+  T c20 = M[1] * M[5] - M[2] * M[4];
+  T c21 = -(M[0] * M[5] - M[2] * M[3]);
+  T c22 = M[0] * M[4] - M[1] * M[3];
+  T det = M[0] * c00 + M[1] * c01 + M[2] * c02;
+  T r = (T)1 / det;
+  // Mi[k][d] = cof[d][k] / det
+  Mi[0] = c00 * r; Mi[1] = c10 * r; Mi[2] = c20 * r;
+  Mi[3] = c01 * r; Mi[4] = c11 * r; Mi[5] = c21 * r;
+  Mi[6] = c02 * r; Mi[7] = c12 * r; Mi[8] = c22 * r;
+  return det;
+}
+
+// Pass 1 of the general path: per-Gauss-point geometry of the lane's element
+// into g[q*GQ + ...]: [0..8] J^{-1} (row k = physical direction), [9] eta*w*detJ,
+// [10] w*detJ, [11..13] pressure-basis coordinates (xh,yh,zh) when PB.
+template <typename T, int NW, int GQ, bool PB>
+__device__ __forceinline__ void geometry_pass(const T *s_c, const T *s_eta, T *g, const LaneMap &L, bool valid)
+{
+  T xq[27];
+#pragma unroll
+  for (int n = 0; n < 27; n++) xq[n] = s_c[3 * brick_node<NW>(L.a, L.b, L.c, n) + L.f];
+  T avg = (T)0, rL = (T)1;
+  if (PB) {
+#pragma unroll
+    for (int n = 0; n < 27; n++) avg += xq[n];
+    avg *= cst<T>(1.0 / 27.0);
+    T Lf = (L.f == 0) ? xq[14] - xq[12] : ((L.f == 1) ? xq[16] - xq[10] : xq[22] - xq[4]);
+    rL = valid ? (T)1 / Lf : (T)0;
+  }
+  interp27(xq);
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const int q = i + 3 * j + 9 * k;
+        T d0 = dcol(i, xq[3 * j + 9 * k], xq[1 + 3 * j + 9 * k], xq[2 + 3 * j + 9 * k]);
+        T d1 = dcol(j, xq[i + 9 * k], xq[i + 3 + 9 * k], xq[i + 6 + 9 * k]);
+        T d2 = dcol(k, xq[i + 3 * j], xq[i + 3 * j + 9], xq[i + 3 * j + 18]);
+        if (!valid) { d0 = (T)(L.f == 0); d1 = (T)(L.f == 1); d2 = (T)(L.f == 2); }
+        if (L.active) {
+          g[q * GQ + 0 + L.f] = d0; // J[0][f]
+          g[q * GQ + 3 + L.f] = d1; // J[1][f]
+          g[q * GQ + 6 + L.f] = d2; // J[2][f]
+          if (PB) g[q * GQ + 11 + L.f] = (xq[q] - avg) * rL;
+        }
+      }
+  __syncwarp();
+  for (int t = 0; t < 9; t++) {
+    const int q = 3 * t + L.f;
+    const int qi = q % 3, qj = (q / 3) % 3, qk = q / 9;
+    T *G = g + q * GQ;
+    T M[9], Mi[9];
+#pragma unroll
+    for (int r = 0; r < 9; r++) M[r] = G[r];
+    T det = inv3(M, Mi);
+    T w = (T)(w1d(qi) * w1d(qj) * w1d(qk)) * det;
+    T eta = valid ? s_eta[q] : (T)0;
+    if (L.active) {
+#pragma unroll
+      for (int r = 0; r < 9; r++) G[r] = Mi[r];
+      G[9] = eta * w;
+      if (GQ > 10) G[10] = valid ? w : (T)0;
+    }
+  }
+  __syncwarp();
+}
+
+// load the lane's component of the element's 27 nodal values and move to Gauss points
+template <typename T, int NW> __device__ __forceinline__ void load_interp(const T *s_x, const LaneMap &L, T uq[27])
+{
+#pragma unroll
+  for (int n = 0; n < 27; n++) uq[n] = s_x[3 * brick_node<NW>(L.a, L.b, L.c, n) + L.f];
+  interp27(uq);
+}
+
+// strain -> stress -> pulled-back test-side vector for one Gauss point.
+// Jr rows rotated so row 0 = physical direction f.  Returns ro[3] (reference dirs).
+template <typename T>
+__device__ __forceinline__ void qp_action(const T Jr[9], T ce, T g0, T g1, T g2, int src1, int src2, T &D0, T &ro0,
+                                          T &ro1, T &ro2)
+{
+  D0 = Jr[0] * g0 + Jr[1] * g1 + Jr[2] * g2;       // dux[f][f]
+  T D1 = Jr[3] * g0 + Jr[4] * g1 + Jr[5] * g2;     // dux[f+1][f]
+  T D2 = Jr[6] * g0 + Jr[7] * g1 + Jr[8] * g2;     // dux[f+2][f]
+  T rc1 = __shfl_sync(0xffffffffu, D2, src1);      // dux[f][f+1]
+  T rc2 = __shfl_sync(0xffffffffu, D1, src2);      // dux[f][f+2]
+  T T0 = ce * (D0 + D0), T1 = ce * (D1 + rc1), T2 = ce * (D2 + rc2);
+  ro0 = Jr[0] * T0 + Jr[3] * T1 + Jr[6] * T2;
+  ro1 = Jr[1] * T0 + Jr[4] * T1 + Jr[7] * T2;
+  ro2 = Jr[2] * T0 + Jr[5] * T1 + Jr[8] * T2;
+}
+
+template <typename T, int i, int j, int k> struct QP {
+  static constexpr int q = i + 3 * j + 9 * k;
+};
+
+// gradient of the Gauss-point field uq at (i,j,k) in reference directions
+#define P3D_GRAD(uq, i, j, k, g0, g1, g2)                                                                       \
+  T g0 = dcol(i, uq[3 * (j) + 9 * (k)], uq[1 + 3 * (j) + 9 * (k)], uq[2 + 3 * (j) + 9 * (k)]);                  \
+  T g1 = dcol(j, uq[(i) + 9 * (k)], uq[(i) + 3 + 9 * (k)], uq[(i) + 6 + 9 * (k)]);                              \
+  T g2 = dcol(k, uq[(i) + 3 * (j)], uq[(i) + 3 * (j) + 9], uq[(i) + 3 * (j) + 18]);
+#define P3D_SCATTER(r, i, j, k, ro0, ro1, ro2)                                                                  \
+  dcolT(i, ro0, r[3 * (j) + 9 * (k)], r[1 + 3 * (j) + 9 * (k)], r[2 + 3 * (j) + 9 * (k)]);                       \
+  dcolT(j, ro1, r[(i) + 9 * (k)], r[(i) + 3 + 9 * (k)], r[(i) + 6 + 9 * (k)]);                                   \
+  dcolT(k, ro2, r[(i) + 3 * (j)], r[(i) + 3 * (j) + 9], r[(i) + 3 * (j) + 18]);
+
+// ---------------------------------------------------------------- A11 affine
+template <typename T, int NW> struct AffineSmem {
+  using BK = Brick<NW>;
+  static constexpr int KS = 36; // J^{-1} (9) + eta*w*detJ (27)
+  static constexpr int OX = 0;
+  static constexpr int OK = align16(3 * BK::NN, sizeof(T));
+  static constexpr int OO = OK + align16(BK::NE * KS, sizeof(T));
+  static constexpr int TOTAL = OO + BK::NE * 81;
+  static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
+};
+
+template <typename T, int NW>
+__global__ void __launch_bounds__(32 * NW) a11_affine_kernel(TileArgs<T> A)
+{
+  using BK = Brick<NW>;
+  using SM = AffineSmem<T, NW>;
+  extern __shared__ __align__(16) unsigned char p3d_smem[];
+  T *sm = reinterpret_cast<T *>(p3d_smem);
+  T *s_x = sm + SM::OX, *s_k = sm + SM::OK, *s_out = sm + SM::OO;
+  const BrickPos b = brick_pos<T, NW>(A);
+  load_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
+  copy_vec(A.kdat + (size_t)blockIdx.x * BK::NE * SM::KS, s_k, BK::NE * SM::KS);
+  __syncthreads();
+
+  const LaneMap L = lane_map();
+  const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
+  const T *K = s_k + L.slot * SM::KS;
+  T Jr[9];
+  {
+    const int r0 = 3 * L.f, r1 = 3 * ((L.f + 1) % 3), r2 = 3 * ((L.f + 2) % 3);
+#pragma unroll
+    for (int d = 0; d < 3; d++) { Jr[d] = K[r0 + d]; Jr[3 + d] = K[r1 + d]; Jr[6 + d] = K[r2 + d]; }
+  }
+  T uq[27], r[27];
+  load_interp<T, NW>(s_x, L, uq);
+#pragma unroll
+  for (int n = 0; n < 27; n++) r[n] = (T)0;
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        P3D_GRAD(uq, i, j, k, g0, g1, g2)
+        T D0, ro0, ro1, ro2;
+        qp_action(Jr, K[9 + i + 3 * j + 9 * k], g0, g1, g2, src1, src2, D0, ro0, ro1, ro2);
+        P3D_SCATTER(r, i, j, k, ro0, ro1, ro2)
+      }
+  interp27T(r);
+  if (L.active) {
+#pragma unroll
+    for (int n = 0; n < 27; n++) s_out[L.slot * 81 + 3 * n + L.f] = r[n];
+  }
+  __syncthreads();
+  gather_store<T, NW>(A, b, s_out, 81, 0);
+}
+
+// ------------------------------------------------------- general geometry
+template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSmem {
+  using BK = Brick<NW>;
+  static constexpr bool NEEDX = DA11 || DA21;
+  static constexpr int GQ = (DA12 || DA21) ? 14 : 10;
+  static constexpr int OX = 0;
+  static constexpr int OC = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OK = OC + align16(3 * BK::NN, sizeof(T));
+  static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
+  static constexpr int TOTAL = OG + BK::NE * 27 * GQ;
+  static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
+};
+
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
+{
+  using BK = Brick<NW>;
+  using SM = GeneralSmem<T, NW, DA11, DA12, DA21>;
+  constexpr int GQ = SM::GQ;
+  constexpr bool PB = DA12 || DA21;
+  constexpr bool NEEDY = DA11 || DA12;
+  extern __shared__ __align__(16) unsigned char p3d_smem[];
+  T *sm = reinterpret_cast<T *>(p3d_smem);
+  T *s_x = sm + SM::OX, *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
+  const BrickPos b = brick_pos<T, NW>(A);
+  if (SM::NEEDX) load_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
+  load_nodes<T, NW>(A, b, A.coords, s_c, false);
+  copy_vec(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  __syncthreads();
+
+  const LaneMap L = lane_map();
+  const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
+  T *g = s_g + L.slot * 27 * GQ;
+  geometry_pass<T, NW, GQ, PB>(s_c, s_k + L.slot * 27, g, L, valid);
+
+  const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
+  const int r0 = 3 * L.f, r1 = 3 * ((L.f + 1) % 3), r2 = 3 * ((L.f + 2) % 3);
+  const size_t eg = (size_t)(b.e0x + L.a) + (size_t)A.mx * ((size_t)(b.e0y + L.b) + (size_t)A.my * (b.e0z + L.c));
+  T uq[27], r[27];
+  if (SM::NEEDX) load_interp<T, NW>(s_x, L, uq);
+#pragma unroll
+  for (int n = 0; n < 27; n++) r[n] = (T)0;
+  T pe0 = 0, pe1 = 0, pe2 = 0, pe3 = 0;
+  if (DA12 && valid) { pe0 = A.p[4 * eg]; pe1 = A.p[4 * eg + 1]; pe2 = A.p[4 * eg + 2]; pe3 = A.p[4 * eg + 3]; }
+  T ap0 = 0, ap1 = 0, ap2 = 0, ap3 = 0;
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const T *G = g + (i + 3 * j + 9 * k) * GQ;
+        T Jr[9];
+#pragma unroll
+        for (int d = 0; d < 3; d++) { Jr[d] = G[r0 + d]; Jr[3 + d] = G[r1 + d]; Jr[6 + d] = G[r2 + d]; }
+        T ro0 = 0, ro1 = 0, ro2 = 0, D0 = 0;
+        if (SM::NEEDX) {
+          P3D_GRAD(uq, i, j, k, g0, g1, g2)
+          if (DA11) {
+            qp_action(Jr, G[9], g0, g1, g2, src1, src2, D0, ro0, ro1, ro2);
+          } else {
+            D0 = Jr[0] * g0 + Jr[1] * g1 + Jr[2] * g2;
+          }
+        }
+        if (PB) {
+          const T c0 = G[10], xh = G[11], yh = G[12], zh = G[13];
+          if (DA12) {
+            T t = -c0 * (pe0 + pe1 * xh + pe2 * yh + pe3 * zh);
+            ro0 += t * Jr[0]; ro1 += t * Jr[1]; ro2 += t * Jr[2];
+          }
+          if (DA21) {
+            T t = -c0 * D0;
+            ap0 += t; ap1 += t * xh; ap2 += t * yh; ap3 += t * zh;
+          }
+        }
+        if (NEEDY) { P3D_SCATTER(r, i, j, k, ro0, ro1, ro2) }
+      }
+  if (DA21) {
+    // divergence = sum over the element's three lanes
+    ap0 += __shfl_sync(0xffffffffu, ap0, src1) + __shfl_sync(0xffffffffu, ap0, src2);
+    ap1 += __shfl_sync(0xffffffffu, ap1, src1) + __shfl_sync(0xffffffffu, ap1, src2);
+    ap2 += __shfl_sync(0xffffffffu, ap2, src1) + __shfl_sync(0xffffffffu, ap2, src2);
+    ap3 += __shfl_sync(0xffffffffu, ap3, src1) + __shfl_sync(0xffffffffu, ap3, src2);
+    if (L.active && valid && L.f == 0) {
+      A.yp[4 * eg] += ap0; A.yp[4 * eg + 1] += ap1; A.yp[4 * eg + 2] += ap2; A.yp[4 * eg + 3] += ap3;
+    }
+  }
+  if (NEEDY) {
+    __syncwarp();
+    interp27T(r);
+    if (L.active) {
+#pragma unroll
+      for (int n = 0; n < 27; n++) g[3 * n + L.f] = r[n];
+    }
+    __syncthreads();
+    gather_store<T, NW>(A, b, s_g, 27 * GQ, DA11 ? 0 : 1);
+  }
+}
+
+// --------------------------------------------------------------- diagonal
+__constant__ double c_B[3][3];
+__constant__ double c_D[3][3];
+
+template <typename T, int NW>
+__global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
+{
+  using BK = Brick<NW>;
+  using SM = GeneralSmem<T, NW, true, false, false>;
+  constexpr int GQ = SM::GQ;
+  extern __shared__ __align__(16) unsigned char p3d_smem[];
+  T *sm = reinterpret_cast<T *>(p3d_smem);
+  T *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
+  const BrickPos b = brick_pos<T, NW>(A);
+  load_nodes<T, NW>(A, b, A.coords, s_c, false);
+  copy_vec(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  __syncthreads();
+  const LaneMap L = lane_map();
+  const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
+  T *g = s_g + L.slot * 27 * GQ;
+  geometry_pass<T, NW, GQ, false>(s_c, s_k + L.slot * 27, g, L, valid);
+  T dg[27];
+#pragma unroll
+  for (int n = 0; n < 27; n++) dg[n] = (T)0;
+  for (int q = 0; q < 27; q++) {
+    const int qi = q % 3, qj = (q / 3) % 3, qk = q / 9;
+    const T *G = g + q * GQ;
+    T Ji[9];
+#pragma unroll
+    for (int r = 0; r < 9; r++) Ji[r] = G[r];
+    const T ce = G[9];
+#pragma unroll
+    for (int n = 0; n < 27; n++) {
+      const int na = n % 3, nb = (n / 3) % 3, nc = n / 9;
+      T r0 = (T)(c_D[qi][na] * c_B[qj][nb] * c_B[qk][nc]);
+      T r1 = (T)(c_B[qi][na] * c_D[qj][nb] * c_B[qk][nc]);
+      T r2 = (T)(c_B[qi][na] * c_B[qj][nb] * c_D[qk][nc]);
+      T d0 = Ji[0] * r0 + Ji[1] * r1 + Ji[2] * r2;
+      T d1 = Ji[3] * r0 + Ji[4] * r1 + Ji[5] * r2;
+      T d2 = Ji[6] * r0 + Ji[7] * r1 + Ji[8] * r2;
+      T df = (L.f == 0) ? d0 : ((L.f == 1) ? d1 : d2);
+      dg[n] += ce * (d0 * d0 + d1 * d1 + d2 * d2 + df * df);
+    }
+  }
+  __syncwarp();
+  if (L.active) {
+#pragma unroll
+    for (int n = 0; n < 27; n++) g[3 * n + L.f] = dg[n];
+  }
+  __syncthreads();
+  gather_store<T, NW>(A, b, s_g, 27 * GQ, 2);
+}
+
+// ---------------------------------------------------------------- setup ---
+// eta (element-lexicographic, FP64) -> brick-ordered [brick][slot][27] in T
+template <typename T, int NW>
+__global__ void pack_eta_kernel(int mx, int my, int mz, int ntx, int nty, int ntz, const double *__restrict__ eta,
+                                T *__restrict__ out)
+{
+  using BK = Brick<NW>;
+  size_t total = (size_t)ntx * nty * ntz * BK::NE * 27;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    int q = idx % 27;
+    size_t rest = idx / 27;
+    int slot = rest % BK::NE;
+    size_t t = rest / BK::NE;
+    int tx = t % ntx, ty = (t / ntx) % nty, tz = t / ((size_t)ntx * nty);
+    int a = slot % TX, bb = (slot / TX) % TY, c = slot / (TX * TY);
+    int ex = tx * TX + a, ey = ty * TY + bb, ez = tz * NW + c;
+    T v = (T)0;
+    if (ex < mx && ey < my && ez < mz) v = (T)eta[27 * ((size_t)ex + (size_t)mx * ((size_t)ey + (size_t)my * ez)) + q];
+    out[idx] = v;
+  }
+}
+
+// count elements that are not parallelepipeds (to relative tolerance tol)
+__global__ void affine_check_kernel(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz,
+                                    const double *__restrict__ coords, double tol, unsigned long long *bad)
+{
+  size_t nel = (size_t)mx * my * mz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nel; e += (size_t)gridDim.x * blockDim.x) {
+    int ex = e % mx, ey = (e / mx) % my, ez = e / ((size_t)mx * my);
+    auto X = [&](int a, int b2, int c, int d) {
+      size_t gi = (size_t)(ox + 2 * ex + a) + (size_t)gx * ((size_t)(oy + 2 * ey + b2) + (size_t)gy * (oz + 2 * ez + c));
+      return coords[3 * gi + d];
+    };
+    double dev = 0.0, h = 0.0;
+    for (int d = 0; d < 3; d++) {
+      double x0 = X(0, 0, 0, d);
+      double j0 = 0.5 * (X(2, 0, 0, d) - x0), j1 = 0.5 * (X(0, 2, 0, d) - x0), j2 = 0.5 * (X(0, 0, 2, d) - x0);
+      h = fmax(h, fmax(fabs(j0), fmax(fabs(j1), fabs(j2))));
+      for (int c = 0; c < 3; c++)
+        for (int b2 = 0; b2 < 3; b2++)
+          for (int a = 0; a < 3; a++) {
+            double pred = x0 + j0 * a + j1 * b2 + j2 * c;
+            dev = fmax(dev, fabs(X(a, b2, c, d) - pred));
+          }
+    }
+    if (!(dev <= tol * h)) atomicAdd(bad, 1ull);
+  }
+}
+
+// per element J^{-1} and eta*w*detJ (affine elements), brick-ordered [brick][slot][36]
+template <typename T, int NW>
+__global__ void pack_affine_kernel(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, int ntx, int nty,
+                                   int ntz, const double *__restrict__ coords, const double *__restrict__ eta,
+                                   T *__restrict__ out)
+{
+  using BK = Brick<NW>;
+  size_t total = (size_t)ntx * nty * ntz * BK::NE;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    int slot = idx % BK::NE;
+    size_t t = idx / BK::NE;
+    int tx = t % ntx, ty = (t / ntx) % nty, tz = t / ((size_t)ntx * nty);
+    int a = slot % TX, bb = (slot / TX) % TY, c = slot / (TX * TY);
+    int ex = tx * TX + a, ey = ty * TY + bb, ez = tz * NW + c;
+    T *o = out + idx * 36;
+    if (!(ex < mx && ey < my && ez < mz)) {
+      for (int r = 0; r < 36; r++) o[r] = (T)0;
+      continue;
+    }
+    auto X = [&](int a2, int b2, int c2, int d) {
+      size_t gi = (size_t)(ox + 2 * ex + a2) + (size_t)gx * ((size_t)(oy + 2 * ey + b2) + (size_t)gy * (oz + 2 * ez + c2));
+      return coords[3 * gi + d];
+    };
+    double M[9], Mi[9];
+    for (int l = 0; l < 3; l++) {
+      M[0 + l] = 0.5 * (X(2, 1, 1, l) - X(0, 1, 1, l)); // dx_l/dxi_0
+      M[3 + l] = 0.5 * (X(1, 2, 1, l) - X(1, 0, 1, l)); // dx_l/dxi_1
+      M[6 + l] = 0.5 * (X(1, 1, 2, l) - X(1, 1, 0, l)); // dx_l/dxi_2
+    }
+    double det = inv3<double>(M, Mi);
+    for (int r = 0; r < 9; r++) o[r] = (T)Mi[r];
+    size_t e = (size_t)ex + (size_t)mx * ((size_t)ey + (size_t)my * ez);
+    for (int q = 0; q < 27; q++) {
+      int qi = q % 3, qj = (q / 3) % 3, qk = q / 9;
+      o[9 + q] = (T)(eta[27 * e + q] * w1d(qi) * w1d(qj) * w1d(qk) * det);
+    }
+  }
+}
+
+} // namespace p3d

@@ -1,0 +1,48 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares
+(no GPU needed: nothing here launches a kernel)."""
+import ctypes as C
+import glob
+import os
+import re
+import subprocess
+
+from ptatin3d_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        txt = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        names |= set(re.findall(r"\b(p3d_[a-z0-9_]+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    missing = [n for n in sorted(declared()) if not hasattr(L, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (p3d_\w+)", out))
+    assert declared() <= exported, declared() - exported
+
+
+def test_bindings_cover_header():
+    assert declared() <= set(_lib.exported_symbols())
+
+
+def test_errors_are_codes_not_exits():
+    L = _lib.lib()
+    d = _lib.MeshDesc()
+    assert L.p3d_mesh_desc_whole(0, 1, 1, 0, C.byref(d)) == _lib.P3D_ERR_ARG
+    assert b"bad sizes" in L.p3d_last_error()
+    assert L.p3d_op_create(None, 64, 0, None) == _lib.P3D_ERR_ARG
+    assert L.p3d_a11_apply(None, None, None, None) == _lib.P3D_ERR_ARG
+    assert L.p3d_mg_prolong(16, 2, 2, 2, 3, None, None, None) == _lib.P3D_ERR_ARG
+
+
+def test_mesh_desc_whole():
+    d = _lib.MeshDesc()
+    assert _lib.lib().p3d_mesh_desc_whole(4, 5, 6, 7, C.byref(d)) == 0
+    assert (d.gx, d.gy, d.gz, d.ox, d.global_faces) == (9, 11, 13, 0, 0x3F)
