@@ -39,13 +39,19 @@ METRIC = "A11 MF apply GDoF/s (FP64, 96^3 Q2 deformed mesh)"
 UNIT = "GDoF/s"
 
 
-def workload(m=96, seed=4):
+def workload(m=96, seed=4, kind="deformed"):
+    """deformed: interior nodes perturbed, per-element log-normal eta (general geometry path);
+    layered: uniform mesh, 6 layers of log10 eta in [-3,3] + 16 inclusions (affine path)."""
     from ptatin3d_b200 import mesh as M
-    c = M.perturb_interior(M.uniform_coords(m, m, m), m, m, m, frac=0.2, seed=seed)
-    eta = M.lognormal_grf_eta(m, m, m, seed=seed, sigma_decades=2.0, corr_len=0.1)
+    c = M.uniform_coords(m, m, m)
+    if kind == "deformed":
+        c = M.perturb_interior(c, m, m, m, frac=0.2, seed=seed)
+        eta = M.lognormal_grf_eta(m, m, m, seed=seed, sigma_decades=2.0, corr_len=0.1)
+    else:
+        eta = M.layered_eta(M.qp_coords(c, m, m, m), seed=seed)
     rng = np.random.default_rng(seed)
     x = rng.uniform(-1.0, 1.0, size=c.size)
-    return dict(m=m, coords=c, eta=eta, x=x, bits=M.FREE_SLIP)
+    return dict(m=m, coords=c, eta=eta, x=x, bits=M.FREE_SLIP, kind=kind)
 
 
 def algorithmic_bytes(m, elem_bytes=8):
@@ -199,7 +205,7 @@ def run_b200(args):
 
     rank, world, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    wl = workload()
+    wl = workload(args.size, kind=args.workload)
     m = wl["m"]
     ndof = wl["x"].size
     desc = mesh_desc_whole(m, m, m, wl["bits"])
@@ -257,6 +263,8 @@ def run_b200(args):
     del op32, x32, y32
 
     # end to end through the reference-facing host-buffer call (x in, y out each step)
+    if args.no_e2e:
+        args.steps_e2e = 0
     xh = torch.tensor(wl["x"], dtype=torch.float64).pin_memory()
     yh = torch.zeros(ndof, dtype=torch.float64).pin_memory()
     xhp, yhp = C.c_void_p(xh.data_ptr()), C.c_void_p(yh.data_ptr())
@@ -264,7 +272,7 @@ def run_b200(args):
         check(L.p3d_a11_apply_host(op.h, xhp, yhp))
     barrier(world)
     t0 = time.perf_counter()
-    ne2e = max(3, args.steps // 2)
+    ne2e = max(3, args.steps // 2) if not args.no_e2e else 1
     for _ in range(ne2e):
         check(L.p3d_a11_apply_host(op.h, xhp, yhp))
     e2e_s = reduce_max((time.perf_counter() - t0) / ne2e, world)
@@ -319,6 +327,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--size", type=int, default=96, help="elements per direction")
+    ap.add_argument("--workload", default="deformed", choices=["deformed", "layered"])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -170,90 +170,118 @@ template <typename T, int NW> __device__ __forceinline__ BrickPos brick_pos(cons
   return b;
 }
 
-// stage a node field (3 comps) of the brick into shared memory; optional Dirichlet masking
+// ------------------------------------------------------ async staging ---
+// cp.async global -> shared copies: every load of a brick is in flight at once
+// (no register round trip); src_bytes = 0 zero-fills the destination.
+template <int BYTES> __device__ __forceinline__ void cp_async(void *smem, const void *gmem, int src_bytes)
+{
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+  else if (BYTES == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Stage a 3-component node field of the brick, row by row (a row = 2TX+1
+// nodes along x = 33 contiguous values in global memory), one warp per row.
+// mask: zero the Dirichlet entries (MatMult column convention).
 template <typename T, int NW>
-__device__ __forceinline__ void load_nodes(const TileArgs<T> &A, const BrickPos &b, const T *__restrict__ src, T *s,
-                                           bool mask)
+__device__ __forceinline__ void stage_nodes(const TileArgs<T> &A, const BrickPos &b, const T *__restrict__ src, T *s,
+                                            bool mask)
 {
   using BK = Brick<NW>;
+  constexpr int ROWLEN = 3 * BK::NX, NROWS = BK::NY * BK::NZ;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nax = 2 * b.ax + 1, nay = 2 * b.ay + 1, naz = 2 * b.az + 1;
   const int exn = A.ox + 2 * A.mx, eyn = A.oy + 2 * A.my, ezn = A.oz + 2 * A.mz;
-  for (int idx = threadIdx.x; idx < 3 * BK::NN; idx += blockDim.x) {
-    int row = idx / (3 * BK::NX), col = idx - row * (3 * BK::NX);
-    int li = col / 3, comp = col - 3 * li;
-    int lj = row % BK::NY, lk = row / BK::NY;
-    T v = (T)0;
-    if (li < nax && lj < nay && lk < naz) {
-      int ix = b.n0x + li, iy = b.n0y + lj, iz = b.n0z + lk;
-      size_t g = (size_t)ix + (size_t)A.gx * ((size_t)iy + (size_t)A.gy * (size_t)iz);
-      v = __ldg(src + 3 * g + comp);
-      if (mask && is_dirichlet(A.dir, ix, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, comp)) v = (T)0;
+  for (int row = warp; row < NROWS; row += NW) {
+    const int lj = row % BK::NY, lk = row / BK::NY;
+    const int iy = b.n0y + lj, iz = b.n0z + lk;
+    const bool rowok = lj < nay && lk < naz;
+    const size_t base = 3 * ((size_t)b.n0x + (size_t)A.gx * ((size_t)iy + (size_t)A.gy * (size_t)iz));
+    for (int col = lane; col < ROWLEN; col += 32) {
+      const int li = col / 3, comp = col - 3 * li;
+      bool ok = rowok && li < nax;
+      if (ok && mask) ok = !is_dirichlet(A.dir, b.n0x + li, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, comp);
+      cp_async<sizeof(T)>(s + row * ROWLEN + col, ok ? (const void *)(src + base + col) : (const void *)src,
+                          ok ? (int)sizeof(T) : 0);
     }
-    s[idx] = v;
   }
 }
 
-// coalesced vector copy global -> shared (n elements of T, both 16-byte aligned)
-template <typename T> __device__ __forceinline__ void copy_vec(const T *__restrict__ g, T *s, int n)
+// contiguous, 16-byte aligned block (brick-ordered coefficients)
+template <typename T> __device__ __forceinline__ void stage_block(const T *__restrict__ g, T *s, int n)
 {
-  const int n4 = (n * (int)sizeof(T)) / 16;
-  const int4 *g4 = reinterpret_cast<const int4 *>(g);
-  int4 *s4 = reinterpret_cast<int4 *>(s);
-  for (int i = threadIdx.x; i < n4; i += blockDim.x) s4[i] = __ldg(g4 + i);
-  for (int i = n4 * (16 / (int)sizeof(T)) + threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
+  const int n16 = (n * (int)sizeof(T)) / 16;
+  for (int i = threadIdx.x; i < n16; i += blockDim.x)
+    cp_async<16>(reinterpret_cast<char *>(s) + 16 * i, reinterpret_cast<const char *>(g) + 16 * i, 16);
+  for (int i = n16 * (16 / (int)sizeof(T)) + threadIdx.x; i < n; i += blockDim.x)
+    cp_async<sizeof(T)>(s + i, g + i, (int)sizeof(T));
 }
 
 // Sum the element contributions of every brick node and add them into y.
-// s_out[slot*ostride + 3*n + f] holds element slot's contribution to its local node n, comp f.
+// s_out[slot*ostride + 3*n + f]: element slot's contribution to its local node n, comp f.
+// s_y: the brick's y values staged at kernel start (y += acc without a global load).
+// Nodes on brick faces shared with a neighbouring brick are added with atomicAdd
+// (fire-and-forget reductions), every other node with a plain store.
 // rowmode: 0 -> Dirichlet rows get x (A11 / full operator), 1 -> 0 (A12), 2 -> 1 (diagonal)
 template <typename T, int NW>
 __device__ __forceinline__ void gather_store(const TileArgs<T> &A, const BrickPos &b, const T *s_out, int ostride,
-                                             int rowmode)
+                                             const T *s_y, int rowmode)
 {
   using BK = Brick<NW>;
+  constexpr int ROWLEN = 3 * BK::NX, NROWS = BK::NY * BK::NZ;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nax = 2 * b.ax + 1, nay = 2 * b.ay + 1, naz = 2 * b.az + 1;
   const int exn = A.ox + 2 * A.mx, eyn = A.oy + 2 * A.my, ezn = A.oz + 2 * A.mz;
   const bool lo_x = b.tx > 0, lo_y = b.ty > 0, lo_z = b.tz > 0;
   const bool hi_x = b.e0x + b.ax < A.mx, hi_y = b.e0y + b.ay < A.my, hi_z = b.e0z + b.az < A.mz;
-  for (int idx = threadIdx.x; idx < 3 * BK::NN; idx += blockDim.x) {
-    int row = idx / (3 * BK::NX), col = idx - row * (3 * BK::NX);
-    int li = col / 3, f = col - 3 * li;
-    int lj = row % BK::NY, lk = row / BK::NY;
-    if (li >= nax || lj >= nay || lk >= naz) continue;
-    // candidate elements along each axis: node 2e+{0,1,2}
-    int ea0 = (li - 1) >> 1, ea1 = li >> 1;
-    int eb0 = (lj - 1) >> 1, eb1 = lj >> 1;
-    int ec0 = (lk - 1) >> 1, ec1 = lk >> 1;
-    T acc = (T)0;
+  for (int row = warp; row < NROWS; row += NW) {
+    const int lj = row % BK::NY, lk = row / BK::NY;
+    if (lj >= nay || lk >= naz) continue;
+    const int iy = b.n0y + lj, iz = b.n0z + lk;
+    const size_t base = 3 * ((size_t)b.n0x + (size_t)A.gx * ((size_t)iy + (size_t)A.gy * (size_t)iz));
+    const int eb0 = (lj - 1) >> 1, eb1 = lj >> 1, ec0 = (lk - 1) >> 1, ec1 = lk >> 1;
+    const bool row_shared = (lj == 0 && lo_y) || (lj == nay - 1 && hi_y) || (lk == 0 && lo_z) || (lk == naz - 1 && hi_z);
+    for (int col = lane; col < ROWLEN; col += 32) {
+      const int li = col / 3, f = col - 3 * li;
+      if (li >= nax) continue;
+      const int ea0 = (li - 1) >> 1, ea1 = li >> 1;
+      T acc = (T)0;
 #pragma unroll
-    for (int kc = 0; kc < 2; kc++) {
-      int ec = kc ? ec1 : ec0;
-      if (ec < 0 || ec >= b.az || (kc && ec1 == ec0)) continue;
+      for (int kc = 0; kc < 2; kc++) {
+        const int ec = kc ? ec1 : ec0;
+        if (ec < 0 || ec >= b.az || (kc && ec1 == ec0)) continue;
 #pragma unroll
-      for (int kb = 0; kb < 2; kb++) {
-        int eb = kb ? eb1 : eb0;
-        if (eb < 0 || eb >= b.ay || (kb && eb1 == eb0)) continue;
+        for (int kb = 0; kb < 2; kb++) {
+          const int eb = kb ? eb1 : eb0;
+          if (eb < 0 || eb >= b.ay || (kb && eb1 == eb0)) continue;
 #pragma unroll
-        for (int ka = 0; ka < 2; ka++) {
-          int ea = ka ? ea1 : ea0;
-          if (ea < 0 || ea >= b.ax || (ka && ea1 == ea0)) continue;
-          int slot = ea + TX * (eb + TY * ec);
-          int n = (li - 2 * ea) + 3 * (lj - 2 * eb) + 9 * (lk - 2 * ec);
-          acc += s_out[slot * ostride + 3 * n + f];
+          for (int ka = 0; ka < 2; ka++) {
+            const int ea = ka ? ea1 : ea0;
+            if (ea < 0 || ea >= b.ax || (ka && ea1 == ea0)) continue;
+            const int slot = ea + TX * (eb + TY * ec);
+            const int n = (li - 2 * ea) + 3 * (lj - 2 * eb) + 9 * (lk - 2 * ec);
+            acc += s_out[slot * ostride + 3 * n + f];
+          }
         }
       }
+      const size_t g = base + col;
+      if (A.bc && is_dirichlet(A.dir, b.n0x + li, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, f)) {
+        const bool own = (li > 0 || !lo_x) && (lj > 0 || !lo_y) && (lk > 0 || !lo_z);
+        if (own) A.y[g] = rowmode == 0 ? A.x[g] : (rowmode == 1 ? (T)0 : (T)1);
+        continue;
+      }
+      const bool shared = row_shared || (li == 0 && lo_x) || (li == nax - 1 && hi_x);
+      if (shared) atomicAdd(A.y + g, acc);
+      else A.y[g] = s_y[row * ROWLEN + col] + acc;
     }
-    int ix = b.n0x + li, iy = b.n0y + lj, iz = b.n0z + lk;
-    size_t g = 3 * ((size_t)ix + (size_t)A.gx * ((size_t)iy + (size_t)A.gy * (size_t)iz)) + f;
-    if (A.bc && is_dirichlet(A.dir, ix, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, f)) {
-      bool own = (li > 0 || !lo_x) && (lj > 0 || !lo_y) && (lk > 0 || !lo_z);
-      if (own) A.y[g] = rowmode == 0 ? A.x[g] : (rowmode == 1 ? (T)0 : (T)1);
-      continue;
-    }
-    bool shared = (li == 0 && lo_x) || (li == nax - 1 && hi_x) || (lj == 0 && lo_y) || (lj == nay - 1 && hi_y) ||
-                  (lk == 0 && lo_z) || (lk == naz - 1 && hi_z);
-    if (shared) atomicAdd(A.y + g, acc);
-    else A.y[g] += acc;
   }
 }
 

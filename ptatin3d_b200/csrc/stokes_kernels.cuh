@@ -163,7 +163,8 @@ template <typename T, int NW> struct AffineSmem {
   using BK = Brick<NW>;
   static constexpr int KS = 36; // J^{-1} (9) + eta*w*detJ (27)
   static constexpr int OX = 0;
-  static constexpr int OK = align16(3 * BK::NN, sizeof(T));
+  static constexpr int OY = OX + align16(3 * BK::NN, sizeof(T));
+  static constexpr int OK = OY + align16(3 * BK::NN, sizeof(T));
   static constexpr int OO = OK + align16(BK::NE * KS, sizeof(T));
   static constexpr int TOTAL = OO + BK::NE * 81;
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
@@ -176,10 +177,12 @@ __global__ void __launch_bounds__(32 * NW) a11_affine_kernel(TileArgs<T> A)
   using SM = AffineSmem<T, NW>;
   extern __shared__ __align__(16) unsigned char p3d_smem[];
   T *sm = reinterpret_cast<T *>(p3d_smem);
-  T *s_x = sm + SM::OX, *s_k = sm + SM::OK, *s_out = sm + SM::OO;
+  T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_k = sm + SM::OK, *s_out = sm + SM::OO;
   const BrickPos b = brick_pos<T, NW>(A);
-  load_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
-  copy_vec(A.kdat + (size_t)blockIdx.x * BK::NE * SM::KS, s_k, BK::NE * SM::KS);
+  stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
+  stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * SM::KS, s_k, BK::NE * SM::KS);
+  stage_nodes<T, NW>(A, b, A.y, s_y, false);
+  cp_async_wait_all();
   __syncthreads();
 
   const LaneMap L = lane_map();
@@ -212,7 +215,7 @@ __global__ void __launch_bounds__(32 * NW) a11_affine_kernel(TileArgs<T> A)
     for (int n = 0; n < 27; n++) s_out[L.slot * 81 + 3 * n + L.f] = r[n];
   }
   __syncthreads();
-  gather_store<T, NW>(A, b, s_out, 81, 0);
+  gather_store<T, NW>(A, b, s_out, 81, s_y, 0);
 }
 
 // ------------------------------------------------------- general geometry
@@ -221,7 +224,8 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSme
   static constexpr bool NEEDX = DA11 || DA21;
   static constexpr int GQ = (DA12 || DA21) ? 14 : 10;
   static constexpr int OX = 0;
-  static constexpr int OC = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OC = OY + align16(3 * BK::NN, sizeof(T));
   static constexpr int OK = OC + align16(3 * BK::NN, sizeof(T));
   static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
   static constexpr int TOTAL = OG + BK::NE * 27 * GQ;
@@ -238,11 +242,13 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
   constexpr bool NEEDY = DA11 || DA12;
   extern __shared__ __align__(16) unsigned char p3d_smem[];
   T *sm = reinterpret_cast<T *>(p3d_smem);
-  T *s_x = sm + SM::OX, *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
+  T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
   const BrickPos b = brick_pos<T, NW>(A);
-  if (SM::NEEDX) load_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
-  load_nodes<T, NW>(A, b, A.coords, s_c, false);
-  copy_vec(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  if (SM::NEEDX) stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
+  stage_nodes<T, NW>(A, b, A.coords, s_c, false);
+  stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  if (NEEDY) stage_nodes<T, NW>(A, b, A.y, s_y, false);
+  cp_async_wait_all();
   __syncthreads();
 
   const LaneMap L = lane_map();
@@ -310,7 +316,7 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
       for (int n = 0; n < 27; n++) g[3 * n + L.f] = r[n];
     }
     __syncthreads();
-    gather_store<T, NW>(A, b, s_g, 27 * GQ, DA11 ? 0 : 1);
+    gather_store<T, NW>(A, b, s_g, 27 * GQ, s_y, DA11 ? 0 : 1);
   }
 }
 
@@ -326,10 +332,12 @@ __global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
   constexpr int GQ = SM::GQ;
   extern __shared__ __align__(16) unsigned char p3d_smem[];
   T *sm = reinterpret_cast<T *>(p3d_smem);
-  T *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
+  T *s_y = sm + SM::OY, *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
   const BrickPos b = brick_pos<T, NW>(A);
-  load_nodes<T, NW>(A, b, A.coords, s_c, false);
-  copy_vec(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  stage_nodes<T, NW>(A, b, A.coords, s_c, false);
+  stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  stage_nodes<T, NW>(A, b, A.y, s_y, false);
+  cp_async_wait_all();
   __syncthreads();
   const LaneMap L = lane_map();
   const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
@@ -364,7 +372,7 @@ __global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
     for (int n = 0; n < 27; n++) g[3 * n + L.f] = dg[n];
   }
   __syncthreads();
-  gather_store<T, NW>(A, b, s_g, 27 * GQ, 2);
+  gather_store<T, NW>(A, b, s_g, 27 * GQ, s_y, 2);
 }
 
 // ---------------------------------------------------------------- setup ---
