@@ -124,6 +124,63 @@ int p3d_a11_apply_host(p3d_op *op, const double *x_host, double *y_host);
 int p3d_mg_prolong(int prec, int cnx, int cny, int cnz, int ndof, const void *xc, void *xf, void *stream);
 int p3d_mg_restrict(int prec, int cnx, int cny, int cnz, int ndof, const void *xf, void *xc, void *stream);
 
+/* ------------------------------------------------------ Stokes solve --- */
+/* Device-resident solve of the Q2-P1disc Stokes system on one whole mesh:
+ * outer FGMRES (FP64 residual and orthogonalisation) right-preconditioned by
+ * the block upper-triangular factorisation [A11 A12; 0 S]^{-1}, S the
+ * viscosity-scaled pressure mass matrix (exact 4x4 block inverse per element),
+ * A11^{-1} by one geometric-multigrid V-cycle: Jacobi-preconditioned
+ * Chebyshev smoothing with the matrix-free A11 on every level above the
+ * coarsest, trilinear node-lattice transfers, and a Galerkin coarse operator
+ * P^T A P inverted densely.  With mg_precision = P3D_PREC_F32 the smoother
+ * applies, transfers and stored coefficients run in FP32 while the outer
+ * Krylov iteration, the Schur update, the Jacobi diagonal and the coarse solve
+ * stay FP64.  Replaces the PETSc solver stack the reference configures in
+ * pTatin3dStokesKSPConfigureFSGMG / pTatin3dCreateStokesOperators
+ * (src/ptatin_driver_linear_ts.c:558-882). */
+typedef struct p3d_solver p3d_solver;
+
+typedef struct p3d_solver_opts {
+  int32_t nlevels;      /* multigrid levels, >= 1 (mesh coarsened by 2 per level)   */
+  int32_t cheb_its;     /* Chebyshev iterations per pre/post smoothing              */
+  double cheb_lo;       /* smoothing interval [cheb_lo*lmax, cheb_hi*lmax]          */
+  double cheb_hi;       /*   (the reference's -esteig 0,0.2,0,1.1)                  */
+  int32_t esteig_its;   /* CG-Lanczos iterations estimating lmax(D^{-1}A)           */
+  int32_t mg_precision; /* P3D_PREC_F64 or P3D_PREC_F32 (mixed precision)           */
+  int32_t restart;      /* FGMRES restart length (<= 38)                            */
+  int32_t max_it;       /* outer iteration limit                                    */
+  double rtol;          /* ||r_k|| <= max(rtol*||r_0||, atol)                       */
+  double atol;
+  int32_t use_graph;    /* capture the preconditioner in a CUDA graph               */
+  int32_t verbose;
+} p3d_solver_opts;
+
+typedef struct p3d_solve_stats {
+  int32_t iterations;   /* outer FGMRES iterations                                  */
+  int32_t converged;
+  double r0, rfinal;    /* unpreconditioned residual 2-norms                        */
+  double setup_ms, solve_ms;
+  double lmax_fine;     /* estimated lmax(D^{-1}A) on the finest level              */
+  int32_t coarse_dofs;
+} p3d_solve_stats;
+
+int p3d_solver_default_opts(p3d_solver_opts *opts);
+/* mesh: a whole mesh (p3d_mesh_desc_whole); mx,my,mz divisible by 2^(nlevels-1). */
+int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, int device, p3d_solver **solver);
+/* Device FP64 arrays: coords 3*nn, eta 27*nel.  Builds the hierarchy, the
+ * operators, smoother bounds, the coarse inverse and the Schur blocks. */
+int p3d_solver_setup(p3d_solver *s, const double *coords_dev, const double *eta_dev);
+/* Right-hand side from a Gauss-point density field and gravity vector
+ * (Dirichlet rows zero); or set b directly (device arrays). */
+int p3d_solver_set_rhs_body_force(p3d_solver *s, const double *rho_dev, double gx, double gy, double gz);
+int p3d_solver_set_rhs(p3d_solver *s, const double *bu_dev, const double *bp_dev);
+/* Solve; u (3*nn) and p (4*nel) are device FP64 arrays holding the initial
+ * guess on entry and the solution on return. */
+int p3d_solver_solve(p3d_solver *s, double *u_dev, double *p_dev, p3d_solve_stats *stats);
+/* One application of the block preconditioner (testing / external Krylov). */
+int p3d_solver_apply_pc(p3d_solver *s, const double *ru, const double *rp, double *zu, double *zp);
+int p3d_solver_destroy(p3d_solver *s);
+
 /* -------------------------------------------------------- diagnostics --- */
 /* Last error message of the calling thread (static storage, never NULL). */
 const char *p3d_last_error(void);

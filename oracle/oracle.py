@@ -181,3 +181,41 @@ def get_diagonal(raw_diag, mask):
     d = raw_diag()
     d[mask.astype(bool)] = 1.0
     return d
+
+
+# ------------------------------------------------------ dense Stokes solve ---
+def body_force(R: Restatement, dims, coords, rho, g=(0.0, 0.0, -1.0)):
+    R.L.o_body_force.argtypes = [C.c_int] * 3 + [_dp, _dp, C.c_double, C.c_double, C.c_double, _dp]
+    bu = np.zeros(coords.size)
+    R.L.o_body_force(*dims, _p(np.ascontiguousarray(coords, dtype=np.float64)),
+                     _p(np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)), *map(float, g), _p(bu))
+    return bu
+
+
+def stokes_dense(R: Restatement, dims, coords, eta, mask):
+    """Assemble [A11 A12; A21 0] with the MatMult boundary convention by probing
+    the oracle operators column by column (small meshes only)."""
+    nu = coords.size
+    nel = dims[0] * dims[1] * dims[2]
+    npr = 4 * nel
+    e = np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)
+    m = mask.astype(bool)
+    K = np.zeros((nu + npr, nu + npr))
+    for j in range(nu):
+        x = np.zeros(nu)
+        x[j] = 1.0
+        K[:nu, j] = matmult_a11(lambda v: R.a11_raw(dims, coords, e, v), x, mask)
+        K[nu:, j] = matmult_a21(lambda v: R.a21_raw(dims, coords, v), x, mask)
+    for j in range(npr):
+        p = np.zeros(npr)
+        p[j] = 1.0
+        K[:nu, nu + j] = matmult_a12(lambda v: R.a12_raw(dims, coords, v), p, mask)
+    return K
+
+
+def stokes_dense_solve(R: Restatement, dims, coords, eta, mask, bu, bp=None):
+    K = stokes_dense(R, dims, coords, eta, mask)
+    nel = dims[0] * dims[1] * dims[2]
+    b = np.concatenate([bu, np.zeros(4 * nel) if bp is None else bp])
+    x = np.linalg.solve(K, b)
+    return x[:coords.size], x[coords.size:]

@@ -463,3 +463,30 @@ void o_bc_insert_value(long n, const uint8_t *mask, double value, double *y)
   for (long k = 0; k < n; k++)
     if (mask[k]) y[k] = value;
 }
+
+/* ------------------------------------------------------- body force --- */
+/* bu_(n,l) += sum_q w detJ N_n(q) rho_q g_l  (the body-force term of the
+ * velocity residual, src/stokes_form_function.c:99-243) */
+void o_body_force(int mx, int my, int mz, const double *coords, const double *rho, double gx, double gy, double gz,
+                  double *bu)
+{
+  o_mesh m = {mx, my, mz};
+  o_tables();
+  long nel = (long)mx * my * mz;
+  double g[3] = {gx, gy, gz};
+  for (long e = 0; e < nel; e++) {
+    long nid[27];
+    double elx[81], iJ[27][3][3], detJ[27];
+    o_element_nodes(&m, e, nid);
+    o_gather3(coords, nid, elx);
+    o_geometry(elx, iJ, detJ);
+    for (int q = 0; q < 27; q++) {
+      int qi = q % 3, qj = (q / 3) % 3, qk = q / 9;
+      double s = WQ[q] * detJ[q] * rho[27 * e + q];
+      for (int n = 0; n < 27; n++) {
+        double N = BAS[qi][n % 3] * BAS[qj][(n / 3) % 3] * BAS[qk][n / 9];
+        for (int l = 0; l < 3; l++) bu[3 * nid[n] + l] += s * N * g[l];
+      }
+    }
+  }
+}

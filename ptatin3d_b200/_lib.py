@@ -38,9 +38,30 @@ class MeshDesc(C.Structure):
                 ("dirichlet", C.c_uint32), ("global_faces", C.c_uint32)]
 
 
+class SolverOpts(C.Structure):
+    _fields_ = [("nlevels", C.c_int32), ("cheb_its", C.c_int32), ("cheb_lo", C.c_double), ("cheb_hi", C.c_double),
+                ("esteig_its", C.c_int32), ("mg_precision", C.c_int32), ("restart", C.c_int32),
+                ("max_it", C.c_int32), ("rtol", C.c_double), ("atol", C.c_double), ("use_graph", C.c_int32),
+                ("verbose", C.c_int32)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("r0", C.c_double), ("rfinal", C.c_double),
+                ("setup_ms", C.c_double), ("solve_ms", C.c_double), ("lmax_fine", C.c_double),
+                ("coarse_dofs", C.c_int32)]
+
+
 _lib = None
 
 _SIGS = {
+    "p3d_solver_default_opts": ([C.POINTER(SolverOpts)], C.c_int),
+    "p3d_solver_create": ([C.POINTER(MeshDesc), C.POINTER(SolverOpts), C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "p3d_solver_setup": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_solver_set_rhs_body_force": ([C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
+    "p3d_solver_set_rhs": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_solver_solve": ([C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveStats)], C.c_int),
+    "p3d_solver_apply_pc": ([C.c_void_p] * 5, C.c_int),
+    "p3d_solver_destroy": ([C.c_void_p], C.c_int),
     "p3d_last_error": ([], C.c_char_p),
     "p3d_kernel_launch_count": ([], C.c_int64),
     "p3d_version": ([], C.c_char_p),

@@ -134,7 +134,7 @@ template <typename T> int launch_diag(p3d_op *op, T *d, cudaStream_t st)
   TileArgs<T> a = tile_args<T>(op, NW_GEN);
   a.y = d; a.kdat = reinterpret_cast<const T *>(op->kgen); a.diag = 1;
   auto kern = diag_general_kernel<T, NW_GEN>;
-  size_t smem = GeneralSmem<T, NW_GEN, true, false, false>::BYTES;
+  size_t smem = DiagSmem<T, NW_GEN>::BYTES;
   int rc = prep_kernel(kern, smem);
   if (rc) return rc;
   if (nbricks_t(a) == 0) return P3D_OK;

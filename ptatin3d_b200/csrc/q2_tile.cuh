@@ -156,6 +156,7 @@ struct BrickPos {
   int ax, ay, az;     // elements actually present
   int n0x, n0y, n0z;  // lattice index of the brick's first node
   int tx, ty, tz;
+  bool on_face; // brick touches a face of the local block
 };
 template <typename T, int NW> __device__ __forceinline__ BrickPos brick_pos(const TileArgs<T> &A)
 {
@@ -167,6 +168,8 @@ template <typename T, int NW> __device__ __forceinline__ BrickPos brick_pos(cons
   b.e0x = b.tx * TX; b.e0y = b.ty * TY; b.e0z = b.tz * NW;
   b.ax = min(TX, A.mx - b.e0x); b.ay = min(TY, A.my - b.e0y); b.az = min(NW, A.mz - b.e0z);
   b.n0x = A.ox + 2 * b.e0x; b.n0y = A.oy + 2 * b.e0y; b.n0z = A.oz + 2 * b.e0z;
+  b.on_face = b.e0x == 0 || b.e0y == 0 || b.e0z == 0 || b.e0x + b.ax == A.mx || b.e0y + b.ay == A.my ||
+              b.e0z + b.az == A.mz;
   return b;
 }
 
@@ -189,8 +192,9 @@ __device__ __forceinline__ void cp_async_wait_all()
 }
 
 // Stage a 3-component node field of the brick, row by row (a row = 2TX+1
-// nodes along x = 33 contiguous values in global memory), one warp per row.
-// mask: zero the Dirichlet entries (MatMult column convention).
+// nodes along x = 33 contiguous values in global memory), one warp per row,
+// lane l copying columns l and l+32.  mask: zero the Dirichlet entries
+// (MatMult column convention); only bricks on a Dirichlet face test entries.
 template <typename T, int NW>
 __device__ __forceinline__ void stage_nodes(const TileArgs<T> &A, const BrickPos &b, const T *__restrict__ src, T *s,
                                             bool mask)
@@ -199,19 +203,23 @@ __device__ __forceinline__ void stage_nodes(const TileArgs<T> &A, const BrickPos
   constexpr int ROWLEN = 3 * BK::NX, NROWS = BK::NY * BK::NZ;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nax = 2 * b.ax + 1, nay = 2 * b.ay + 1, naz = 2 * b.az + 1;
+  const int li0 = lane / 3, c0 = lane - 3 * li0; // column `lane`
+  const bool ok0 = li0 < nax, ok1 = lane == 0 && 10 < nax; // column 32 = node 10, comp 2
+  const bool domask = mask && A.dir && b.on_face;
   const int exn = A.ox + 2 * A.mx, eyn = A.oy + 2 * A.my, ezn = A.oz + 2 * A.mz;
   for (int row = warp; row < NROWS; row += NW) {
     const int lj = row % BK::NY, lk = row / BK::NY;
+    if (lj >= nay || lk >= naz) continue;
     const int iy = b.n0y + lj, iz = b.n0z + lk;
-    const bool rowok = lj < nay && lk < naz;
-    const size_t base = 3 * ((size_t)b.n0x + (size_t)A.gx * ((size_t)iy + (size_t)A.gy * (size_t)iz));
-    for (int col = lane; col < ROWLEN; col += 32) {
-      const int li = col / 3, comp = col - 3 * li;
-      bool ok = rowok && li < nax;
-      if (ok && mask) ok = !is_dirichlet(A.dir, b.n0x + li, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, comp);
-      cp_async<sizeof(T)>(s + row * ROWLEN + col, ok ? (const void *)(src + base + col) : (const void *)src,
-                          ok ? (int)sizeof(T) : 0);
+    const T *gr = src + 3 * ((size_t)b.n0x + (size_t)A.gx * ((size_t)iy + (size_t)A.gy * (size_t)iz));
+    T *sr = s + row * ROWLEN;
+    bool m0 = ok0, m1 = ok1;
+    if (domask) {
+      m0 = m0 && !is_dirichlet(A.dir, b.n0x + li0, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, c0);
+      m1 = m1 && !is_dirichlet(A.dir, b.n0x + 10, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, 2);
     }
+    cp_async<sizeof(T)>(sr + lane, m0 ? (const void *)(gr + lane) : (const void *)src, m0 ? (int)sizeof(T) : 0);
+    if (lane == 0) cp_async<sizeof(T)>(sr + 32, m1 ? (const void *)(gr + 32) : (const void *)src, m1 ? (int)sizeof(T) : 0);
   }
 }
 
@@ -225,15 +233,35 @@ template <typename T> __device__ __forceinline__ void stage_block(const T *__res
     cp_async<sizeof(T)>(s + i, g + i, (int)sizeof(T));
 }
 
-// Sum the element contributions of every brick node and add them into y.
-// s_out[slot*ostride + 3*n + f]: element slot's contribution to its local node n, comp f.
-// s_y: the brick's y values staged at kernel start (y += acc without a global load).
-// Nodes on brick faces shared with a neighbouring brick are added with atomicAdd
-// (fire-and-forget reductions), every other node with a plain store.
+// Add the lane's 27 nodal contributions r[] into the brick's node tile s_acc
+// (zeroed by the caller).  Elements whose (a,b,c) parities agree share no node,
+// so the 8 parity classes take turns and every update is a plain shared-memory
+// read-modify-write.  Must be reached by every thread of the CTA.
+template <typename T, int NW>
+__device__ __forceinline__ void accumulate_phases(T *s_acc, const T r[27], int a, int bb, int c, int f, bool doit)
+{
+  using BK = Brick<NW>;
+  const int par = (a & 1) | ((bb & 1) << 1) | ((c & 1) << 2);
+  T *base = s_acc + 3 * (2 * a + BK::NX * (2 * bb + BK::NY * 2 * c)) + f;
+  for (int ph = 0; ph < 8; ph++) {
+    if (doit && ph == par) {
+#pragma unroll
+      for (int n = 0; n < 27; n++) {
+        const int off = 3 * ((n % 3) + BK::NX * (((n / 3) % 3) + BK::NY * (n / 9)));
+        base[off] += r[n];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Write the accumulated brick tile into y: y = y_staged + acc for nodes no
+// other CTA touches, atomicAdd (fire-and-forget reduction) for nodes on
+// brick faces shared with a neighbouring brick, Dirichlet rows by the owner.
 // rowmode: 0 -> Dirichlet rows get x (A11 / full operator), 1 -> 0 (A12), 2 -> 1 (diagonal)
 template <typename T, int NW>
-__device__ __forceinline__ void gather_store(const TileArgs<T> &A, const BrickPos &b, const T *s_out, int ostride,
-                                             const T *s_y, int rowmode)
+__device__ __forceinline__ void write_tile(const TileArgs<T> &A, const BrickPos &b, const T *s_acc, const T *s_y,
+                                           int rowmode)
 {
   using BK = Brick<NW>;
   constexpr int ROWLEN = 3 * BK::NX, NROWS = BK::NY * BK::NZ;
@@ -242,45 +270,32 @@ __device__ __forceinline__ void gather_store(const TileArgs<T> &A, const BrickPo
   const int exn = A.ox + 2 * A.mx, eyn = A.oy + 2 * A.my, ezn = A.oz + 2 * A.mz;
   const bool lo_x = b.tx > 0, lo_y = b.ty > 0, lo_z = b.tz > 0;
   const bool hi_x = b.e0x + b.ax < A.mx, hi_y = b.e0y + b.ay < A.my, hi_z = b.e0z + b.az < A.mz;
+  const bool dobc = A.bc && A.dir && b.on_face;
+  // the (at most two) columns of this lane
+  const int li0 = lane / 3, f0 = lane - 3 * li0;
+  const bool ok0 = li0 < nax, ok1 = lane == 0 && 10 < nax;
+  const bool xs0 = (li0 == 0 && lo_x) || (li0 == nax - 1 && hi_x), xs1 = (10 == nax - 1 && hi_x);
+  const bool own0 = li0 > 0 || !lo_x, own1 = true;
   for (int row = warp; row < NROWS; row += NW) {
     const int lj = row % BK::NY, lk = row / BK::NY;
     if (lj >= nay || lk >= naz) continue;
     const int iy = b.n0y + lj, iz = b.n0z + lk;
     const size_t base = 3 * ((size_t)b.n0x + (size_t)A.gx * ((size_t)iy + (size_t)A.gy * (size_t)iz));
-    const int eb0 = (lj - 1) >> 1, eb1 = lj >> 1, ec0 = (lk - 1) >> 1, ec1 = lk >> 1;
-    const bool row_shared = (lj == 0 && lo_y) || (lj == nay - 1 && hi_y) || (lk == 0 && lo_z) || (lk == naz - 1 && hi_z);
-    for (int col = lane; col < ROWLEN; col += 32) {
-      const int li = col / 3, f = col - 3 * li;
-      if (li >= nax) continue;
-      const int ea0 = (li - 1) >> 1, ea1 = li >> 1;
-      T acc = (T)0;
+    const bool rs = (lj == 0 && lo_y) || (lj == nay - 1 && hi_y) || (lk == 0 && lo_z) || (lk == naz - 1 && hi_z);
+    const bool rown = (lj > 0 || !lo_y) && (lk > 0 || !lo_z);
 #pragma unroll
-      for (int kc = 0; kc < 2; kc++) {
-        const int ec = kc ? ec1 : ec0;
-        if (ec < 0 || ec >= b.az || (kc && ec1 == ec0)) continue;
-#pragma unroll
-        for (int kb = 0; kb < 2; kb++) {
-          const int eb = kb ? eb1 : eb0;
-          if (eb < 0 || eb >= b.ay || (kb && eb1 == eb0)) continue;
-#pragma unroll
-          for (int ka = 0; ka < 2; ka++) {
-            const int ea = ka ? ea1 : ea0;
-            if (ea < 0 || ea >= b.ax || (ka && ea1 == ea0)) continue;
-            const int slot = ea + TX * (eb + TY * ec);
-            const int n = (li - 2 * ea) + 3 * (lj - 2 * eb) + 9 * (lk - 2 * ec);
-            acc += s_out[slot * ostride + 3 * n + f];
-          }
-        }
-      }
+    for (int k = 0; k < 2; k++) {
+      const bool ok = k ? ok1 : ok0;
+      if (!ok) continue;
+      const int col = k ? 32 : lane, li = k ? 10 : li0, f = k ? 2 : f0;
       const size_t g = base + col;
-      if (A.bc && is_dirichlet(A.dir, b.n0x + li, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, f)) {
-        const bool own = (li > 0 || !lo_x) && (lj > 0 || !lo_y) && (lk > 0 || !lo_z);
-        if (own) A.y[g] = rowmode == 0 ? A.x[g] : (rowmode == 1 ? (T)0 : (T)1);
+      if (dobc && is_dirichlet(A.dir, b.n0x + li, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, f)) {
+        if (rown && (k ? own1 : own0)) A.y[g] = rowmode == 0 ? A.x[g] : (rowmode == 1 ? (T)0 : (T)1);
         continue;
       }
-      const bool shared = row_shared || (li == 0 && lo_x) || (li == nax - 1 && hi_x);
-      if (shared) atomicAdd(A.y + g, acc);
-      else A.y[g] = s_y[row * ROWLEN + col] + acc;
+      const T v = s_acc[row * ROWLEN + col];
+      if (rs || (k ? xs1 : xs0)) atomicAdd(A.y + g, v);
+      else A.y[g] = s_y[row * ROWLEN + col] + v;
     }
   }
 }

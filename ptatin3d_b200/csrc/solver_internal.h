@@ -1,0 +1,38 @@
+// Internal declarations of the solver translation units (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#define P3D_MDOT_MAX 40     // max vectors in one fused multi-dot (FGMRES restart + 1)
+#define P3D_MDOT_BLOCKS 592 // 4 x 148 SMs
+
+namespace p3d {
+
+// vec_kernels.cu
+template <typename A, typename B> void v_convert(size_t n, const A *x, B *y, cudaStream_t s);
+template <typename T> void v_axpby(size_t n, T a, const T *x, T b, T *y, cudaStream_t s);
+template <typename T> void v_scale(size_t n, T a, T *y, cudaStream_t s);
+template <typename T> void v_jacobi(size_t n, const double *dinv, const T *r, T *z, cudaStream_t s);
+template <typename T> void v_cheb_init(size_t n, const double *dinv, const T *r, T inv_theta, T *d, cudaStream_t s);
+template <typename T>
+void v_cheb_step(size_t n, const double *dinv, T *x, T *r, const T *Ad, T *d, T c1, T c2, cudaStream_t s);
+template <typename T> void v_residual(size_t n, const T *b, const T *Ax, T *r, cudaStream_t s);
+template <typename T> void v_mask(int nx, int ny, int nz, uint32_t dir, T *v, cudaStream_t s);
+template <typename T>
+void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s);
+template <typename T> void v_maxpy(size_t n, int k, const double *h, const T *const *V_dev, T *w, double sign, cudaStream_t s);
+void v_block4(size_t nel, const double *B, const double *x, double *y, double alpha, cudaStream_t s);
+void v_dense_mv(int n, const double *M, const double *x, double *y, cudaStream_t s);
+
+// setup_kernels.cu (whole-mesh lattices, FP64)
+void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *eta, double *Binv, cudaStream_t s);
+void s_body_force(int mx, int my, int mz, const double *coords, const double *rho, double g[3], double *bu, cudaStream_t s);
+void s_restrict_eta(int mxc, int myc, int mzc, const double *eta_f, double *eta_c, cudaStream_t s);
+void s_inject_coords(int cnx, int cny, int cnz, const double *cf, double *cc, cudaStream_t s);
+
+// mg_transfer.cu
+template <typename T> int mg_prolong(int cnx, int cny, int cnz, int ndof, const T *xc, T *xf, cudaStream_t st);
+template <typename T> int mg_restrict(int cnx, int cny, int cnz, int ndof, const T *xf, T *xc, cudaStream_t st);
+
+} // namespace p3d

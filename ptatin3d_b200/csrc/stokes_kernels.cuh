@@ -165,8 +165,8 @@ template <typename T, int NW> struct AffineSmem {
   static constexpr int OX = 0;
   static constexpr int OY = OX + align16(3 * BK::NN, sizeof(T));
   static constexpr int OK = OY + align16(3 * BK::NN, sizeof(T));
-  static constexpr int OO = OK + align16(BK::NE * KS, sizeof(T));
-  static constexpr int TOTAL = OO + BK::NE * 81;
+  static constexpr int OA = OK + align16(BK::NE * KS, sizeof(T)); // node-tile accumulator
+  static constexpr int TOTAL = OA + 3 * BK::NN;
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
 };
 
@@ -177,15 +177,17 @@ __global__ void __launch_bounds__(32 * NW) a11_affine_kernel(TileArgs<T> A)
   using SM = AffineSmem<T, NW>;
   extern __shared__ __align__(16) unsigned char p3d_smem[];
   T *sm = reinterpret_cast<T *>(p3d_smem);
-  T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_k = sm + SM::OK, *s_out = sm + SM::OO;
+  T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_k = sm + SM::OK, *s_acc = sm + SM::OA;
   const BrickPos b = brick_pos<T, NW>(A);
   stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
   stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * SM::KS, s_k, BK::NE * SM::KS);
   stage_nodes<T, NW>(A, b, A.y, s_y, false);
+  for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
   cp_async_wait_all();
   __syncthreads();
 
   const LaneMap L = lane_map();
+  const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
   const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
   const T *K = s_k + L.slot * SM::KS;
   T Jr[9];
@@ -210,25 +212,28 @@ __global__ void __launch_bounds__(32 * NW) a11_affine_kernel(TileArgs<T> A)
         P3D_SCATTER(r, i, j, k, ro0, ro1, ro2)
       }
   interp27T(r);
-  if (L.active) {
-#pragma unroll
-    for (int n = 0; n < 27; n++) s_out[L.slot * 81 + 3 * n + L.f] = r[n];
-  }
-  __syncthreads();
-  gather_store<T, NW>(A, b, s_out, 81, s_y, 0);
+  accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
+  write_tile<T, NW>(A, b, s_acc, s_y, 0);
 }
 
 // ------------------------------------------------------- general geometry
+// Geometry is built one Gauss-point plane (9 points, fixed k) at a time: the
+// interpolated coordinates of each element stay in shared memory and every
+// lane inverts 3 of the plane's 9 Jacobians, so the per-element geometry table
+// holds 9 points instead of 27 (3x less shared memory, more CTAs per SM).
 template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSmem {
   using BK = Brick<NW>;
   static constexpr bool NEEDX = DA11 || DA21;
+  static constexpr bool NEEDY = DA11 || DA12;
   static constexpr int GQ = (DA12 || DA21) ? 14 : 10;
+  static constexpr int CT = align16(3 * BK::NN, sizeof(T));  // coordinate tile / accumulator
+  static constexpr int CQ = align16(BK::NE * 81, sizeof(T)); // Gauss-point coordinates
   static constexpr int OX = 0;
   static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
-  static constexpr int OC = OY + align16(3 * BK::NN, sizeof(T));
-  static constexpr int OK = OC + align16(3 * BK::NN, sizeof(T));
+  static constexpr int OC = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OK = OC + (CT > CQ ? CT : CQ);
   static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
-  static constexpr int TOTAL = OG + BK::NE * 27 * GQ;
+  static constexpr int TOTAL = OG + BK::NE * 9 * GQ;
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
 };
 
@@ -239,7 +244,7 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
   using SM = GeneralSmem<T, NW, DA11, DA12, DA21>;
   constexpr int GQ = SM::GQ;
   constexpr bool PB = DA12 || DA21;
-  constexpr bool NEEDY = DA11 || DA12;
+  constexpr bool NEEDY = SM::NEEDY;
   extern __shared__ __align__(16) unsigned char p3d_smem[];
   T *sm = reinterpret_cast<T *>(p3d_smem);
   T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
@@ -253,8 +258,30 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
 
   const LaneMap L = lane_map();
   const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
-  T *g = s_g + L.slot * 27 * GQ;
-  geometry_pass<T, NW, GQ, PB>(s_c, s_k + L.slot * 27, g, L, valid);
+  // coordinates at the Gauss points (lane f: coordinate f) and the pressure-basis scaling
+  T avg = (T)0, rL = (T)1;
+  {
+    T xq[27];
+#pragma unroll
+    for (int n = 0; n < 27; n++) xq[n] = s_c[3 * brick_node<NW>(L.a, L.b, L.c, n) + L.f];
+    if (PB) {
+#pragma unroll
+      for (int n = 0; n < 27; n++) avg += xq[n];
+      avg *= cst<T>(1.0 / 27.0);
+      T Lf = (L.f == 0) ? xq[14] - xq[12] : ((L.f == 1) ? xq[16] - xq[10] : xq[22] - xq[4]);
+      rL = valid ? (T)1 / Lf : (T)0;
+    }
+    interp27(xq);
+    __syncthreads(); // every warp has read the coordinate tile: reuse it for the Gauss-point coordinates
+    if (L.active) {
+#pragma unroll
+      for (int n = 0; n < 27; n++) s_c[L.slot * 81 + L.f * 27 + n] = xq[n];
+    }
+  }
+  __syncwarp();
+  const T *X = s_c + L.slot * 81 + L.f * 27;
+  const T *eta_e = s_k + L.slot * 27;
+  T *g = s_g + L.slot * 9 * GQ;
 
   const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
   const int r0 = 3 * L.f, r1 = 3 * ((L.f + 1) % 3), r2 = 3 * ((L.f + 2) % 3);
@@ -267,12 +294,54 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
   if (DA12 && valid) { pe0 = A.p[4 * eg]; pe1 = A.p[4 * eg + 1]; pe2 = A.p[4 * eg + 2]; pe3 = A.p[4 * eg + 3]; }
   T ap0 = 0, ap1 = 0, ap2 = 0, ap3 = 0;
 #pragma unroll
-  for (int k = 0; k < 3; k++)
+  for (int k = 0; k < 3; k++) {
+    // ---- plane k: Jacobian columns (lane f owns column f), then 3 inversions per lane
+    {
+      T xp[27];
+#pragma unroll
+      for (int n = 0; n < 27; n++) xp[n] = X[n];
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          const int q9 = i + 3 * j;
+          T d0 = dcol(i, xp[3 * j + 9 * k], xp[1 + 3 * j + 9 * k], xp[2 + 3 * j + 9 * k]);
+          T d1 = dcol(j, xp[i + 9 * k], xp[i + 3 + 9 * k], xp[i + 6 + 9 * k]);
+          T d2 = dcol(k, xp[i + 3 * j], xp[i + 3 * j + 9], xp[i + 3 * j + 18]);
+          if (!valid) { d0 = (T)(L.f == 0); d1 = (T)(L.f == 1); d2 = (T)(L.f == 2); }
+          if (L.active) {
+            g[q9 * GQ + 0 + L.f] = d0;
+            g[q9 * GQ + 3 + L.f] = d1;
+            g[q9 * GQ + 6 + L.f] = d2;
+            if (PB) g[q9 * GQ + 11 + L.f] = (xp[q9 + 9 * k] - avg) * rL;
+          }
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      const int q9 = 3 * t + L.f; // i = f, j = t
+      T *G = g + q9 * GQ;
+      T M[9], Mi[9];
+#pragma unroll
+      for (int rr = 0; rr < 9; rr++) M[rr] = G[rr];
+      T det = inv3(M, Mi);
+      T w = (T)(w1d(L.f) * w1d(t) * w1d(k)) * det;
+      T eta = valid ? eta_e[q9 + 9 * k] : (T)0;
+      if (L.active) {
+#pragma unroll
+        for (int rr = 0; rr < 9; rr++) G[rr] = Mi[rr];
+        G[9] = eta * w;
+        if (GQ > 10) G[10] = valid ? w : (T)0;
+      }
+    }
+    __syncwarp();
+    // ---- the plane's 9 Gauss points
 #pragma unroll
     for (int j = 0; j < 3; j++)
 #pragma unroll
       for (int i = 0; i < 3; i++) {
-        const T *G = g + (i + 3 * j + 9 * k) * GQ;
+        const T *G = g + (i + 3 * j) * GQ;
         T Jr[9];
 #pragma unroll
         for (int d = 0; d < 3; d++) { Jr[d] = G[r0 + d]; Jr[3 + d] = G[r1 + d]; Jr[6 + d] = G[r2 + d]; }
@@ -298,6 +367,8 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
         }
         if (NEEDY) { P3D_SCATTER(r, i, j, k, ro0, ro1, ro2) }
       }
+    __syncwarp(); // the next plane overwrites this element's table
+  }
   if (DA21) {
     // divergence = sum over the element's three lanes
     ap0 += __shfl_sync(0xffffffffu, ap0, src1) + __shfl_sync(0xffffffffu, ap0, src2);
@@ -309,14 +380,13 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
     }
   }
   if (NEEDY) {
-    __syncwarp();
     interp27T(r);
-    if (L.active) {
-#pragma unroll
-      for (int n = 0; n < 27; n++) g[3 * n + L.f] = r[n];
-    }
+    __syncthreads(); // every warp is done with the Gauss-point coordinates: reuse as the accumulator
+    T *s_acc = s_c;
+    for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
     __syncthreads();
-    gather_store<T, NW>(A, b, s_g, 27 * GQ, s_y, DA11 ? 0 : 1);
+    accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
+    write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
   }
 }
 
@@ -324,11 +394,22 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
 __constant__ double c_B[3][3];
 __constant__ double c_D[3][3];
 
+template <typename T, int NW> struct DiagSmem {
+  using BK = Brick<NW>;
+  static constexpr int GQ = 10;
+  static constexpr int OY = 0;
+  static constexpr int OC = OY + align16(3 * BK::NN, sizeof(T));
+  static constexpr int OK = OC + align16(3 * BK::NN, sizeof(T));
+  static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
+  static constexpr int TOTAL = OG + BK::NE * 27 * GQ;
+  static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
+};
+
 template <typename T, int NW>
 __global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
 {
   using BK = Brick<NW>;
-  using SM = GeneralSmem<T, NW, true, false, false>;
+  using SM = DiagSmem<T, NW>;
   constexpr int GQ = SM::GQ;
   extern __shared__ __align__(16) unsigned char p3d_smem[];
   T *sm = reinterpret_cast<T *>(p3d_smem);
@@ -366,13 +447,12 @@ __global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
       dg[n] += ce * (d0 * d0 + d1 * d1 + d2 * d2 + df * df);
     }
   }
-  __syncwarp();
-  if (L.active) {
-#pragma unroll
-    for (int n = 0; n < 27; n++) g[3 * n + L.f] = dg[n];
-  }
   __syncthreads();
-  gather_store<T, NW>(A, b, s_g, 27 * GQ, s_y, 2);
+  T *s_acc = s_c;
+  for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
+  __syncthreads();
+  accumulate_phases<T, NW>(s_acc, dg, L.a, L.b, L.c, L.f, L.active && valid);
+  write_tile<T, NW>(A, b, s_acc, s_y, 2);
 }
 
 // ---------------------------------------------------------------- setup ---

@@ -1,0 +1,740 @@
+// Device-resident Q2-P1disc Stokes solver (see p3d_solver_* in include/p3d_b200.h).
+//
+// Host code here only sequences kernels; every vector lives in HBM.  The
+// structure follows the solver the reference assembles from PETSc objects
+// (src/ptatin_driver_linear_ts.c:558-882 and the options of
+// tests/application/linear/sinker_mf_8x8x8/opts): FGMRES outer iteration,
+// PCFIELDSPLIT Schur "upper" factorisation, PCMG on the velocity block with
+// Chebyshev/Jacobi smoothing, DMDA trilinear transfers and a Galerkin coarse
+// operator.  It is not a translation of PETSc: Chebyshev, Lanczos, FGMRES,
+// Gauss-Jordan are restated from their textbook definitions (Saad,
+// "Iterative Methods for Sparse Linear Systems", Alg. 12.1 (Chebyshev),
+// 6.15/9.6 (FGMRES), 6.17 (Lanczos from CG)).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "p3d_b200.h"
+#include "p3d_internal.h"
+#include "solver_internal.h"
+
+namespace p3d {
+
+struct Level {
+  int m[3] = {0, 0, 0}, n[3] = {0, 0, 0};
+  size_t nv = 0;                 // velocity dofs
+  p3d_op *op64 = nullptr;        // FP64 operator (smoothing in FP64 mode, Galerkin probe, esteig)
+  p3d_op *op32 = nullptr;        // FP32 operator (mixed mode smoothing)
+  double *coords = nullptr, *eta = nullptr;
+  double *dinv = nullptr;        // FP64 inverse diagonal (Dirichlet slots 1)
+  double lmax = 0.0;
+  void *b = nullptr, *x = nullptr, *r = nullptr, *d = nullptr, *t = nullptr; // MG precision work vectors
+};
+
+} // namespace p3d
+
+struct p3d_solver {
+  p3d_mesh_desc mesh;
+  p3d_solver_opts o;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  std::vector<p3d::Level> lv; // lv[0] coarsest ... lv[L-1] finest
+  // coarse solve
+  int nc = 0;
+  double *cinv = nullptr;          // dense inverse of the Galerkin coarse operator
+  double *cb64 = nullptr, *cx64 = nullptr;
+  // Stokes system
+  size_t nu = 0, np = 0, N = 0;
+  double *Binv = nullptr; // Schur block inverses
+  double *bvec = nullptr; // rhs [bu; bp]
+  // FGMRES
+  double *V = nullptr, *Z = nullptr, *w = nullptr;
+  double **Vptr = nullptr; // device array of pointers to V_j
+  double *part = nullptr, *hdev = nullptr;
+  double *hhost = nullptr; // pinned
+  // preconditioner buffers (fixed for graph capture)
+  double *pc_in = nullptr, *pc_out = nullptr, *pc_t = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  bool setup_done = false, rhs_set = false;
+  double setup_ms = 0.0;
+};
+
+namespace p3d {
+
+static double now_ms()
+{
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+#define CK(call)                                                                                                       \
+  do {                                                                                                                 \
+    int rc_ = (call);                                                                                                  \
+    if (rc_) return rc_;                                                                                               \
+  } while (0)
+#define CU(call, what) CK(cuda_check((call), what))
+
+static uint32_t level_dir(const p3d_solver *s) { return s->mesh.dirichlet; }
+
+// y = A11 x on level l in precision T (BC_MATMULT), y overwritten
+template <typename T> static int a11(p3d_solver *s, Level &L, const T *x, T *y)
+{
+  CU(cudaMemsetAsync(y, 0, L.nv * sizeof(T), s->st), "memset");
+  p3d_op *op = sizeof(T) == 8 ? L.op64 : L.op32;
+  return launch_a11<T>(op, x, y, s->st);
+}
+
+// Chebyshev smoothing on level l: x <- x + K steps for A x = b (zero_guess: x = 0 on entry)
+template <typename T> static int smooth(p3d_solver *s, Level &L, const T *b, T *x, bool zero_guess)
+{
+  const size_t n = L.nv;
+  T *r = (T *)L.r, *d = (T *)L.d, *t = (T *)L.t;
+  const double lo = s->o.cheb_lo * L.lmax, hi = s->o.cheb_hi * L.lmax;
+  const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+  if (zero_guess) {
+    CU(cudaMemsetAsync(x, 0, n * sizeof(T), s->st), "memset");
+    CU(cudaMemcpyAsync(r, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s->st), "copy");
+  } else {
+    CK(a11<T>(s, L, x, t));
+    v_residual<T>(n, b, t, r, s->st);
+  }
+  v_cheb_init<T>(n, L.dinv, r, (T)(1.0 / theta), d, s->st);
+  double rho = 1.0 / sigma;
+  const int K = std::max(1, s->o.cheb_its);
+  for (int k = 0; k < K; k++) {
+    if (k == K - 1) {
+      v_axpby<T>(n, (T)1, d, (T)1, x, s->st); // x += d
+      break;
+    }
+    CK(a11<T>(s, L, d, t));
+    double rho_new = 1.0 / (2.0 * sigma - rho);
+    v_cheb_step<T>(n, L.dinv, x, r, t, d, (T)(rho_new * rho), (T)(2.0 * rho_new / delta), s->st);
+    rho = rho_new;
+  }
+  return P3D_OK;
+}
+
+// coarse solve: x = Ac^{-1} b (FP64 dense inverse)
+template <typename T> static int coarse_solve(p3d_solver *s, const T *b, T *x)
+{
+  Level &L = s->lv[0];
+  v_mask<T>(L.n[0], L.n[1], L.n[2], level_dir(s), const_cast<T *>(b), s->st);
+  if (sizeof(T) == 8) {
+    v_dense_mv(s->nc, s->cinv, (const double *)b, (double *)x, s->st);
+  } else {
+    v_convert<float, double>(L.nv, (const float *)b, s->cb64, s->st);
+    v_dense_mv(s->nc, s->cinv, s->cb64, s->cx64, s->st);
+    v_convert<double, float>(L.nv, s->cx64, (float *)x, s->st);
+  }
+  return P3D_OK;
+}
+
+// V-cycle on level l: x = MG(b), x overwritten
+template <typename T> static int vcycle(p3d_solver *s, int l, const T *b, T *x)
+{
+  if (l == 0) return coarse_solve<T>(s, b, x);
+  Level &L = s->lv[l], &C = s->lv[l - 1];
+  const uint32_t dir = level_dir(s);
+  CK(smooth<T>(s, L, b, x, true));
+  T *t = (T *)L.t, *r = (T *)L.r;
+  CK(a11<T>(s, L, x, t));
+  v_residual<T>(L.nv, b, t, r, s->st);
+  v_mask<T>(L.n[0], L.n[1], L.n[2], dir, r, s->st);
+  CK(mg_restrict<T>(C.n[0], C.n[1], C.n[2], 3, r, (T *)C.b, s->st));
+  v_mask<T>(C.n[0], C.n[1], C.n[2], dir, (T *)C.b, s->st);
+  CK(vcycle<T>(s, l - 1, (const T *)C.b, (T *)C.x));
+  CK(mg_prolong<T>(C.n[0], C.n[1], C.n[2], 3, (const T *)C.x, t, s->st));
+  v_mask<T>(L.n[0], L.n[1], L.n[2], dir, t, s->st);
+  v_axpby<T>(L.nv, (T)1, t, (T)1, x, s->st);
+  CK(smooth<T>(s, L, b, x, false));
+  return P3D_OK;
+}
+
+// block upper-triangular preconditioner: zp = S^{-1} rp ; zu = MG(ru - A12 zp)
+static int apply_pc(p3d_solver *s, const double *in, double *out)
+{
+  const double *ru = in, *rp = in + s->nu;
+  double *zu = out, *zp = out + s->nu;
+  Level &F = s->lv.back();
+  v_block4(s->np / 4, s->Binv, rp, zp, 1.0, s->st);
+  double *t = s->pc_t;
+  CU(cudaMemsetAsync(t, 0, s->nu * 8, s->st), "memset");
+  CK((launch_general<double, false, true, false>(F.op64, nullptr, zp, t, nullptr, s->st)));
+  v_axpby<double>(s->nu, 1.0, ru, -1.0, t, s->st); // t = ru - A12 zp
+  if (s->o.mg_precision == P3D_PREC_F64) {
+    CK(vcycle<double>(s, (int)s->lv.size() - 1, t, zu));
+  } else {
+    v_convert<double, float>(s->nu, t, (float *)F.b, s->st);
+    CK(vcycle<float>(s, (int)s->lv.size() - 1, (const float *)F.b, (float *)F.x));
+    v_convert<float, double>(s->nu, (const float *)F.x, zu, s->st);
+  }
+  return P3D_OK;
+}
+
+static int run_pc(p3d_solver *s, const double *in, double *out)
+{
+  if (s->gexec) {
+    CU(cudaMemcpyAsync(s->pc_in, in, s->N * 8, cudaMemcpyDeviceToDevice, s->st), "pc copy in");
+    CU(cudaGraphLaunch(s->gexec, s->st), "graph launch");
+    count_launch(1);
+    CU(cudaMemcpyAsync(out, s->pc_out, s->N * 8, cudaMemcpyDeviceToDevice, s->st), "pc copy out");
+    return P3D_OK;
+  }
+  return apply_pc(s, in, out);
+}
+
+// full operator y = [A11 A12; A21 0] x (BC_MATMULT)
+static int stokes_op(p3d_solver *s, const double *x, double *y)
+{
+  CU(cudaMemsetAsync(y, 0, s->N * 8, s->st), "memset");
+  Level &F = s->lv.back();
+  return launch_general<double, true, true, true>(F.op64, x, x + s->nu, y, y + s->nu, s->st);
+}
+
+// ||v||_2 (FP64)
+static int norm2(p3d_solver *s, const double *v, size_t n, double *out)
+{
+  CU(cudaMemcpyAsync(s->Vptr + P3D_MDOT_MAX - 1, &v, sizeof(double *), cudaMemcpyHostToDevice, s->st), "ptr");
+  v_mdot<double>(n, 1, (const double *const *)(s->Vptr + P3D_MDOT_MAX - 1), v, s->part, s->hdev + 2 * P3D_MDOT_MAX, s->st);
+  CU(cudaMemcpyAsync(s->hhost + 2 * P3D_MDOT_MAX, s->hdev + 2 * P3D_MDOT_MAX, 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+  CU(cudaStreamSynchronize(s->st), "sync");
+  *out = std::sqrt(std::max(0.0, s->hhost[2 * P3D_MDOT_MAX]));
+  return P3D_OK;
+}
+
+// largest eigenvalue of a symmetric tridiagonal matrix (bisection on Sturm counts)
+static double tridiag_lmax(const std::vector<double> &a, const std::vector<double> &b)
+{
+  int n = (int)a.size();
+  double lo = 1e300, hi = -1e300;
+  for (int i = 0; i < n; i++) {
+    double r = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(b[i]) : 0.0);
+    lo = std::min(lo, a[i] - r);
+    hi = std::max(hi, a[i] + r);
+  }
+  auto count_below = [&](double x) {
+    int c = 0;
+    double q = a[0] - x;
+    if (q < 0) c++;
+    for (int i = 1; i < n; i++) {
+      double qq = (std::fabs(q) < 1e-300) ? 1e-300 : q;
+      q = a[i] - x - b[i - 1] * b[i - 1] / qq;
+      if (q < 0) c++;
+    }
+    return c;
+  };
+  for (int it = 0; it < 200; it++) {
+    double mid = 0.5 * (lo + hi);
+    if (count_below(mid) >= n) hi = mid;
+    else lo = mid;
+  }
+  return hi;
+}
+
+// lmax(D^{-1} A) of level L by CG-Lanczos (FP64)
+static int estimate_lmax(p3d_solver *s, Level &L)
+{
+  const size_t n = L.nv;
+  double *x = (double *)L.x, *r = (double *)L.r, *z = (double *)L.d, *p = (double *)L.b, *q = (double *)L.t;
+  // deterministic pseudo-random start, Dirichlet entries zero
+  std::vector<double> h(n);
+  uint64_t st = 0x9E3779B97F4A7C15ull;
+  for (size_t i = 0; i < n; i++) {
+    st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+    h[i] = (double)(st >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+  }
+  CU(cudaMemcpyAsync(r, h.data(), n * 8, cudaMemcpyHostToDevice, s->st), "h2d");
+  v_mask<double>(L.n[0], L.n[1], L.n[2], level_dir(s), r, s->st);
+  (void)x;
+  v_jacobi<double>(n, L.dinv, r, z, s->st);
+  CU(cudaMemcpyAsync(p, z, n * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
+  auto dot = [&](const double *a, const double *b, double *out) -> int {
+    const double *ptrs[1] = {a};
+    CU(cudaMemcpyAsync(s->Vptr + P3D_MDOT_MAX - 1, ptrs, sizeof(double *), cudaMemcpyHostToDevice, s->st), "ptr");
+    v_mdot<double>(n, 1, (const double *const *)(s->Vptr + P3D_MDOT_MAX - 1), b, s->part, s->hdev, s->st);
+    CU(cudaMemcpyAsync(s->hhost, s->hdev, 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+    CU(cudaStreamSynchronize(s->st), "sync");
+    *out = s->hhost[0];
+    return P3D_OK;
+  };
+  double rz;
+  CK(dot(r, z, &rz));
+  std::vector<double> alpha, beta;
+  const int K = std::max(2, s->o.esteig_its);
+  for (int k = 0; k < K && rz > 0; k++) {
+    CK(a11<double>(s, L, p, q));
+    double pq;
+    CK(dot(p, q, &pq));
+    if (!(pq > 0)) break;
+    double a = rz / pq;
+    alpha.push_back(a);
+    v_axpby<double>(n, -a, q, 1.0, r, s->st);
+    v_jacobi<double>(n, L.dinv, r, z, s->st);
+    double rz2;
+    CK(dot(r, z, &rz2));
+    double bt = rz2 / rz;
+    beta.push_back(bt);
+    v_axpby<double>(n, 1.0, z, bt, p, s->st);
+    rz = rz2;
+  }
+  int m = (int)alpha.size();
+  if (m == 0) return set_error(P3D_ERR_BREAKDOWN, "esteig: CG broke down at the first step");
+  std::vector<double> ta(m), tb(std::max(1, m - 1));
+  for (int j = 0; j < m; j++) {
+    ta[j] = 1.0 / alpha[j] + (j > 0 ? beta[j - 1] / alpha[j - 1] : 0.0);
+    if (j + 1 < m) tb[j] = std::sqrt(std::max(0.0, beta[j])) / alpha[j];
+  }
+  L.lmax = tridiag_lmax(ta, tb);
+  if (!(L.lmax > 0) || !std::isfinite(L.lmax)) return set_error(P3D_ERR_BREAKDOWN, "esteig: bad lmax %g", L.lmax);
+  return P3D_OK;
+}
+
+// in-place Gauss-Jordan inversion of a dense SPD matrix (no pivoting), one step per pivot
+__global__ void k_gj_step(int n, int k, double *__restrict__ A, double *__restrict__ colk, double *__restrict__ rowk)
+{
+  // phase handled by the host loop: colk/rowk hold column and row k before the update
+  size_t total = (size_t)n * n;
+  double piv = rowk[k];
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    int i = idx / n, j = idx % n;
+    double v;
+    if (i == k) v = (j == k) ? 1.0 / piv : rowk[j] / piv;
+    else if (j == k) v = -colk[i] / piv;
+    else v = A[idx] - colk[i] * rowk[j] / piv;
+    A[idx] = v;
+  }
+}
+__global__ void k_gj_save(int n, int k, const double *__restrict__ A, double *__restrict__ colk, double *__restrict__ rowk)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    colk[i] = A[(size_t)i * n + k];
+    rowk[i] = A[(size_t)k * n + i];
+  }
+}
+
+// Galerkin coarse operator Ac = P~^T A1 P~ (+ identity on coarse Dirichlet rows), inverted in place
+static int build_coarse(p3d_solver *s)
+{
+  Level &C = s->lv[0];
+  const int nc = (int)C.nv;
+  s->nc = nc;
+  const uint32_t dir = level_dir(s);
+  CK(dev_alloc((void **)&s->cinv, (size_t)nc * nc * 8, "coarse operator"));
+  CK(dev_alloc((void **)&s->cb64, (size_t)nc * 8, "coarse vec"));
+  CK(dev_alloc((void **)&s->cx64, (size_t)nc * 8, "coarse vec"));
+  // coarse Dirichlet mask on the host
+  std::vector<char> isdir(nc, 0);
+  {
+    int nx = C.n[0], ny = C.n[1], nz = C.n[2];
+    for (int k = 0; k < nz; k++)
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++)
+          for (int c = 0; c < 3; c++) {
+            bool d = false;
+            d |= (i == 0) && (dir >> (0 + c) & 1u);
+            d |= (i == nx - 1) && (dir >> (3 + c) & 1u);
+            d |= (j == 0) && (dir >> (6 + c) & 1u);
+            d |= (j == ny - 1) && (dir >> (9 + c) & 1u);
+            d |= (k == 0) && (dir >> (12 + c) & 1u);
+            d |= (k == nz - 1) && (dir >> (15 + c) & 1u);
+            isdir[3 * ((size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k)) + c] = d;
+          }
+  }
+  if (s->lv.size() == 1) {
+    // single level: probe the operator itself
+    for (int j = 0; j < nc; j++) {
+      double *e = s->cb64;
+      CU(cudaMemsetAsync(e, 0, nc * 8, s->st), "memset");
+      double one = 1.0;
+      CU(cudaMemcpyAsync(e + j, &one, 8, cudaMemcpyHostToDevice, s->st), "h2d");
+      CK(a11<double>(s, C, e, s->cinv + (size_t)j * nc));
+    }
+  } else {
+    Level &F = s->lv[1];
+    double *ef = (double *)F.b, *yf = (double *)F.t;
+    for (int j = 0; j < nc; j++) {
+      double *col = s->cinv + (size_t)j * nc;
+      if (isdir[j]) {
+        CU(cudaMemsetAsync(col, 0, nc * 8, s->st), "memset");
+        double one = 1.0;
+        CU(cudaMemcpyAsync(col + j, &one, 8, cudaMemcpyHostToDevice, s->st), "h2d");
+        continue;
+      }
+      CU(cudaMemsetAsync(s->cb64, 0, nc * 8, s->st), "memset");
+      double one = 1.0;
+      CU(cudaMemcpyAsync(s->cb64 + j, &one, 8, cudaMemcpyHostToDevice, s->st), "h2d");
+      CK(mg_prolong<double>(C.n[0], C.n[1], C.n[2], 3, s->cb64, ef, s->st));
+      v_mask<double>(F.n[0], F.n[1], F.n[2], dir, ef, s->st);
+      CK(a11<double>(s, F, ef, yf));
+      v_mask<double>(F.n[0], F.n[1], F.n[2], dir, yf, s->st);
+      CK(mg_restrict<double>(C.n[0], C.n[1], C.n[2], 3, yf, col, s->st));
+      v_mask<double>(C.n[0], C.n[1], C.n[2], dir, col, s->st);
+    }
+  }
+  // Ac is symmetric: columns stored as rows is the same matrix.  Invert in place.
+  double *colk = nullptr, *rowk = nullptr;
+  CK(dev_alloc((void **)&colk, (size_t)nc * 8, "gj"));
+  CK(dev_alloc((void **)&rowk, (size_t)nc * 8, "gj"));
+  int g = (int)std::min<size_t>(((size_t)nc * nc + 255) / 256, 148 * 16);
+  for (int k = 0; k < nc; k++) {
+    k_gj_save<<<(nc + 255) / 256, 256, 0, s->st>>>(nc, k, s->cinv, colk, rowk);
+    k_gj_step<<<g, 256, 0, s->st>>>(nc, k, s->cinv, colk, rowk);
+  }
+  count_launch(2 * nc);
+  int rc = cuda_check(cudaStreamSynchronize(s->st), "coarse inverse");
+  cudaFree(colk);
+  cudaFree(rowk);
+  return rc;
+}
+
+static void free_level(Level &L)
+{
+  p3d_op_destroy(L.op64);
+  p3d_op_destroy(L.op32);
+  L.op64 = L.op32 = nullptr;
+  for (void *p : {(void *)L.coords, (void *)L.eta, (void *)L.dinv, L.b, L.x, L.r, L.d, L.t})
+    if (p) cudaFree(p);
+  L.coords = L.eta = L.dinv = nullptr;
+  L.b = L.x = L.r = L.d = L.t = nullptr;
+}
+
+static int solver_setup(p3d_solver *s, const double *coords, const double *eta)
+{
+  double t0 = now_ms();
+  const int nlev = (int)s->lv.size();
+  const bool mixed = s->o.mg_precision == P3D_PREC_F32;
+  const size_t es = mixed ? 4 : 8;
+  // hierarchy: finest first
+  for (int l = nlev - 1; l >= 0; l--) {
+    Level &L = s->lv[l];
+    size_t nn = (size_t)L.n[0] * L.n[1] * L.n[2], nel = (size_t)L.m[0] * L.m[1] * L.m[2];
+    if (!L.coords) CK(dev_alloc((void **)&L.coords, 3 * nn * 8, "level coords"));
+    if (!L.eta) CK(dev_alloc((void **)&L.eta, 27 * nel * 8, "level eta"));
+    if (l == nlev - 1) {
+      CU(cudaMemcpyAsync(L.coords, coords, 3 * nn * 8, cudaMemcpyDeviceToDevice, s->st), "coords");
+      CU(cudaMemcpyAsync(L.eta, eta, 27 * nel * 8, cudaMemcpyDeviceToDevice, s->st), "eta");
+    } else {
+      Level &F = s->lv[l + 1];
+      s_inject_coords(L.n[0], L.n[1], L.n[2], F.coords, L.coords, s->st);
+      s_restrict_eta(L.m[0], L.m[1], L.m[2], F.eta, L.eta, s->st);
+    }
+    CU(cudaStreamSynchronize(s->st), "hierarchy");
+    p3d_mesh_desc d;
+    p3d_mesh_desc_whole(L.m[0], L.m[1], L.m[2], s->mesh.dirichlet, &d);
+    if (!L.op64) CK(p3d_op_create(&d, P3D_PREC_F64, s->device, &L.op64));
+    CK(p3d_op_set_coefficients_device(L.op64, L.coords, L.eta, P3D_GEOM_AUTO));
+    CK(p3d_op_set_bc_mode(L.op64, P3D_BC_MATMULT));
+    if (mixed && l > 0) {
+      if (!L.op32) CK(p3d_op_create(&d, P3D_PREC_F32, s->device, &L.op32));
+      CK(p3d_op_set_coefficients_device(L.op32, L.coords, L.eta, P3D_GEOM_AUTO));
+      CK(p3d_op_set_bc_mode(L.op32, P3D_BC_MATMULT));
+    }
+    // work vectors: FP64 for esteig/Galerkin probing, reused as MG-precision vectors
+    for (void **p : {&L.b, &L.x, &L.r, &L.d, &L.t})
+      if (!*p) CK(dev_alloc(p, L.nv * 8, "level vector"));
+    (void)es;
+    if (!L.dinv) CK(dev_alloc((void **)&L.dinv, L.nv * 8, "dinv"));
+    CU(cudaMemsetAsync(L.t, 0, L.nv * 8, s->st), "memset");
+    CK(launch_diag<double>(L.op64, (double *)L.t, s->st));
+    // dinv = 1 / diag
+    std::vector<double> hd(L.nv);
+    CU(cudaMemcpyAsync(hd.data(), L.t, L.nv * 8, cudaMemcpyDeviceToHost, s->st), "d2h diag");
+    CU(cudaStreamSynchronize(s->st), "diag");
+    for (auto &v : hd) {
+      if (!(v > 0) || !std::isfinite(v)) return set_error(P3D_ERR_BREAKDOWN, "non-positive A11 diagonal %g", v);
+      v = 1.0 / v;
+    }
+    CU(cudaMemcpyAsync(L.dinv, hd.data(), L.nv * 8, cudaMemcpyHostToDevice, s->st), "h2d dinv");
+    if (l > 0) CK(estimate_lmax(s, L));
+  }
+  CK(build_coarse(s));
+  // Schur blocks on the fine mesh
+  Level &F = s->lv.back();
+  size_t nel = (size_t)F.m[0] * F.m[1] * F.m[2];
+  if (!s->Binv) CK(dev_alloc((void **)&s->Binv, 16 * nel * 8, "schur blocks"));
+  s_schur_blocks(F.m[0], F.m[1], F.m[2], F.coords, F.eta, s->Binv, s->st);
+  CU(cudaStreamSynchronize(s->st), "schur");
+  // preconditioner graph
+  if (s->o.use_graph) {
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    if (s->graph) { cudaGraphDestroy(s->graph); s->graph = nullptr; }
+    CU(cudaMemsetAsync(s->pc_in, 0, s->N * 8, s->st), "memset");
+    CK(apply_pc(s, s->pc_in, s->pc_out)); // eager run: sets kernel attributes before capture
+    CU(cudaStreamSynchronize(s->st), "pc warm");
+    CU(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int rc = apply_pc(s, s->pc_in, s->pc_out);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s->st, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    CU(e, "end capture");
+    s->graph = g;
+    CU(cudaGraphInstantiate(&s->gexec, g, 0), "graph instantiate");
+  }
+  s->setup_done = true;
+  s->setup_ms = now_ms() - t0;
+  return P3D_OK;
+}
+
+// FGMRES(m), right preconditioned; x = [u; p]
+static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
+{
+  const int m = s->o.restart;
+  const size_t N = s->N;
+  double *V = s->V, *Z = s->Z, *w = s->w;
+  std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+  double r0 = -1.0, rnorm = 0.0;
+  int its = 0;
+  bool conv = false;
+  while (its < s->o.max_it) {
+    // r = b - A x  into V_0
+    CK(stokes_op(s, x, w));
+    v_residual<double>(N, s->bvec, w, V, s->st);
+    double beta;
+    CK(norm2(s, V, N, &beta));
+    if (r0 < 0) r0 = beta;
+    rnorm = beta;
+    if (!std::isfinite(beta)) return set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual");
+    const double tol = std::max(s->o.rtol * r0, s->o.atol);
+    if (beta <= tol) { conv = true; break; }
+    v_scale<double>(N, 1.0 / beta, V, s->st);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int j = 0;
+    for (; j < m && its < s->o.max_it; j++, its++) {
+      double *vj = V + (size_t)j * N, *zj = Z + (size_t)j * N, *vn = V + (size_t)(j + 1) * N;
+      CK(run_pc(s, vj, zj));
+      CK(stokes_op(s, zj, w));
+      // two passes of classical Gram-Schmidt, coefficients on the device
+      for (int pass = 0; pass < 2; pass++) {
+        v_mdot<double>(N, j + 1, (const double *const *)s->Vptr, w, s->part, s->hdev, s->st);
+        v_maxpy<double>(N, j + 1, s->hdev, (const double *const *)s->Vptr, w, -1.0, s->st);
+        CU(cudaMemcpyAsync(s->hhost + pass * P3D_MDOT_MAX, s->hdev, (j + 1) * 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+      }
+      double hn;
+      CK(norm2(s, w, N, &hn)); // synchronizes
+      for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = s->hhost[i] + s->hhost[P3D_MDOT_MAX + i];
+      H[(size_t)(j + 1) * m + j] = hn;
+      if (hn > 0) {
+        CU(cudaMemcpyAsync(vn, w, N * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
+        v_scale<double>(N, 1.0 / hn, vn, s->st);
+      }
+      // Givens
+      for (int i = 0; i < j; i++) {
+        double a = H[(size_t)i * m + j], b = H[(size_t)(i + 1) * m + j];
+        H[(size_t)i * m + j] = cs[i] * a + sn[i] * b;
+        H[(size_t)(i + 1) * m + j] = -sn[i] * a + cs[i] * b;
+      }
+      double a = H[(size_t)j * m + j], b = H[(size_t)(j + 1) * m + j];
+      double rr = std::hypot(a, b);
+      cs[j] = rr > 0 ? a / rr : 1.0;
+      sn[j] = rr > 0 ? b / rr : 0.0;
+      H[(size_t)j * m + j] = rr;
+      H[(size_t)(j + 1) * m + j] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      rnorm = std::fabs(g[j + 1]);
+      if (s->o.verbose) fprintf(stderr, "  fgmres %3d  |r| %.6e\n", its + 1, rnorm);
+      if (!std::isfinite(rnorm)) return set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual estimate");
+      if (rnorm <= tol || hn == 0.0) { j++; its++; conv = rnorm <= tol; break; }
+    }
+    // y = H^{-1} g ; x += Z y
+    for (int i = j - 1; i >= 0; i--) {
+      double acc = g[i];
+      for (int k = i + 1; k < j; k++) acc -= H[(size_t)i * m + k] * y[k];
+      y[i] = acc / H[(size_t)i * m + i];
+    }
+    for (int i = 0; i < j; i++) v_axpby<double>(N, y[i], Z + (size_t)i * N, 1.0, x, s->st);
+    if (conv) break;
+  }
+  // true residual
+  CK(stokes_op(s, x, w));
+  v_residual<double>(N, s->bvec, w, w, s->st);
+  double rt;
+  CK(norm2(s, w, N, &rt));
+  stats->iterations = its;
+  stats->r0 = r0;
+  stats->rfinal = rt;
+  stats->converged = conv || rt <= std::max(s->o.rtol * r0, s->o.atol) * 1.0000001;
+  return P3D_OK;
+}
+
+} // namespace p3d
+
+using namespace p3d;
+
+extern "C" {
+
+int p3d_solver_default_opts(p3d_solver_opts *o)
+{
+  if (!o) return set_error(P3D_ERR_ARG, "null opts");
+  o->nlevels = 4;
+  o->cheb_its = 3;
+  o->cheb_lo = 0.2;
+  o->cheb_hi = 1.1;
+  o->esteig_its = 10;
+  o->mg_precision = P3D_PREC_F64;
+  o->restart = 30;
+  o->max_it = 200;
+  o->rtol = 1e-6;
+  o->atol = 0.0;
+  o->use_graph = 1;
+  o->verbose = 0;
+  return P3D_OK;
+}
+
+int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, int device, p3d_solver **out)
+{
+  if (!mesh || !out) return set_error(P3D_ERR_ARG, "solver_create: null argument");
+  *out = nullptr;
+  p3d_solver_opts o;
+  if (opts) o = *opts;
+  else p3d_solver_default_opts(&o);
+  if (mesh->ox || mesh->oy || mesh->oz || mesh->gx != 2 * mesh->mx + 1 || mesh->gy != 2 * mesh->my + 1 ||
+      mesh->gz != 2 * mesh->mz + 1)
+    return set_error(P3D_ERR_ARG, "solver_create: the solver takes a whole mesh (no ghost layers)");
+  if (o.nlevels < 1 || o.restart < 1 || o.restart > P3D_MDOT_MAX - 2 || o.max_it < 1 || o.cheb_its < 1 ||
+      !(o.cheb_hi > o.cheb_lo) || o.cheb_lo <= 0 || (o.mg_precision != 64 && o.mg_precision != 32))
+    return set_error(P3D_ERR_ARG, "solver_create: bad options");
+  int f = 1 << (o.nlevels - 1);
+  if (mesh->mx % f || mesh->my % f || mesh->mz % f)
+    return set_error(P3D_ERR_ARG, "solver_create: %dx%dx%d not divisible by 2^(nlevels-1)=%d", mesh->mx, mesh->my,
+                     mesh->mz, f);
+  CK(cuda_check(cudaSetDevice(device), "cudaSetDevice"));
+  p3d_solver *s = new p3d_solver();
+  s->mesh = *mesh;
+  s->o = o;
+  s->device = device;
+  int rc = cuda_check(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking), "stream");
+  s->lv.resize(o.nlevels);
+  for (int l = 0; l < o.nlevels; l++) {
+    int c = 1 << (o.nlevels - 1 - l);
+    Level &L = s->lv[l];
+    L.m[0] = mesh->mx / c; L.m[1] = mesh->my / c; L.m[2] = mesh->mz / c;
+    for (int d = 0; d < 3; d++) L.n[d] = 2 * L.m[d] + 1;
+    L.nv = 3ull * L.n[0] * L.n[1] * L.n[2];
+  }
+  Level &F = s->lv.back();
+  s->nu = F.nv;
+  s->np = 4ull * F.m[0] * F.m[1] * F.m[2];
+  s->N = s->nu + s->np;
+  const size_t N = s->N;
+  const int m = o.restart;
+  if (!rc) rc = dev_alloc((void **)&s->V, (size_t)(m + 1) * N * 8, "FGMRES V");
+  if (!rc) rc = dev_alloc((void **)&s->Z, (size_t)m * N * 8, "FGMRES Z");
+  if (!rc) rc = dev_alloc((void **)&s->w, N * 8, "FGMRES w");
+  if (!rc) rc = dev_alloc((void **)&s->bvec, N * 8, "rhs");
+  if (!rc) rc = dev_alloc((void **)&s->pc_in, N * 8, "pc in");
+  if (!rc) rc = dev_alloc((void **)&s->pc_out, N * 8, "pc out");
+  if (!rc) rc = dev_alloc((void **)&s->pc_t, s->nu * 8, "pc t");
+  if (!rc) rc = dev_alloc((void **)&s->Vptr, P3D_MDOT_MAX * sizeof(double *), "V ptrs");
+  if (!rc) rc = dev_alloc((void **)&s->part, (size_t)P3D_MDOT_BLOCKS * P3D_MDOT_MAX * 8, "partials");
+  if (!rc) rc = dev_alloc((void **)&s->hdev, 3 * P3D_MDOT_MAX * 8, "h");
+  if (!rc) rc = cuda_check(cudaMallocHost((void **)&s->hhost, 3 * P3D_MDOT_MAX * 8), "pinned h");
+  if (!rc) {
+    std::vector<double *> ptrs(P3D_MDOT_MAX, nullptr);
+    for (int j = 0; j <= m; j++) ptrs[j] = s->V + (size_t)j * N;
+    rc = cuda_check(cudaMemcpy(s->Vptr, ptrs.data(), P3D_MDOT_MAX * sizeof(double *), cudaMemcpyHostToDevice), "ptrs");
+  }
+  if (!rc) rc = cuda_check(cudaMemset(s->bvec, 0, N * 8), "rhs zero");
+  if (rc) {
+    p3d_solver_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return P3D_OK;
+}
+
+int p3d_solver_setup(p3d_solver *s, const double *coords, const double *eta)
+{
+  if (!s || !coords || !eta) return set_error(P3D_ERR_ARG, "solver_setup: null argument");
+  cudaSetDevice(s->device);
+  return solver_setup(s, coords, eta);
+}
+
+int p3d_solver_set_rhs_body_force(p3d_solver *s, const double *rho, double gx, double gy, double gz)
+{
+  if (!s || !rho) return set_error(P3D_ERR_ARG, "set_rhs_body_force: null argument");
+  if (!s->setup_done) return set_error(P3D_ERR_STATE, "set_rhs_body_force before setup");
+  Level &F = s->lv.back();
+  CU(cudaMemsetAsync(s->bvec, 0, s->N * 8, s->st), "memset");
+  double g[3] = {gx, gy, gz};
+  s_body_force(F.m[0], F.m[1], F.m[2], F.coords, rho, g, s->bvec, s->st);
+  v_mask<double>(F.n[0], F.n[1], F.n[2], s->mesh.dirichlet, s->bvec, s->st);
+  s->rhs_set = true;
+  return cuda_check(cudaStreamSynchronize(s->st), "rhs");
+}
+
+int p3d_solver_set_rhs(p3d_solver *s, const double *bu, const double *bp)
+{
+  if (!s || !bu || !bp) return set_error(P3D_ERR_ARG, "set_rhs: null argument");
+  CU(cudaMemcpyAsync(s->bvec, bu, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "rhs u");
+  CU(cudaMemcpyAsync(s->bvec + s->nu, bp, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "rhs p");
+  s->rhs_set = true;
+  return cuda_check(cudaStreamSynchronize(s->st), "rhs");
+}
+
+int p3d_solver_solve(p3d_solver *s, double *u, double *p, p3d_solve_stats *stats)
+{
+  if (!s || !u || !p) return set_error(P3D_ERR_ARG, "solve: null argument");
+  if (!s->setup_done || !s->rhs_set) return set_error(P3D_ERR_STATE, "solve before setup / rhs");
+  cudaSetDevice(s->device);
+  p3d_solve_stats local;
+  memset(&local, 0, sizeof local);
+  double t0 = now_ms();
+  // x = [u; p] assembled in pc_out scratch? use a dedicated copy in w-sized buffer: reuse pc_in
+  double *x = nullptr;
+  CK(dev_alloc((void **)&x, s->N * 8, "solution"));
+  int rc = cuda_check(cudaMemcpyAsync(x, u, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "x u");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(x + s->nu, p, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "x p");
+  if (!rc) rc = fgmres(s, x, &local);
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(u, x, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "u out");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(p, x + s->nu, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "p out");
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(s->st), "solve sync");
+  cudaFree(x);
+  local.solve_ms = now_ms() - t0;
+  local.setup_ms = s->setup_ms;
+  local.lmax_fine = s->lv.back().lmax;
+  local.coarse_dofs = s->nc;
+  if (stats) *stats = local;
+  if (rc) return rc;
+  if (!local.converged) return set_error(P3D_ERR_NOCONV, "FGMRES: %d iterations, |r| %.3e / %.3e", local.iterations,
+                                         local.rfinal, local.r0);
+  return P3D_OK;
+}
+
+int p3d_solver_apply_pc(p3d_solver *s, const double *ru, const double *rp, double *zu, double *zp)
+{
+  if (!s || !ru || !rp || !zu || !zp) return set_error(P3D_ERR_ARG, "apply_pc: null argument");
+  if (!s->setup_done) return set_error(P3D_ERR_STATE, "apply_pc before setup");
+  CU(cudaMemcpyAsync(s->pc_in, ru, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
+  CU(cudaMemcpyAsync(s->pc_in + s->nu, rp, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
+  CK(run_pc(s, s->pc_in, s->w));
+  CU(cudaMemcpyAsync(zu, s->w, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
+  CU(cudaMemcpyAsync(zp, s->w + s->nu, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
+  return cuda_check(cudaStreamSynchronize(s->st), "apply_pc");
+}
+
+int p3d_solver_destroy(p3d_solver *s)
+{
+  if (!s) return P3D_OK;
+  cudaSetDevice(s->device);
+  if (s->st) cudaStreamSynchronize(s->st);
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  for (auto &L : s->lv) free_level(L);
+  for (void *p : {(void *)s->cinv, (void *)s->cb64, (void *)s->cx64, (void *)s->Binv, (void *)s->bvec, (void *)s->V,
+                  (void *)s->Z, (void *)s->w, (void *)s->Vptr, (void *)s->part, (void *)s->hdev, (void *)s->pc_in,
+                  (void *)s->pc_out, (void *)s->pc_t})
+    if (p) cudaFree(p);
+  if (s->hhost) cudaFreeHost(s->hhost);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+  return P3D_OK;
+}
+
+} // extern "C"

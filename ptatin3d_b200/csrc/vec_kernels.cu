@@ -1,0 +1,233 @@
+// Vector kernels of the device-resident Stokes solver: grid-stride elementwise
+// updates (fused where the Chebyshev and FGMRES recurrences allow), FP64
+// reductions (two-phase, deterministic), Dirichlet masking by lattice face
+// test, precision conversion, the per-element 4x4 Schur block apply and a
+// dense matrix-vector product for the coarse-grid solve.
+#include <cuda_runtime.h>
+
+#include "p3d_internal.h"
+#include "q2_tile.cuh"
+#include "solver_internal.h"
+
+namespace p3d {
+
+static int vgrid(size_t n)
+{
+  size_t g = (n + 255) / 256;
+  size_t cap = 148 * 8;
+  if (g > cap) g = cap;
+  return g < 1 ? 1 : (int)g;
+}
+
+#define GS_LOOP(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
+
+template <typename A, typename B> __global__ void k_convert(size_t n, const A *__restrict__ x, B *__restrict__ y)
+{
+  GS_LOOP(i, n) y[i] = (B)x[i];
+}
+template <typename T> __global__ void k_axpby(size_t n, T a, const T *__restrict__ x, T b, T *__restrict__ y)
+{
+  GS_LOOP(i, n) y[i] = a * x[i] + b * y[i];
+}
+template <typename T> __global__ void k_scale(size_t n, T a, T *__restrict__ y)
+{
+  GS_LOOP(i, n) y[i] *= a;
+}
+// z = dinv .* r   (dinv stored in FP64)
+template <typename T> __global__ void k_jacobi(size_t n, const double *__restrict__ dinv, const T *__restrict__ r, T *__restrict__ z)
+{
+  GS_LOOP(i, n) z[i] = (T)(dinv[i] * (double)r[i]);
+}
+// Chebyshev start: r = b - A x was formed in r (or r = b when x = 0);
+// d = dinv .* r / theta
+template <typename T>
+__global__ void k_cheb_init(size_t n, const double *__restrict__ dinv, const T *__restrict__ r, T inv_theta, T *__restrict__ d)
+{
+  GS_LOOP(i, n) d[i] = (T)(dinv[i] * (double)r[i]) * inv_theta;
+}
+// x += d ; r -= Ad ; d = c1 d + c2 dinv .* r   (one pass for the Chebyshev recurrence)
+template <typename T>
+__global__ void k_cheb_step(size_t n, const double *__restrict__ dinv, T *__restrict__ x, T *__restrict__ r,
+                            const T *__restrict__ Ad, T *__restrict__ d, T c1, T c2)
+{
+  GS_LOOP(i, n)
+  {
+    T di = d[i];
+    x[i] += di;
+    T ri = r[i] - Ad[i];
+    r[i] = ri;
+    d[i] = c1 * di + c2 * (T)(dinv[i] * (double)ri);
+  }
+}
+// r = b - Ax
+template <typename T> __global__ void k_residual(size_t n, const T *__restrict__ b, const T *__restrict__ Ax, T *__restrict__ r)
+{
+  GS_LOOP(i, n) r[i] = b[i] - Ax[i];
+}
+
+// zero the Dirichlet dofs of a whole-mesh velocity vector (face test on the lattice)
+template <typename T>
+__global__ void k_mask(int nx, int ny, int nz, uint32_t dir, T *__restrict__ v)
+{
+  size_t nn = (size_t)nx * ny * nz;
+  GS_LOOP(node, nn)
+  {
+    int i = node % nx, j = (node / nx) % ny, k = node / ((size_t)nx * ny);
+    if (!(i == 0 || j == 0 || k == 0 || i == nx - 1 || j == ny - 1 || k == nz - 1)) continue;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      if (is_dirichlet(dir, i, j, k, 0, 0, 0, nx - 1, ny - 1, nz - 1, c)) v[3 * node + c] = (T)0;
+  }
+}
+
+// partial dot products  part[blk*k + j] = sum_i V_j[i] w[i]   (FP64 accumulation)
+template <typename T>
+__global__ void k_mdot_partial(size_t n, int k, const T *const *__restrict__ V, const T *__restrict__ w, double *__restrict__ part)
+{
+  __shared__ double red[32][P3D_MDOT_MAX];
+  double acc[P3D_MDOT_MAX];
+  for (int j = 0; j < k; j++) acc[j] = 0.0;
+  GS_LOOP(i, n)
+  {
+    double wi = (double)w[i];
+    for (int j = 0; j < k; j++) acc[j] += (double)V[j][i] * wi;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j = 0; j < k; j++) {
+    double v = acc[j];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][j] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < k) {
+    double s = 0.0;
+    for (int q = 0; q < nw; q++) s += red[q][threadIdx.x];
+    part[(size_t)blockIdx.x * k + threadIdx.x] = s;
+  }
+}
+__global__ void k_sum_partials(int nblk, int k, const double *__restrict__ part, double *__restrict__ out)
+{
+  // one warp per output
+  int j = blockIdx.x;
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += 32) s += part[(size_t)b * k + j];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) out[j] = s;
+}
+// w -= sum_j h_j V_j   (h on device)
+template <typename T>
+__global__ void k_maxpy(size_t n, int k, const double *__restrict__ h, const T *const *__restrict__ V, T *__restrict__ w, double sign)
+{
+  GS_LOOP(i, n)
+  {
+    double s = 0.0;
+    for (int j = 0; j < k; j++) s += h[j] * (double)V[j][i];
+    w[i] = (T)((double)w[i] + sign * s);
+  }
+}
+
+// y = blockdiag(B_e) x  with B_e 4x4 per element (Schur approximation inverse)
+__global__ void k_block4(size_t nel, const double *__restrict__ B, const double *__restrict__ x, double *__restrict__ y, double alpha)
+{
+  GS_LOOP(e, nel)
+  {
+    const double *b = B + 16 * e;
+    double x0 = x[4 * e], x1 = x[4 * e + 1], x2 = x[4 * e + 2], x3 = x[4 * e + 3];
+    for (int r = 0; r < 4; r++) y[4 * e + r] = alpha * (b[4 * r] * x0 + b[4 * r + 1] * x1 + b[4 * r + 2] * x2 + b[4 * r + 3] * x3);
+  }
+}
+
+// y = M x, M dense row-major n x n (coarse-grid inverse); one warp per row
+__global__ void k_dense_mv(int n, const double *__restrict__ M, const double *__restrict__ x, double *__restrict__ y)
+{
+  int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int c = lane; c < n; c += 32) s += M[(size_t)row * n + c] * x[c];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) y[row] = s;
+}
+
+// ------------------------------------------------------------ host API ---
+template <typename A, typename B> void v_convert(size_t n, const A *x, B *y, cudaStream_t s)
+{
+  k_convert<<<vgrid(n), 256, 0, s>>>(n, x, y);
+  count_launch(1);
+}
+template <typename T> void v_axpby(size_t n, T a, const T *x, T b, T *y, cudaStream_t s)
+{
+  k_axpby<<<vgrid(n), 256, 0, s>>>(n, a, x, b, y);
+  count_launch(1);
+}
+template <typename T> void v_scale(size_t n, T a, T *y, cudaStream_t s)
+{
+  k_scale<<<vgrid(n), 256, 0, s>>>(n, a, y);
+  count_launch(1);
+}
+template <typename T> void v_jacobi(size_t n, const double *dinv, const T *r, T *z, cudaStream_t s)
+{
+  k_jacobi<<<vgrid(n), 256, 0, s>>>(n, dinv, r, z);
+  count_launch(1);
+}
+template <typename T> void v_cheb_init(size_t n, const double *dinv, const T *r, T inv_theta, T *d, cudaStream_t s)
+{
+  k_cheb_init<<<vgrid(n), 256, 0, s>>>(n, dinv, r, inv_theta, d);
+  count_launch(1);
+}
+template <typename T>
+void v_cheb_step(size_t n, const double *dinv, T *x, T *r, const T *Ad, T *d, T c1, T c2, cudaStream_t s)
+{
+  k_cheb_step<<<vgrid(n), 256, 0, s>>>(n, dinv, x, r, Ad, d, c1, c2);
+  count_launch(1);
+}
+template <typename T> void v_residual(size_t n, const T *b, const T *Ax, T *r, cudaStream_t s)
+{
+  k_residual<<<vgrid(n), 256, 0, s>>>(n, b, Ax, r);
+  count_launch(1);
+}
+template <typename T> void v_mask(int nx, int ny, int nz, uint32_t dir, T *v, cudaStream_t s)
+{
+  if (!dir) return;
+  k_mask<<<vgrid((size_t)nx * ny * nz), 256, 0, s>>>(nx, ny, nz, dir, v);
+  count_launch(1);
+}
+template <typename T>
+void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s)
+{
+  k_mdot_partial<<<P3D_MDOT_BLOCKS, 256, 0, s>>>(n, k, V_dev, w, part);
+  k_sum_partials<<<k, 32, 0, s>>>(P3D_MDOT_BLOCKS, k, part, out_dev);
+  count_launch(2);
+}
+template <typename T> void v_maxpy(size_t n, int k, const double *h, const T *const *V_dev, T *w, double sign, cudaStream_t s)
+{
+  k_maxpy<<<vgrid(n), 256, 0, s>>>(n, k, h, V_dev, w, sign);
+  count_launch(1);
+}
+void v_block4(size_t nel, const double *B, const double *x, double *y, double alpha, cudaStream_t s)
+{
+  k_block4<<<vgrid(nel), 256, 0, s>>>(nel, B, x, y, alpha);
+  count_launch(1);
+}
+void v_dense_mv(int n, const double *M, const double *x, double *y, cudaStream_t s)
+{
+  k_dense_mv<<<(n + 7) / 8, 256, 0, s>>>(n, M, x, y);
+  count_launch(1);
+}
+
+template void v_convert<double, float>(size_t, const double *, float *, cudaStream_t);
+template void v_convert<float, double>(size_t, const float *, double *, cudaStream_t);
+#define P3D_INST(T)                                                                                                    \
+  template void v_axpby<T>(size_t, T, const T *, T, T *, cudaStream_t);                                                \
+  template void v_scale<T>(size_t, T, T *, cudaStream_t);                                                              \
+  template void v_jacobi<T>(size_t, const double *, const T *, T *, cudaStream_t);                                     \
+  template void v_cheb_init<T>(size_t, const double *, const T *, T, T *, cudaStream_t);                               \
+  template void v_cheb_step<T>(size_t, const double *, T *, T *, const T *, T *, T, T, cudaStream_t);                  \
+  template void v_residual<T>(size_t, const T *, const T *, T *, cudaStream_t);                                        \
+  template void v_mask<T>(int, int, int, uint32_t, T *, cudaStream_t);                                                 \
+  template void v_mdot<T>(size_t, int, const T *const *, const T *, double *, double *, cudaStream_t);                 \
+  template void v_maxpy<T>(size_t, int, const double *, const T *const *, T *, double, cudaStream_t);
+P3D_INST(double)
+P3D_INST(float)
+
+} // namespace p3d

@@ -1,0 +1,92 @@
+"""Device-resident Stokes solve (FGMRES + Schur upper + GMG) from Python.
+
+Mirrors the reference driver's linear solve
+(pTatin3d_linear_viscous_forward_model_driver, src/ptatin_driver_linear_ts.c:884-1100)
+for one whole mesh: build the operators on a hierarchy, set the body-force
+right-hand side, solve to a relative residual tolerance.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import PREC_F32, PREC_F64, SolverOpts, SolveStats, check, lib
+from .operators import _ptr, mesh_desc_whole
+
+
+def default_opts(**kw) -> SolverOpts:
+    o = SolverOpts()
+    check(lib().p3d_solver_default_opts(C.byref(o)))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise KeyError(k)
+        setattr(o, k, v)
+    return o
+
+
+def max_levels(m: int, coarse_min: int = 2) -> int:
+    """Levels such that the mesh halves cleanly down to a coarse size >= coarse_min."""
+    lev = 1
+    while m % 2 == 0 and m // 2 >= coarse_min:
+        m //= 2
+        lev += 1
+    return lev
+
+
+class StokesSolver:
+    def __init__(self, mx, my, mz, dirichlet, device=0, **opts):
+        self.dims = (mx, my, mz)
+        self.desc = mesh_desc_whole(mx, my, mz, dirichlet)
+        self.opts = default_opts(**opts)
+        h = C.c_void_p()
+        check(lib().p3d_solver_create(C.byref(self.desc), C.byref(self.opts), device, C.byref(h)))
+        self.h = h
+        self.nu = 3 * (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1)
+        self.np = 4 * mx * my * mz
+        self.device = torch.device("cuda", device)
+
+    def _dev(self, a):
+        if isinstance(a, torch.Tensor):
+            return a.to(device=self.device, dtype=torch.float64).contiguous()
+        return torch.tensor(np.ascontiguousarray(a, dtype=np.float64).reshape(-1), device=self.device)
+
+    def setup(self, coords, eta):
+        c, e = self._dev(coords), self._dev(eta)
+        check(lib().p3d_solver_setup(self.h, _ptr(c), _ptr(e)))
+
+    def set_rhs_body_force(self, rho, g=(0.0, 0.0, -1.0)):
+        r = self._dev(rho)
+        check(lib().p3d_solver_set_rhs_body_force(self.h, _ptr(r), *map(float, g)))
+
+    def set_rhs(self, bu, bp):
+        check(lib().p3d_solver_set_rhs(self.h, _ptr(self._dev(bu)), _ptr(self._dev(bp))))
+
+    def solve(self, u=None, p=None, raise_on_noconv=True):
+        u = torch.zeros(self.nu, dtype=torch.float64, device=self.device) if u is None else self._dev(u)
+        p = torch.zeros(self.np, dtype=torch.float64, device=self.device) if p is None else self._dev(p)
+        st = SolveStats()
+        rc = lib().p3d_solver_solve(self.h, _ptr(u), _ptr(p), C.byref(st))
+        if rc != 0 and (raise_on_noconv or rc != _lib.P3D_ERR_NOCONV):
+            check(rc)
+        stats = {f: getattr(st, f) for f, _ in SolveStats._fields_}
+        return u, p, stats
+
+    def apply_pc(self, ru, rp):
+        zu = torch.empty(self.nu, dtype=torch.float64, device=self.device)
+        zp = torch.empty(self.np, dtype=torch.float64, device=self.device)
+        check(lib().p3d_solver_apply_pc(self.h, _ptr(self._dev(ru)), _ptr(self._dev(rp)), _ptr(zu), _ptr(zp)))
+        return zu, zp
+
+    def destroy(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().p3d_solver_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -1,0 +1,118 @@
+"""GPU Stokes solve (FGMRES + Schur upper + GMG) against the CPU oracle.
+
+The oracle solve assembles [A11 A12; A21 0] by probing the CPU restatement's
+operators and solves it densely (small meshes).  Solver-level PETSc parity is
+not available (PETSc is not vendored), so the solve is checked against this
+exact discrete solution instead.
+"""
+import numpy as np
+import pytest
+import torch
+
+from cases import rel
+from oracle.oracle import body_force, stokes_dense_solve
+from ptatin3d_b200 import PREC_F32, PREC_F64, P3DError
+from ptatin3d_b200 import mesh as M
+from ptatin3d_b200.solver import StokesSolver
+
+pytestmark = pytest.mark.gpu
+
+# free slip on the walls and the base, free surface on top (z max)
+BITS = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
+
+
+def sinker(m, nsph=2, radius=0.2, contrast=1e2, seed=1, deform=0.0):
+    c = M.uniform_coords(m, m, m)
+    if deform:
+        c = M.perturb_interior(c, m, m, m, frac=deform, seed=seed)
+    qp = M.qp_coords(c, m, m, m)
+    cen, r = M.random_sinkers(nsph, seed, radius)
+    eta = M.sinker_eta(qp, cen, r, 1.0, contrast)
+    rho = M.sinker_density(qp, cen, r, 1.0, 1.01)
+    return c, eta, rho
+
+
+@pytest.mark.parametrize("deform", [0.0, 0.1])
+def test_solve_matches_dense_oracle(cuda, restatement, deform):
+    m = 4
+    c, eta, rho = sinker(m, deform=deform)
+    mask = M.dirichlet_mask(m, m, m, BITS)
+    bu = body_force(restatement, (m, m, m), c, rho)
+    bu[mask.astype(bool)] = 0.0
+    u_ref, p_ref = stokes_dense_solve(restatement, (m, m, m), c, eta, mask, bu)
+    S = StokesSolver(m, m, m, BITS, nlevels=2, rtol=1e-11, max_it=300)
+    S.setup(c, eta)
+    S.set_rhs_body_force(rho, (0.0, 0.0, -1.0))
+    u, p, st = S.solve()
+    assert st["converged"]
+    assert rel(u.cpu().numpy(), u_ref) <= 1e-8
+    assert rel(p.cpu().numpy(), p_ref) <= 1e-7
+
+
+def test_rhs_matches_oracle(cuda, restatement):
+    m = 6
+    c, eta, rho = sinker(m, deform=0.1)
+    bu_ref = body_force(restatement, (m, m, m), c, rho, (0.3, -0.2, -1.0))
+    bu_ref[M.dirichlet_mask(m, m, m, BITS).astype(bool)] = 0.0
+    sols = []
+    for use_kernel in (True, False):
+        S = StokesSolver(m, m, m, BITS, nlevels=2, rtol=1e-11, max_it=300)
+        S.setup(c, eta)
+        if use_kernel:
+            S.set_rhs_body_force(rho, (0.3, -0.2, -1.0))
+        else:
+            S.set_rhs(bu_ref, np.zeros(S.np))
+        sols.append(S.solve()[0].cpu().numpy())
+    assert rel(sols[0], sols[1]) <= 1e-9
+
+
+@pytest.mark.parametrize("prec", [PREC_F64, PREC_F32])
+def test_multilevel_solve_converges(cuda, prec):
+    m = 16
+    c, eta, rho = sinker(m, nsph=4, radius=0.12, contrast=1e4)
+    S = StokesSolver(m, m, m, BITS, nlevels=3, rtol=1e-6, mg_precision=prec)
+    S.setup(c, eta)
+    S.set_rhs_body_force(rho)
+    u, p, st = S.solve()
+    assert st["converged"] and st["iterations"] < 120
+    assert st["rfinal"] <= 1.0000001e-6 * st["r0"]
+
+
+def test_mixed_precision_error_vs_fp64_oracle_solve(cuda):
+    m = 16
+    c, eta, rho = sinker(m, nsph=4, radius=0.12, contrast=1e4)
+    ref = StokesSolver(m, m, m, BITS, nlevels=3, rtol=1e-11, max_it=400)
+    ref.setup(c, eta)
+    ref.set_rhs_body_force(rho)
+    u64, p64, _ = ref.solve()
+    mix = StokesSolver(m, m, m, BITS, nlevels=3, rtol=1e-8, mg_precision=PREC_F32, max_it=400)
+    mix.setup(c, eta)
+    mix.set_rhs_body_force(rho)
+    u32, p32, st = mix.solve()
+    assert st["converged"]
+    assert rel(u32.cpu().numpy(), u64.cpu().numpy()) <= 1e-6
+    assert rel(p32.cpu().numpy(), p64.cpu().numpy()) <= 1e-5
+
+
+def test_graph_and_eager_preconditioner_agree(cuda):
+    m = 8
+    c, eta, rho = sinker(m)
+    a = StokesSolver(m, m, m, BITS, nlevels=3, use_graph=1)
+    b = StokesSolver(m, m, m, BITS, nlevels=3, use_graph=0)
+    for s in (a, b):
+        s.setup(c, eta)
+    rng = np.random.default_rng(0)
+    ru = rng.standard_normal(a.nu)
+    ru[M.dirichlet_mask(m, m, m, BITS).astype(bool)] = 0.0
+    rp = rng.standard_normal(a.np)
+    za = a.apply_pc(ru, rp)
+    zb = b.apply_pc(ru, rp)
+    for x, y in zip(za, zb):
+        assert rel(x.cpu().numpy(), y.cpu().numpy()) <= 1e-14
+
+
+def test_solver_rejects_bad_sizes(cuda):
+    with pytest.raises(P3DError):
+        StokesSolver(6, 6, 6, BITS, nlevels=3)  # 6 not divisible by 4
+    with pytest.raises(P3DError):
+        StokesSolver(8, 8, 8, BITS, restart=200)
