@@ -171,7 +171,7 @@ template <typename T, int NW> struct AffineSmem {
 };
 
 template <typename T, int NW>
-__global__ void __launch_bounds__(32 * NW) a11_affine_kernel(TileArgs<T> A)
+__global__ void __launch_bounds__(32 * NW, 4) a11_affine_kernel(TileArgs<T> A)
 {
   using BK = Brick<NW>;
   using SM = AffineSmem<T, NW>;

@@ -62,7 +62,8 @@ class StokesSolver:
         check(lib().p3d_solver_set_rhs_body_force(self.h, _ptr(r), *map(float, g)))
 
     def set_rhs(self, bu, bp):
-        check(lib().p3d_solver_set_rhs(self.h, _ptr(self._dev(bu)), _ptr(self._dev(bp))))
+        bu_d, bp_d = self._dev(bu), self._dev(bp)  # keep both alive across the call
+        check(lib().p3d_solver_set_rhs(self.h, _ptr(bu_d), _ptr(bp_d)))
 
     def solve(self, u=None, p=None, raise_on_noconv=True):
         u = torch.zeros(self.nu, dtype=torch.float64, device=self.device) if u is None else self._dev(u)
@@ -77,7 +78,8 @@ class StokesSolver:
     def apply_pc(self, ru, rp):
         zu = torch.empty(self.nu, dtype=torch.float64, device=self.device)
         zp = torch.empty(self.np, dtype=torch.float64, device=self.device)
-        check(lib().p3d_solver_apply_pc(self.h, _ptr(self._dev(ru)), _ptr(self._dev(rp)), _ptr(zu), _ptr(zp)))
+        ru_d, rp_d = self._dev(ru), self._dev(rp)  # keep both alive across the call
+        check(lib().p3d_solver_apply_pc(self.h, _ptr(ru_d), _ptr(rp_d), _ptr(zu), _ptr(zp)))
         return zu, zp
 
     def destroy(self):
