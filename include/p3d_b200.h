@@ -116,6 +116,18 @@ int p3d_stokes_apply(p3d_op *op, const void *u, const void *p, void *yu, void *y
  * SpMVOp "+=" contract), and returns when y is complete. */
 int p3d_a11_apply_host(p3d_op *op, const double *x_host, double *y_host);
 
+/* Same result as p3d_a11_apply_host, without allocating any device memory
+ * (no counterpart in the reference).  For callers that may not call
+ * cudaMalloc/cudaFree, e.g. a MatShell callback running while the application
+ * owns the device memory pool.  The x/y staging lives in a fixed file-scope
+ * device array of P3D_NOALLOC_MAX_DOFS doubles each, resident on every device
+ * that loads the library until the process exits; larger meshes return
+ * P3D_ERR_ARG.  The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  Calls share
+ * the array: calls whose work overlaps on the GPU race. */
+#define P3D_NOALLOC_MAX_DOFS 107811 /* 3 * 33^3: a 16^3-element Q2 mesh */
+int p3d_a11_apply_host_noalloc(p3d_op *op, const double *x_host, double *y_host);
+
 /* --------------------------------------- multigrid transfer (DMDA) ---- */
 /* Trilinear prolongation on the node lattice, coarse (cnx,cny,cnz) nodes ->
  * fine (2c-1) nodes, `ndof` interleaved components; xf = P xc (overwrite).
