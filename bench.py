@@ -36,6 +36,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "A11 MF apply GDoF/s (FP64, 96^3 Q2 deformed mesh)"
+# the reference's flop count of one element apply (src/stokes_operators_cuda.cu:520-522)
+REF_FLOPS_PER_EL = 17253
 UNIT = "GDoF/s"
 
 
@@ -174,6 +176,51 @@ def cpu_reference_apply(wl, steps, warmup, threads=None):
     return dt, n
 
 
+SOLVE_WORKLOAD = ("Stokes solve, Q2-P1disc 32^3 unit cube, 8 sinkers r=0.1 (eta contrast 1e4, density +1%), "
+                  "g=-z, free slip walls/base, free surface top; FGMRES(30) + Schur upper (geometric-mean "
+                  "viscosity-scaled mass matrix) + 4-level Galerkin GMG, Chebyshev(3)/Jacobi, rtol 1e-6")
+
+
+def solve_leg(device, m=32, seed=1):
+    """FP64 vs mixed-precision device-resident Stokes solve, each checked
+    against an FP64 solve converged to rtol 1e-10."""
+    import torch
+
+    from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
+    from ptatin3d_b200 import mesh as M
+    from ptatin3d_b200.solver import StokesSolver
+    bits = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
+    c = M.uniform_coords(m, m, m)
+    qp = M.qp_coords(c, m, m, m)
+    cen, r = M.random_sinkers(8, seed, 0.1)
+    eta = M.sinker_eta(qp, cen, r, 1.0, 1e4)
+    rho = M.sinker_density(qp, cen, r, 1.0, 1.01)
+    out = {}
+    sols = {}
+    for name, prec, rtol in (("ref", PREC_F64, 1e-10), ("fp64", PREC_F64, 1e-6), ("mixed", PREC_F32, 1e-6)):
+        S = StokesSolver(m, m, m, bits, device=device, nlevels=4, rtol=rtol, max_it=8000, mg_precision=prec,
+                         schur_eta=SCHUR_ETA_GEOMEAN)
+        S.setup(c, eta)
+        S.set_rhs_body_force(rho)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, p, st = S.solve(raise_on_noconv=False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        sols[name] = (u.cpu().numpy(), p.cpu().numpy())
+        out[name] = {"s": dt, "iterations": st["iterations"], "converged": bool(st["converged"]),
+                     "rel_residual": st["rfinal"] / st["r0"], "setup_s": st["setup_ms"] * 1e-3}
+        S.destroy()
+    ur, pr = sols["ref"]
+    for name in ("fp64", "mixed"):
+        u, p = sols[name]
+        out[name]["u_err"] = float(np.linalg.norm(u - ur) / np.linalg.norm(ur))
+        out[name]["p_err"] = float(np.linalg.norm(p - pr) / np.linalg.norm(pr))
+    return {"workload": SOLVE_WORKLOAD, "unit": "s", "fp64_s": out["fp64"]["s"], "mixed_s": out["mixed"]["s"],
+            "speedup_mixed_vs_fp64": out["fp64"]["s"] / out["mixed"]["s"], "fp64": out["fp64"], "mixed": out["mixed"],
+            "oracle_solve": out["ref"]}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -296,6 +343,10 @@ def run_b200(args):
         except Exception as exc:  # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
 
+    solve = None
+    if rank == 0 and not args.no_solve:
+        solve = solve_leg(local)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
@@ -312,7 +363,10 @@ def run_b200(args):
                 "gpu_launches": launches,
                 "clocks": clk.summary(),
                 "fp32_apply": {"ms": f32_ms, "GDoF/s": ndof / (f32_ms * 1e-3) / 1e9,
-                               "hbm_frac": algorithmic_bytes(m, 4) / (f32_ms * 1e-3) / 1e9 / peak}}
+                               "hbm_frac": algorithmic_bytes(m, 4) / (f32_ms * 1e-3) / 1e9 / peak},
+                "fp64_alu": {"flop_per_element": REF_FLOPS_PER_EL,
+                             "TFLOP/s": REF_FLOPS_PER_EL * m ** 3 / (kern_ms * 1e-3) / 1e12},
+                "solve": solve}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -328,6 +382,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--no-solve", action="store_true", help="skip the FP64 vs mixed-precision Stokes solve leg")
     ap.add_argument("--size", type=int, default=96, help="elements per direction")
     ap.add_argument("--workload", default="deformed", choices=["deformed", "layered"])
     args = ap.parse_args()

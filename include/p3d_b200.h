@@ -159,13 +159,35 @@ typedef struct p3d_solver_opts {
   double cheb_hi;       /*   (the reference's -esteig 0,0.2,0,1.1)                  */
   int32_t esteig_its;   /* CG-Lanczos iterations estimating lmax(D^{-1}A)           */
   int32_t mg_precision; /* P3D_PREC_F64 or P3D_PREC_F32 (mixed precision)           */
-  int32_t restart;      /* FGMRES restart length (<= 38)                            */
+  int32_t restart;      /* FGMRES restart length (<= P3D_MAX_RESTART)               */
   int32_t max_it;       /* outer iteration limit                                    */
   double rtol;          /* ||r_k|| <= max(rtol*||r_0||, atol)                       */
   double atol;
   int32_t use_graph;    /* capture the preconditioner in a CUDA graph               */
   int32_t verbose;
+  int32_t inner_its;    /* velocity-block solve inside the preconditioner: 0 = one
+                           V-cycle; k > 0 = k conjugate-gradient iterations on A11
+                           preconditioned by the V-cycle (the reference's inner
+                           -fieldsplit_u_ksp, run for a fixed count so that it
+                           stays inside the captured graph)                       */
+  int32_t coarse_op;    /* operators of the coarse levels: P3D_COARSE_GALERKIN
+                           (P^T A P, 27-point block stencils probed from the
+                           finer level) or P3D_COARSE_REDISC (matrix-free
+                           rediscretisation with restricted viscosity)            */
+  int32_t schur_eta;    /* viscosity weighting of the pressure mass matrix in the
+                           Schur approximation: P3D_SCHUR_ETA_QP (1/eta at every
+                           quadrature point, the reference's ScaledMassMatrix) or
+                           P3D_SCHUR_ETA_GEOMEAN (1/eta_e, eta_e the element's
+                           geometric-mean viscosity)                              */
 } p3d_solver_opts;
+
+#define P3D_SCHUR_ETA_QP 0
+#define P3D_SCHUR_ETA_GEOMEAN 1
+#define P3D_COARSE_GALERKIN 0
+#define P3D_COARSE_REDISC 1
+
+#define P3D_MAX_RESTART 120   /* FGMRES basis vectors kept                        */
+#define P3D_COARSE_MAX_DOFS 16384 /* largest coarse level inverted densely        */
 
 typedef struct p3d_solve_stats {
   int32_t iterations;   /* outer FGMRES iterations                                  */
@@ -191,6 +213,9 @@ int p3d_solver_set_rhs(p3d_solver *s, const double *bu_dev, const double *bp_dev
 int p3d_solver_solve(p3d_solver *s, double *u_dev, double *p_dev, p3d_solve_stats *stats);
 /* One application of the block preconditioner (testing / external Krylov). */
 int p3d_solver_apply_pc(p3d_solver *s, const double *ru, const double *rp, double *zu, double *zp);
+/* y = A_l x with the FP64 velocity operator of multigrid level `level`
+ * (0 = coarsest), Dirichlet rows identity (testing the hierarchy). */
+int p3d_solver_level_apply(p3d_solver *s, int level, const double *x_dev, double *y_dev);
 int p3d_solver_destroy(p3d_solver *s);
 
 /* -------------------------------------------------------- diagnostics --- */

@@ -16,6 +16,10 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libp3d_b200
 P3D_OK = 0
 P3D_ERR_ARG, P3D_ERR_CUDA, P3D_ERR_STATE, P3D_ERR_NOMEM, P3D_ERR_NOCONV, P3D_ERR_BREAKDOWN, P3D_ERR_TIMEOUT = range(1, 8)
 PREC_F64, PREC_F32 = 64, 32
+COARSE_GALERKIN, COARSE_REDISC = 0, 1
+SCHUR_ETA_QP, SCHUR_ETA_GEOMEAN = 0, 1
+MAX_RESTART = 120
+COARSE_MAX_DOFS = 16384
 GEOM_AUTO, GEOM_GENERAL, GEOM_AFFINE = 0, 1, 2
 BC_NONE, BC_MATMULT = 0, 1
 FACE_IMIN, FACE_IMAX, FACE_JMIN, FACE_JMAX, FACE_KMIN, FACE_KMAX = range(6)
@@ -42,7 +46,8 @@ class SolverOpts(C.Structure):
     _fields_ = [("nlevels", C.c_int32), ("cheb_its", C.c_int32), ("cheb_lo", C.c_double), ("cheb_hi", C.c_double),
                 ("esteig_its", C.c_int32), ("mg_precision", C.c_int32), ("restart", C.c_int32),
                 ("max_it", C.c_int32), ("rtol", C.c_double), ("atol", C.c_double), ("use_graph", C.c_int32),
-                ("verbose", C.c_int32)]
+                ("verbose", C.c_int32), ("inner_its", C.c_int32), ("coarse_op", C.c_int32),
+                ("schur_eta", C.c_int32)]
 
 
 class SolveStats(C.Structure):
@@ -62,6 +67,7 @@ _SIGS = {
     "p3d_solver_solve": ([C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveStats)], C.c_int),
     "p3d_solver_apply_pc": ([C.c_void_p] * 5, C.c_int),
     "p3d_solver_destroy": ([C.c_void_p], C.c_int),
+    "p3d_solver_level_apply": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_last_error": ([], C.c_char_p),
     "p3d_kernel_launch_count": ([], C.c_int64),
     "p3d_version": ([], C.c_char_p),

@@ -2,7 +2,9 @@
 //
 //   s_schur_blocks : inverse of the viscosity-scaled pressure mass matrix,
 //                    dense 4x4 per element for P1disc
-//                    (src/stokes_assembly.c:299-450 assembles the same blocks)
+//                    (src/stokes_assembly.c:299-450 assembles the same blocks
+//                    with 1/eta per quadrature point; the element geometric
+//                    mean of eta is the alternative weighting)
 //   s_body_force   : velocity right-hand side from a density field and gravity,
 //                    b_(n,l) = sum_q w detJ N_n rho_q g_l (the body-force part of
 //                    FormFunctionLocal_U, src/stokes_form_function.c:99-243)
@@ -82,7 +84,7 @@ __device__ void gather_element(int mx, int my, size_t e, const double *coords, d
 }
 
 __global__ void k_schur_blocks(int mx, int my, int mz, const double *__restrict__ coords, const double *__restrict__ eta,
-                               double *__restrict__ Binv)
+                               int geomean, double *__restrict__ Binv)
 {
   size_t nel = (size_t)mx * my * mz;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nel; e += (size_t)gridDim.x * blockDim.x) {
@@ -94,10 +96,15 @@ __global__ void k_schur_blocks(int mx, int my, int mz, const double *__restrict_
     for (int l = 0; l < 3; l++) avg[l] /= 27.0;
     double L[3] = {X[14][0] - X[12][0], X[16][1] - X[10][1], X[22][2] - X[4][2]};
     double S[4][4] = {};
+    double eg = 0.0;
+    if (geomean) {
+      for (int q = 0; q < 27; q++) eg += log(eta[27 * e + q]);
+      eg = exp(eg / 27.0);
+    }
     for (int q = 0; q < 27; q++) {
       QPGeom g = qp_geom(X, q);
       double Np[4] = {1.0, (g.xq[0] - avg[0]) / L[0], (g.xq[1] - avg[1]) / L[1], (g.xq[2] - avg[2]) / L[2]};
-      double s = -g.w * g.detJ / eta[27 * e + q];
+      double s = -g.w * g.detJ / (geomean ? eg : eta[27 * e + q]);
       for (int i = 0; i < 4; i++)
         for (int j = 0; j < 4; j++) S[i][j] += s * Np[i] * Np[j];
     }
@@ -190,9 +197,10 @@ __global__ void k_inject(int cnx, int cny, int cnz, const double *__restrict__ c
   }
 }
 
-void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *eta, double *Binv, cudaStream_t s)
+void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *eta, int geomean, double *Binv,
+                    cudaStream_t s)
 {
-  k_schur_blocks<<<sgrid((size_t)mx * my * mz), 128, 0, s>>>(mx, my, mz, coords, eta, Binv);
+  k_schur_blocks<<<sgrid((size_t)mx * my * mz), 128, 0, s>>>(mx, my, mz, coords, eta, geomean, Binv);
   count_launch(1);
 }
 void s_body_force(int mx, int my, int mz, const double *coords, const double *rho, double g[3], double *bu, cudaStream_t s)

@@ -4,7 +4,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
-#define P3D_MDOT_MAX 40     // max vectors in one fused multi-dot (FGMRES restart + 1)
+#define P3D_MDOT_CHUNK 8    // vectors per multi-dot / multi-axpy launch (register accumulators)
 #define P3D_MDOT_BLOCKS 592 // 4 x 148 SMs
 
 namespace p3d {
@@ -22,14 +22,26 @@ template <typename T> void v_mask(int nx, int ny, int nz, uint32_t dir, T *v, cu
 template <typename T>
 void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s);
 template <typename T> void v_maxpy(size_t n, int k, const double *h, const T *const *V_dev, T *w, double sign, cudaStream_t s);
+template <typename T>
+void v_cg_xr(size_t n, const double *num, const double *den, T *x, T *r, const T *p, const T *q, bool update_r, cudaStream_t s);
+template <typename T> void v_cg_p(size_t n, const double *num, const double *den, const T *z, T *p, cudaStream_t s);
 void v_block4(size_t nel, const double *B, const double *x, double *y, double alpha, cudaStream_t s);
 void v_dense_mv(int n, const double *M, const double *x, double *y, cudaStream_t s);
 
 // setup_kernels.cu (whole-mesh lattices, FP64)
-void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *eta, double *Binv, cudaStream_t s);
+void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *eta, int geomean, double *Binv,
+                    cudaStream_t s);
 void s_body_force(int mx, int my, int mz, const double *coords, const double *rho, double g[3], double *bu, cudaStream_t s);
 void s_restrict_eta(int mxc, int myc, int mzc, const double *eta_f, double *eta_c, cudaStream_t s);
 void s_inject_coords(int cnx, int cny, int cnz, const double *cf, double *cc, cudaStream_t s);
+
+// galerkin.cu (27-point block-stencil coarse operators)
+template <typename T> void g_apply(int nx, int ny, int nz, const T *G, const T *x, T *y, cudaStream_t s);
+void g_probe_vec(int nx, int ny, int nz, int ci, int cj, int ck, int d, uint32_t dir, double *x, cudaStream_t s);
+void g_probe_scatter(int nx, int ny, int nz, int ci, int cj, int ck, int d, const double *y, double *G, cudaStream_t s);
+void g_dirichlet(int nx, int ny, int nz, uint32_t dir, double *G, cudaStream_t s);
+void g_diag(int nx, int ny, int nz, const double *G, double *d, cudaStream_t s);
+void g_dense(int nx, int ny, int nz, const double *G, double *M, cudaStream_t s);
 
 // mg_transfer.cu
 template <typename T> int mg_prolong(int cnx, int cny, int cnz, int ndof, const T *xc, T *xf, cudaStream_t st);

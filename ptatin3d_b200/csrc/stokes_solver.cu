@@ -33,6 +33,9 @@ struct Level {
   double *coords = nullptr, *eta = nullptr;
   double *dinv = nullptr;        // FP64 inverse diagonal (Dirichlet slots 1)
   double lmax = 0.0;
+  bool gal = false;              // Galerkin level: 27-point block stencil instead of a matrix-free operator
+  double *G64 = nullptr;         // stencil coefficients (FP64, always kept)
+  float *G32 = nullptr;          // FP32 copy (mixed mode smoothing)
   void *b = nullptr, *x = nullptr, *r = nullptr, *d = nullptr, *t = nullptr; // MG precision work vectors
 };
 
@@ -54,9 +57,14 @@ struct p3d_solver {
   double *bvec = nullptr; // rhs [bu; bp]
   // FGMRES
   double *V = nullptr, *Z = nullptr, *w = nullptr;
-  double **Vptr = nullptr; // device array of pointers to V_j
+  double **Vptr = nullptr; // device array of pointers: V_0..V_m, then one scratch slot
   double *part = nullptr, *hdev = nullptr;
-  double *hhost = nullptr; // pinned
+  double *hhost = nullptr; // pinned; [0,hs) and [hs,2hs) Gram-Schmidt passes, 2hs norm
+  int hs = 0;              // restart + 1
+  // inner conjugate gradient on A11 (MG precision vectors, device-held scalars)
+  void *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_q = nullptr;
+  void **cg_ptr = nullptr; // device pointers {p, r} for the dot kernels
+  double *cg_sc = nullptr; // {rz (2 slots, alternating), pq}
   // preconditioner buffers (fixed for graph capture)
   double *pc_in = nullptr, *pc_out = nullptr, *pc_t = nullptr;
   cudaGraph_t graph = nullptr;
@@ -84,6 +92,10 @@ static uint32_t level_dir(const p3d_solver *s) { return s->mesh.dirichlet; }
 // y = A11 x on level l in precision T (BC_MATMULT), y overwritten
 template <typename T> static int a11(p3d_solver *s, Level &L, const T *x, T *y)
 {
+  if (L.gal) {
+    g_apply<T>(L.n[0], L.n[1], L.n[2], sizeof(T) == 8 ? (const T *)L.G64 : (const T *)L.G32, x, y, s->st);
+    return P3D_OK;
+  }
   CU(cudaMemsetAsync(y, 0, L.nv * sizeof(T), s->st), "memset");
   p3d_op *op = sizeof(T) == 8 ? L.op64 : L.op32;
   return launch_a11<T>(op, x, y, s->st);
@@ -155,6 +167,43 @@ template <typename T> static int vcycle(p3d_solver *s, int l, const T *b, T *x)
   return P3D_OK;
 }
 
+// Velocity block of the preconditioner, x ~ A11^{-1} b on the finest level.
+// inner_its = 0: one V-cycle.  inner_its = k: k iterations of conjugate
+// gradients preconditioned by the V-cycle (a symmetric positive definite
+// operator: Chebyshev pre/post smoothing with the same polynomial and an exact
+// coarse solve), x_0 = 0.  The step lengths never leave the device, so the
+// whole solve is one captured graph.  b may be overwritten (it is the CG
+// residual when it aliases cg_r).
+template <typename T> static int velocity_solve(p3d_solver *s, const T *b, T *x)
+{
+  const int top = (int)s->lv.size() - 1;
+  const int K = s->o.inner_its;
+  if (K <= 0) return vcycle<T>(s, top, b, x);
+  Level &F = s->lv.back();
+  const size_t n = F.nv;
+  T *r = (T *)s->cg_r, *z = (T *)s->cg_z, *p = (T *)s->cg_p, *q = (T *)s->cg_q;
+  const T *const *pp = (const T *const *)s->cg_ptr;     // {p}
+  const T *const *pr = (const T *const *)s->cg_ptr + 1; // {r}
+  double *sc = s->cg_sc;
+  if ((const void *)b != (const void *)r) CU(cudaMemcpyAsync(r, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s->st), "copy");
+  CU(cudaMemsetAsync(x, 0, n * sizeof(T), s->st), "memset");
+  CK(vcycle<T>(s, top, r, z));
+  CU(cudaMemcpyAsync(p, z, n * sizeof(T), cudaMemcpyDeviceToDevice, s->st), "copy");
+  v_mdot<T>(n, 1, pr, z, s->part, sc + 0, s->st); // rz
+  for (int k = 0; k < K; k++) {
+    double *rz = sc + (k & 1), *rz_new = sc + ((k + 1) & 1), *pq = sc + 2;
+    CK(a11<T>(s, F, p, q));
+    v_mdot<T>(n, 1, pp, q, s->part, pq, s->st);
+    const bool last = k == K - 1;
+    v_cg_xr<T>(n, rz, pq, x, r, p, q, !last, s->st);
+    if (last) break;
+    CK(vcycle<T>(s, top, r, z));
+    v_mdot<T>(n, 1, pr, z, s->part, rz_new, s->st);
+    v_cg_p<T>(n, rz_new, rz, z, p, s->st);
+  }
+  return P3D_OK;
+}
+
 // block upper-triangular preconditioner: zp = S^{-1} rp ; zu = MG(ru - A12 zp)
 static int apply_pc(p3d_solver *s, const double *in, double *out)
 {
@@ -167,10 +216,10 @@ static int apply_pc(p3d_solver *s, const double *in, double *out)
   CK((launch_general<double, false, true, false>(F.op64, nullptr, zp, t, nullptr, s->st)));
   v_axpby<double>(s->nu, 1.0, ru, -1.0, t, s->st); // t = ru - A12 zp
   if (s->o.mg_precision == P3D_PREC_F64) {
-    CK(vcycle<double>(s, (int)s->lv.size() - 1, t, zu));
+    CK(velocity_solve<double>(s, t, zu));
   } else {
-    v_convert<double, float>(s->nu, t, (float *)F.b, s->st);
-    CK(vcycle<float>(s, (int)s->lv.size() - 1, (const float *)F.b, (float *)F.x));
+    v_convert<double, float>(s->nu, t, (float *)s->cg_r, s->st);
+    CK(velocity_solve<float>(s, (const float *)s->cg_r, (float *)F.x));
     v_convert<float, double>(s->nu, (const float *)F.x, zu, s->st);
   }
   return P3D_OK;
@@ -199,11 +248,12 @@ static int stokes_op(p3d_solver *s, const double *x, double *y)
 // ||v||_2 (FP64)
 static int norm2(p3d_solver *s, const double *v, size_t n, double *out)
 {
-  CU(cudaMemcpyAsync(s->Vptr + P3D_MDOT_MAX - 1, &v, sizeof(double *), cudaMemcpyHostToDevice, s->st), "ptr");
-  v_mdot<double>(n, 1, (const double *const *)(s->Vptr + P3D_MDOT_MAX - 1), v, s->part, s->hdev + 2 * P3D_MDOT_MAX, s->st);
-  CU(cudaMemcpyAsync(s->hhost + 2 * P3D_MDOT_MAX, s->hdev + 2 * P3D_MDOT_MAX, 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+  const int slot = s->hs, h = 2 * s->hs;
+  CU(cudaMemcpyAsync(s->Vptr + slot, &v, sizeof(double *), cudaMemcpyHostToDevice, s->st), "ptr");
+  v_mdot<double>(n, 1, (const double *const *)(s->Vptr + slot), v, s->part, s->hdev + h, s->st);
+  CU(cudaMemcpyAsync(s->hhost + h, s->hdev + h, 8, cudaMemcpyDeviceToHost, s->st), "d2h");
   CU(cudaStreamSynchronize(s->st), "sync");
-  *out = std::sqrt(std::max(0.0, s->hhost[2 * P3D_MDOT_MAX]));
+  *out = std::sqrt(std::max(0.0, s->hhost[h]));
   return P3D_OK;
 }
 
@@ -255,11 +305,12 @@ static int estimate_lmax(p3d_solver *s, Level &L)
   CU(cudaMemcpyAsync(p, z, n * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
   auto dot = [&](const double *a, const double *b, double *out) -> int {
     const double *ptrs[1] = {a};
-    CU(cudaMemcpyAsync(s->Vptr + P3D_MDOT_MAX - 1, ptrs, sizeof(double *), cudaMemcpyHostToDevice, s->st), "ptr");
-    v_mdot<double>(n, 1, (const double *const *)(s->Vptr + P3D_MDOT_MAX - 1), b, s->part, s->hdev, s->st);
-    CU(cudaMemcpyAsync(s->hhost, s->hdev, 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+    const int slot = s->hs, h = 2 * s->hs;
+    CU(cudaMemcpyAsync(s->Vptr + slot, ptrs, sizeof(double *), cudaMemcpyHostToDevice, s->st), "ptr");
+    v_mdot<double>(n, 1, (const double *const *)(s->Vptr + slot), b, s->part, s->hdev + h, s->st);
+    CU(cudaMemcpyAsync(s->hhost + h, s->hdev + h, 8, cudaMemcpyDeviceToHost, s->st), "d2h");
     CU(cudaStreamSynchronize(s->st), "sync");
-    *out = s->hhost[0];
+    *out = s->hhost[h];
     return P3D_OK;
   };
   double rz;
@@ -345,7 +396,10 @@ static int build_coarse(p3d_solver *s)
             isdir[3 * ((size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k)) + c] = d;
           }
   }
-  if (s->lv.size() == 1) {
+  if (C.gal) {
+    CU(cudaMemsetAsync(s->cinv, 0, (size_t)nc * nc * 8, s->st), "memset");
+    g_dense(C.n[0], C.n[1], C.n[2], C.G64, s->cinv, s->st);
+  } else if (s->lv.size() == 1) {
     // single level: probe the operator itself
     for (int j = 0; j < nc; j++) {
       double *e = s->cb64;
@@ -392,14 +446,44 @@ static int build_coarse(p3d_solver *s)
   return rc;
 }
 
+// Galerkin operator of level l from level l+1: Ac = P~^T A P~ (P~ = P with
+// Dirichlet rows and columns removed) + identity on the Dirichlet dofs, probed
+// with the 81 colour/component vectors.
+static int build_galerkin(p3d_solver *s, int l)
+{
+  Level &C = s->lv[l], &F = s->lv[l + 1];
+  const uint32_t dir = level_dir(s);
+  const size_t nn = (size_t)C.n[0] * C.n[1] * C.n[2];
+  if (!C.G64) CK(dev_alloc((void **)&C.G64, 243 * nn * 8, "galerkin stencil"));
+  CU(cudaMemsetAsync(C.G64, 0, 243 * nn * 8, s->st), "memset");
+  double *xc = (double *)C.x, *yc = (double *)C.r, *xf = (double *)F.b, *yf = (double *)F.t;
+  for (int ck = 0; ck < 3; ck++)
+    for (int cj = 0; cj < 3; cj++)
+      for (int ci = 0; ci < 3; ci++)
+        for (int d = 0; d < 3; d++) {
+          g_probe_vec(C.n[0], C.n[1], C.n[2], ci, cj, ck, d, dir, xc, s->st);
+          CK(mg_prolong<double>(C.n[0], C.n[1], C.n[2], 3, xc, xf, s->st));
+          v_mask<double>(F.n[0], F.n[1], F.n[2], dir, xf, s->st);
+          CK(a11<double>(s, F, xf, yf));
+          v_mask<double>(F.n[0], F.n[1], F.n[2], dir, yf, s->st);
+          CK(mg_restrict<double>(C.n[0], C.n[1], C.n[2], 3, yf, yc, s->st));
+          v_mask<double>(C.n[0], C.n[1], C.n[2], dir, yc, s->st);
+          g_probe_scatter(C.n[0], C.n[1], C.n[2], ci, cj, ck, d, yc, C.G64, s->st);
+        }
+  g_dirichlet(C.n[0], C.n[1], C.n[2], dir, C.G64, s->st);
+  return cuda_check(cudaStreamSynchronize(s->st), "galerkin");
+}
+
 static void free_level(Level &L)
 {
   p3d_op_destroy(L.op64);
   p3d_op_destroy(L.op32);
   L.op64 = L.op32 = nullptr;
-  for (void *p : {(void *)L.coords, (void *)L.eta, (void *)L.dinv, L.b, L.x, L.r, L.d, L.t})
+  for (void *p : {(void *)L.coords, (void *)L.eta, (void *)L.dinv, L.b, L.x, L.r, L.d, L.t, (void *)L.G64, (void *)L.G32})
     if (p) cudaFree(p);
   L.coords = L.eta = L.dinv = nullptr;
+  L.G64 = nullptr;
+  L.G32 = nullptr;
   L.b = L.x = L.r = L.d = L.t = nullptr;
 }
 
@@ -408,39 +492,47 @@ static int solver_setup(p3d_solver *s, const double *coords, const double *eta)
   double t0 = now_ms();
   const int nlev = (int)s->lv.size();
   const bool mixed = s->o.mg_precision == P3D_PREC_F32;
-  const size_t es = mixed ? 4 : 8;
   // hierarchy: finest first
   for (int l = nlev - 1; l >= 0; l--) {
     Level &L = s->lv[l];
     size_t nn = (size_t)L.n[0] * L.n[1] * L.n[2], nel = (size_t)L.m[0] * L.m[1] * L.m[2];
-    if (!L.coords) CK(dev_alloc((void **)&L.coords, 3 * nn * 8, "level coords"));
-    if (!L.eta) CK(dev_alloc((void **)&L.eta, 27 * nel * 8, "level eta"));
-    if (l == nlev - 1) {
-      CU(cudaMemcpyAsync(L.coords, coords, 3 * nn * 8, cudaMemcpyDeviceToDevice, s->st), "coords");
-      CU(cudaMemcpyAsync(L.eta, eta, 27 * nel * 8, cudaMemcpyDeviceToDevice, s->st), "eta");
-    } else {
-      Level &F = s->lv[l + 1];
-      s_inject_coords(L.n[0], L.n[1], L.n[2], F.coords, L.coords, s->st);
-      s_restrict_eta(L.m[0], L.m[1], L.m[2], F.eta, L.eta, s->st);
-    }
-    CU(cudaStreamSynchronize(s->st), "hierarchy");
-    p3d_mesh_desc d;
-    p3d_mesh_desc_whole(L.m[0], L.m[1], L.m[2], s->mesh.dirichlet, &d);
-    if (!L.op64) CK(p3d_op_create(&d, P3D_PREC_F64, s->device, &L.op64));
-    CK(p3d_op_set_coefficients_device(L.op64, L.coords, L.eta, P3D_GEOM_AUTO));
-    CK(p3d_op_set_bc_mode(L.op64, P3D_BC_MATMULT));
-    if (mixed && l > 0) {
-      if (!L.op32) CK(p3d_op_create(&d, P3D_PREC_F32, s->device, &L.op32));
-      CK(p3d_op_set_coefficients_device(L.op32, L.coords, L.eta, P3D_GEOM_AUTO));
-      CK(p3d_op_set_bc_mode(L.op32, P3D_BC_MATMULT));
-    }
+    L.gal = l < nlev - 1 && s->o.coarse_op == P3D_COARSE_GALERKIN;
     // work vectors: FP64 for esteig/Galerkin probing, reused as MG-precision vectors
     for (void **p : {&L.b, &L.x, &L.r, &L.d, &L.t})
       if (!*p) CK(dev_alloc(p, L.nv * 8, "level vector"));
-    (void)es;
     if (!L.dinv) CK(dev_alloc((void **)&L.dinv, L.nv * 8, "dinv"));
-    CU(cudaMemsetAsync(L.t, 0, L.nv * 8, s->st), "memset");
-    CK(launch_diag<double>(L.op64, (double *)L.t, s->st));
+    if (L.gal) {
+      CK(build_galerkin(s, l));
+      g_diag(L.n[0], L.n[1], L.n[2], L.G64, (double *)L.t, s->st);
+      if (mixed && l > 0) {
+        if (!L.G32) CK(dev_alloc((void **)&L.G32, 243 * nn * 4, "galerkin stencil f32"));
+        v_convert<double, float>(243 * nn, L.G64, L.G32, s->st);
+      }
+    } else {
+      if (!L.coords) CK(dev_alloc((void **)&L.coords, 3 * nn * 8, "level coords"));
+      if (!L.eta) CK(dev_alloc((void **)&L.eta, 27 * nel * 8, "level eta"));
+      if (l == nlev - 1) {
+        CU(cudaMemcpyAsync(L.coords, coords, 3 * nn * 8, cudaMemcpyDeviceToDevice, s->st), "coords");
+        CU(cudaMemcpyAsync(L.eta, eta, 27 * nel * 8, cudaMemcpyDeviceToDevice, s->st), "eta");
+      } else {
+        Level &F = s->lv[l + 1];
+        s_inject_coords(L.n[0], L.n[1], L.n[2], F.coords, L.coords, s->st);
+        s_restrict_eta(L.m[0], L.m[1], L.m[2], F.eta, L.eta, s->st);
+      }
+      CU(cudaStreamSynchronize(s->st), "hierarchy");
+      p3d_mesh_desc d;
+      p3d_mesh_desc_whole(L.m[0], L.m[1], L.m[2], s->mesh.dirichlet, &d);
+      if (!L.op64) CK(p3d_op_create(&d, P3D_PREC_F64, s->device, &L.op64));
+      CK(p3d_op_set_coefficients_device(L.op64, L.coords, L.eta, P3D_GEOM_AUTO));
+      CK(p3d_op_set_bc_mode(L.op64, P3D_BC_MATMULT));
+      if (mixed && l > 0) {
+        if (!L.op32) CK(p3d_op_create(&d, P3D_PREC_F32, s->device, &L.op32));
+        CK(p3d_op_set_coefficients_device(L.op32, L.coords, L.eta, P3D_GEOM_AUTO));
+        CK(p3d_op_set_bc_mode(L.op32, P3D_BC_MATMULT));
+      }
+      CU(cudaMemsetAsync(L.t, 0, L.nv * 8, s->st), "memset");
+      CK(launch_diag<double>(L.op64, (double *)L.t, s->st));
+    }
     // dinv = 1 / diag
     std::vector<double> hd(L.nv);
     CU(cudaMemcpyAsync(hd.data(), L.t, L.nv * 8, cudaMemcpyDeviceToHost, s->st), "d2h diag");
@@ -457,7 +549,7 @@ static int solver_setup(p3d_solver *s, const double *coords, const double *eta)
   Level &F = s->lv.back();
   size_t nel = (size_t)F.m[0] * F.m[1] * F.m[2];
   if (!s->Binv) CK(dev_alloc((void **)&s->Binv, 16 * nel * 8, "schur blocks"));
-  s_schur_blocks(F.m[0], F.m[1], F.m[2], F.coords, F.eta, s->Binv, s->st);
+  s_schur_blocks(F.m[0], F.m[1], F.m[2], F.coords, F.eta, s->o.schur_eta == P3D_SCHUR_ETA_GEOMEAN, s->Binv, s->st);
   CU(cudaStreamSynchronize(s->st), "schur");
   // preconditioner graph
   if (s->o.use_graph) {
@@ -513,11 +605,11 @@ static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
       for (int pass = 0; pass < 2; pass++) {
         v_mdot<double>(N, j + 1, (const double *const *)s->Vptr, w, s->part, s->hdev, s->st);
         v_maxpy<double>(N, j + 1, s->hdev, (const double *const *)s->Vptr, w, -1.0, s->st);
-        CU(cudaMemcpyAsync(s->hhost + pass * P3D_MDOT_MAX, s->hdev, (j + 1) * 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+        CU(cudaMemcpyAsync(s->hhost + pass * s->hs, s->hdev, (j + 1) * 8, cudaMemcpyDeviceToHost, s->st), "d2h");
       }
       double hn;
       CK(norm2(s, w, N, &hn)); // synchronizes
-      for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = s->hhost[i] + s->hhost[P3D_MDOT_MAX + i];
+      for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = s->hhost[i] + s->hhost[s->hs + i];
       H[(size_t)(j + 1) * m + j] = hn;
       if (hn > 0) {
         CU(cudaMemcpyAsync(vn, w, N * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
@@ -584,6 +676,9 @@ int p3d_solver_default_opts(p3d_solver_opts *o)
   o->atol = 0.0;
   o->use_graph = 1;
   o->verbose = 0;
+  o->inner_its = 0;
+  o->coarse_op = P3D_COARSE_GALERKIN;
+  o->schur_eta = P3D_SCHUR_ETA_QP;
   return P3D_OK;
 }
 
@@ -597,13 +692,21 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
   if (mesh->ox || mesh->oy || mesh->oz || mesh->gx != 2 * mesh->mx + 1 || mesh->gy != 2 * mesh->my + 1 ||
       mesh->gz != 2 * mesh->mz + 1)
     return set_error(P3D_ERR_ARG, "solver_create: the solver takes a whole mesh (no ghost layers)");
-  if (o.nlevels < 1 || o.restart < 1 || o.restart > P3D_MDOT_MAX - 2 || o.max_it < 1 || o.cheb_its < 1 ||
-      !(o.cheb_hi > o.cheb_lo) || o.cheb_lo <= 0 || (o.mg_precision != 64 && o.mg_precision != 32))
+  if (o.nlevels < 1 || o.nlevels > 12 || o.restart < 1 || o.restart > P3D_MAX_RESTART || o.max_it < 1 ||
+      o.cheb_its < 1 || !(o.cheb_hi > o.cheb_lo) || o.cheb_lo <= 0 || (o.mg_precision != 64 && o.mg_precision != 32) ||
+      o.inner_its < 0 || o.inner_its > 1000 || (o.coarse_op != P3D_COARSE_GALERKIN && o.coarse_op != P3D_COARSE_REDISC) ||
+      (o.schur_eta != P3D_SCHUR_ETA_QP && o.schur_eta != P3D_SCHUR_ETA_GEOMEAN))
     return set_error(P3D_ERR_ARG, "solver_create: bad options");
   int f = 1 << (o.nlevels - 1);
   if (mesh->mx % f || mesh->my % f || mesh->mz % f)
     return set_error(P3D_ERR_ARG, "solver_create: %dx%dx%d not divisible by 2^(nlevels-1)=%d", mesh->mx, mesh->my,
                      mesh->mz, f);
+  {
+    const long long cdofs = 3ll * (2 * (mesh->mx / f) + 1) * (2 * (mesh->my / f) + 1) * (2 * (mesh->mz / f) + 1);
+    if (cdofs > P3D_COARSE_MAX_DOFS)
+      return set_error(P3D_ERR_ARG, "solver_create: coarse level of %lld dofs exceeds the dense limit %d (add levels)",
+                       cdofs, P3D_COARSE_MAX_DOFS);
+  }
   CK(cuda_check(cudaSetDevice(device), "cudaSetDevice"));
   p3d_solver *s = new p3d_solver();
   s->mesh = *mesh;
@@ -631,14 +734,29 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
   if (!rc) rc = dev_alloc((void **)&s->pc_in, N * 8, "pc in");
   if (!rc) rc = dev_alloc((void **)&s->pc_out, N * 8, "pc out");
   if (!rc) rc = dev_alloc((void **)&s->pc_t, s->nu * 8, "pc t");
-  if (!rc) rc = dev_alloc((void **)&s->Vptr, P3D_MDOT_MAX * sizeof(double *), "V ptrs");
-  if (!rc) rc = dev_alloc((void **)&s->part, (size_t)P3D_MDOT_BLOCKS * P3D_MDOT_MAX * 8, "partials");
-  if (!rc) rc = dev_alloc((void **)&s->hdev, 3 * P3D_MDOT_MAX * 8, "h");
-  if (!rc) rc = cuda_check(cudaMallocHost((void **)&s->hhost, 3 * P3D_MDOT_MAX * 8), "pinned h");
+  s->hs = m + 1;
+  if (!rc) rc = dev_alloc((void **)&s->Vptr, (size_t)(m + 2) * sizeof(double *), "V ptrs");
+  if (!rc) rc = dev_alloc((void **)&s->part, (size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK * 8, "partials");
+  if (!rc) rc = dev_alloc((void **)&s->hdev, (size_t)(2 * s->hs + 2) * 8, "h");
+  if (!rc) rc = cuda_check(cudaMallocHost((void **)&s->hhost, (size_t)(2 * s->hs + 2) * 8), "pinned h");
   if (!rc) {
-    std::vector<double *> ptrs(P3D_MDOT_MAX, nullptr);
+    std::vector<double *> ptrs(m + 2, nullptr);
     for (int j = 0; j <= m; j++) ptrs[j] = s->V + (size_t)j * N;
-    rc = cuda_check(cudaMemcpy(s->Vptr, ptrs.data(), P3D_MDOT_MAX * sizeof(double *), cudaMemcpyHostToDevice), "ptrs");
+    rc = cuda_check(cudaMemcpy(s->Vptr, ptrs.data(), (m + 2) * sizeof(double *), cudaMemcpyHostToDevice), "ptrs");
+  }
+  // velocity-solve vectors (sized for FP64; the mixed path uses them as FP32)
+  if (!rc) rc = dev_alloc(&s->cg_r, s->nu * 8, "cg r");
+  if (!rc && o.inner_its > 0) {
+    rc = dev_alloc(&s->cg_z, s->nu * 8, "cg z");
+    if (!rc) rc = dev_alloc(&s->cg_p, s->nu * 8, "cg p");
+    if (!rc) rc = dev_alloc(&s->cg_q, s->nu * 8, "cg q");
+    if (!rc) rc = dev_alloc((void **)&s->cg_ptr, 2 * sizeof(void *), "cg ptrs");
+    if (!rc) rc = dev_alloc((void **)&s->cg_sc, 4 * 8, "cg scalars");
+    if (!rc) {
+      void *ptrs[2] = {s->cg_p, s->cg_r};
+      rc = cuda_check(cudaMemcpy(s->cg_ptr, ptrs, sizeof ptrs, cudaMemcpyHostToDevice), "cg ptrs");
+    }
+    if (!rc) rc = cuda_check(cudaMemset(s->cg_sc, 0, 4 * 8), "cg scalars");
   }
   if (!rc) rc = cuda_check(cudaMemset(s->bvec, 0, N * 8), "rhs zero");
   if (rc) {
@@ -719,6 +837,16 @@ int p3d_solver_apply_pc(p3d_solver *s, const double *ru, const double *rp, doubl
   return cuda_check(cudaStreamSynchronize(s->st), "apply_pc");
 }
 
+int p3d_solver_level_apply(p3d_solver *s, int level, const double *x, double *y)
+{
+  if (!s || !x || !y) return set_error(P3D_ERR_ARG, "level_apply: null argument");
+  if (!s->setup_done) return set_error(P3D_ERR_STATE, "level_apply before setup");
+  if (level < 0 || level >= (int)s->lv.size()) return set_error(P3D_ERR_ARG, "level_apply: no level %d", level);
+  cudaSetDevice(s->device);
+  CK(a11<double>(s, s->lv[level], x, y));
+  return cuda_check(cudaStreamSynchronize(s->st), "level_apply");
+}
+
 int p3d_solver_destroy(p3d_solver *s)
 {
   if (!s) return P3D_OK;
@@ -729,7 +857,8 @@ int p3d_solver_destroy(p3d_solver *s)
   for (auto &L : s->lv) free_level(L);
   for (void *p : {(void *)s->cinv, (void *)s->cb64, (void *)s->cx64, (void *)s->Binv, (void *)s->bvec, (void *)s->V,
                   (void *)s->Z, (void *)s->w, (void *)s->Vptr, (void *)s->part, (void *)s->hdev, (void *)s->pc_in,
-                  (void *)s->pc_out, (void *)s->pc_t})
+                  (void *)s->pc_out, (void *)s->pc_t, s->cg_r, s->cg_z, s->cg_p, s->cg_q, (void *)s->cg_ptr,
+                  (void *)s->cg_sc})
     if (p) cudaFree(p);
   if (s->hhost) cudaFreeHost(s->hhost);
   if (s->st) cudaStreamDestroy(s->st);

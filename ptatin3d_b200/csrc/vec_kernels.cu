@@ -80,29 +80,37 @@ __global__ void k_mask(int nx, int ny, int nz, uint32_t dir, T *__restrict__ v)
   }
 }
 
-// partial dot products  part[blk*k + j] = sum_i V_j[i] w[i]   (FP64 accumulation)
-template <typename T>
-__global__ void k_mdot_partial(size_t n, int k, const T *const *__restrict__ V, const T *__restrict__ w, double *__restrict__ part)
+// partial dot products  part[blk*KC + j] = sum_i V_j[i] w[i]   (FP64 accumulation),
+// KC vectors per launch so that the accumulators stay in registers
+template <typename T, int KC>
+__global__ void k_mdot_partial(size_t n, const T *const *__restrict__ V, const T *__restrict__ w, double *__restrict__ part)
 {
-  __shared__ double red[32][P3D_MDOT_MAX];
-  double acc[P3D_MDOT_MAX];
-  for (int j = 0; j < k; j++) acc[j] = 0.0;
+  __shared__ double red[32][KC];
+  const T *v[KC];
+  double acc[KC];
+#pragma unroll
+  for (int j = 0; j < KC; j++) {
+    v[j] = V[j];
+    acc[j] = 0.0;
+  }
   GS_LOOP(i, n)
   {
     double wi = (double)w[i];
-    for (int j = 0; j < k; j++) acc[j] += (double)V[j][i] * wi;
+#pragma unroll
+    for (int j = 0; j < KC; j++) acc[j] += (double)v[j][i] * wi;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int j = 0; j < k; j++) {
-    double v = acc[j];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) red[warp][j] = v;
+#pragma unroll
+  for (int j = 0; j < KC; j++) {
+    double x = acc[j];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[warp][j] = x;
   }
   __syncthreads();
-  if (threadIdx.x < k) {
-    double s = 0.0;
-    for (int q = 0; q < nw; q++) s += red[q][threadIdx.x];
-    part[(size_t)blockIdx.x * k + threadIdx.x] = s;
+  if (threadIdx.x < KC) {
+    double x = 0.0;
+    for (int q = 0; q < nw; q++) x += red[q][threadIdx.x];
+    part[(size_t)blockIdx.x * KC + threadIdx.x] = x;
   }
 }
 __global__ void k_sum_partials(int nblk, int k, const double *__restrict__ part, double *__restrict__ out)
@@ -114,16 +122,49 @@ __global__ void k_sum_partials(int nblk, int k, const double *__restrict__ part,
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if (threadIdx.x == 0) out[j] = s;
 }
-// w -= sum_j h_j V_j   (h on device)
-template <typename T>
-__global__ void k_maxpy(size_t n, int k, const double *__restrict__ h, const T *const *__restrict__ V, T *__restrict__ w, double sign)
+// w += sign * sum_j h_j V_j   (h on device), KC vectors per launch
+template <typename T, int KC>
+__global__ void k_maxpy(size_t n, const double *__restrict__ h, const T *const *__restrict__ V, T *__restrict__ w, double sign)
 {
+  const T *v[KC];
+  double c[KC];
+#pragma unroll
+  for (int j = 0; j < KC; j++) {
+    v[j] = V[j];
+    c[j] = sign * h[j];
+  }
   GS_LOOP(i, n)
   {
-    double s = 0.0;
-    for (int j = 0; j < k; j++) s += h[j] * (double)V[j][i];
-    w[i] = (T)((double)w[i] + sign * s);
+    double s = (double)w[i];
+#pragma unroll
+    for (int j = 0; j < KC; j++) s += c[j] * (double)v[j][i];
+    w[i] = (T)s;
   }
+}
+
+// Conjugate-gradient updates with the step lengths held on the device (so a
+// fixed number of CG iterations can be captured in a CUDA graph):
+//   alpha = num/den ; x += alpha p ; r -= alpha q (when update_r)
+template <typename T>
+__global__ void k_cg_xr(size_t n, const double *__restrict__ num, const double *__restrict__ den, T *__restrict__ x,
+                        T *__restrict__ r, const T *__restrict__ p, const T *__restrict__ q, int update_r)
+{
+  const double d = *den, a0 = *num / d;
+  const double a = (d > 0.0 && isfinite(a0)) ? a0 : 0.0; // breakdown: leave x, r unchanged
+  GS_LOOP(i, n)
+  {
+    x[i] = (T)((double)x[i] + a * (double)p[i]);
+    if (update_r) r[i] = (T)((double)r[i] - a * (double)q[i]);
+  }
+}
+//   beta = num/den ; p = z + beta p
+template <typename T>
+__global__ void k_cg_p(size_t n, const double *__restrict__ num, const double *__restrict__ den, const T *__restrict__ z,
+                       T *__restrict__ p)
+{
+  const double d = *den, b0 = *num / d;
+  const double b = (d != 0.0 && isfinite(b0)) ? b0 : 0.0;
+  GS_LOOP(i, n) p[i] = (T)((double)z[i] + b * (double)p[i]);
 }
 
 // y = blockdiag(B_e) x  with B_e 4x4 per element (Schur approximation inverse)
@@ -192,16 +233,60 @@ template <typename T> void v_mask(int nx, int ny, int nz, uint32_t dir, T *v, cu
   k_mask<<<vgrid((size_t)nx * ny * nz), 256, 0, s>>>(nx, ny, nz, dir, v);
   count_launch(1);
 }
+template <typename T, int KC> static void mdot_chunk(size_t n, const T *const *V_dev, const T *w, double *part, double *out, cudaStream_t s)
+{
+  k_mdot_partial<T, KC><<<P3D_MDOT_BLOCKS, 256, 0, s>>>(n, V_dev, w, part);
+  k_sum_partials<<<KC, 32, 0, s>>>(P3D_MDOT_BLOCKS, KC, part, out);
+  count_launch(2);
+}
 template <typename T>
 void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s)
 {
-  k_mdot_partial<<<P3D_MDOT_BLOCKS, 256, 0, s>>>(n, k, V_dev, w, part);
-  k_sum_partials<<<k, 32, 0, s>>>(P3D_MDOT_BLOCKS, k, part, out_dev);
-  count_launch(2);
+  for (int j0 = 0; j0 < k; j0 += P3D_MDOT_CHUNK) {
+    const int kc = k - j0 < P3D_MDOT_CHUNK ? k - j0 : P3D_MDOT_CHUNK;
+    const T *const *V = V_dev + j0;
+    double *o = out_dev + j0;
+    switch (kc) {
+    case 1: mdot_chunk<T, 1>(n, V, w, part, o, s); break;
+    case 2: mdot_chunk<T, 2>(n, V, w, part, o, s); break;
+    case 3: mdot_chunk<T, 3>(n, V, w, part, o, s); break;
+    case 4: mdot_chunk<T, 4>(n, V, w, part, o, s); break;
+    case 5: mdot_chunk<T, 5>(n, V, w, part, o, s); break;
+    case 6: mdot_chunk<T, 6>(n, V, w, part, o, s); break;
+    case 7: mdot_chunk<T, 7>(n, V, w, part, o, s); break;
+    default: mdot_chunk<T, 8>(n, V, w, part, o, s); break;
+    }
+  }
 }
 template <typename T> void v_maxpy(size_t n, int k, const double *h, const T *const *V_dev, T *w, double sign, cudaStream_t s)
 {
-  k_maxpy<<<vgrid(n), 256, 0, s>>>(n, k, h, V_dev, w, sign);
+  for (int j0 = 0; j0 < k; j0 += P3D_MDOT_CHUNK) {
+    const int kc = k - j0 < P3D_MDOT_CHUNK ? k - j0 : P3D_MDOT_CHUNK;
+    const double *hh = h + j0;
+    const T *const *V = V_dev + j0;
+    const int g = vgrid(n);
+    switch (kc) {
+    case 1: k_maxpy<T, 1><<<g, 256, 0, s>>>(n, hh, V, w, sign); break;
+    case 2: k_maxpy<T, 2><<<g, 256, 0, s>>>(n, hh, V, w, sign); break;
+    case 3: k_maxpy<T, 3><<<g, 256, 0, s>>>(n, hh, V, w, sign); break;
+    case 4: k_maxpy<T, 4><<<g, 256, 0, s>>>(n, hh, V, w, sign); break;
+    case 5: k_maxpy<T, 5><<<g, 256, 0, s>>>(n, hh, V, w, sign); break;
+    case 6: k_maxpy<T, 6><<<g, 256, 0, s>>>(n, hh, V, w, sign); break;
+    case 7: k_maxpy<T, 7><<<g, 256, 0, s>>>(n, hh, V, w, sign); break;
+    default: k_maxpy<T, 8><<<g, 256, 0, s>>>(n, hh, V, w, sign); break;
+    }
+    count_launch(1);
+  }
+}
+template <typename T>
+void v_cg_xr(size_t n, const double *num, const double *den, T *x, T *r, const T *p, const T *q, bool update_r, cudaStream_t s)
+{
+  k_cg_xr<<<vgrid(n), 256, 0, s>>>(n, num, den, x, r, p, q, update_r ? 1 : 0);
+  count_launch(1);
+}
+template <typename T> void v_cg_p(size_t n, const double *num, const double *den, const T *z, T *p, cudaStream_t s)
+{
+  k_cg_p<<<vgrid(n), 256, 0, s>>>(n, num, den, z, p);
   count_launch(1);
 }
 void v_block4(size_t nel, const double *B, const double *x, double *y, double alpha, cudaStream_t s)
@@ -226,7 +311,9 @@ template void v_convert<float, double>(size_t, const float *, double *, cudaStre
   template void v_residual<T>(size_t, const T *, const T *, T *, cudaStream_t);                                        \
   template void v_mask<T>(int, int, int, uint32_t, T *, cudaStream_t);                                                 \
   template void v_mdot<T>(size_t, int, const T *const *, const T *, double *, double *, cudaStream_t);                 \
-  template void v_maxpy<T>(size_t, int, const double *, const T *const *, T *, double, cudaStream_t);
+  template void v_maxpy<T>(size_t, int, const double *, const T *const *, T *, double, cudaStream_t);              \
+  template void v_cg_xr<T>(size_t, const double *, const double *, T *, T *, const T *, const T *, bool, cudaStream_t); \
+  template void v_cg_p<T>(size_t, const double *, const double *, const T *, T *, cudaStream_t);
 P3D_INST(double)
 P3D_INST(float)
 

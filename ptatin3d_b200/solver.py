@@ -82,6 +82,13 @@ class StokesSolver:
         check(lib().p3d_solver_apply_pc(self.h, _ptr(ru_d), _ptr(rp_d), _ptr(zu), _ptr(zp)))
         return zu, zp
 
+    def level_apply(self, level, x):
+        """FP64 velocity operator of multigrid level `level` (0 = coarsest)."""
+        xd = self._dev(x)
+        y = torch.empty_like(xd)
+        check(lib().p3d_solver_level_apply(self.h, int(level), _ptr(xd), _ptr(y)))
+        return y
+
     def destroy(self):
         if getattr(self, "h", None) is not None and self.h.value:
             lib().p3d_solver_destroy(self.h)

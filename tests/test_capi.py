@@ -46,3 +46,24 @@ def test_mesh_desc_whole():
     d = _lib.MeshDesc()
     assert _lib.lib().p3d_mesh_desc_whole(4, 5, 6, 7, C.byref(d)) == 0
     assert (d.gx, d.gy, d.gz, d.ox, d.global_faces) == (9, 11, 13, 0, 0x3F)
+
+
+def test_solver_options_defaults_and_checks():
+    """Option defaults and validation happen on the host, before any device call."""
+    L = _lib.lib()
+    o = _lib.SolverOpts()
+    assert L.p3d_solver_default_opts(C.byref(o)) == 0
+    assert (o.nlevels, o.cheb_its, o.restart, o.inner_its, o.coarse_op, o.schur_eta) == \
+        (4, 3, 30, 0, _lib.COARSE_GALERKIN, _lib.SCHUR_ETA_QP)
+    assert (o.cheb_lo, o.cheb_hi) == (0.2, 1.1)
+    d = _lib.MeshDesc()
+    assert L.p3d_mesh_desc_whole(16, 16, 16, 0, C.byref(d)) == 0
+    h = C.c_void_p()
+    o.restart = _lib.MAX_RESTART + 1
+    assert L.p3d_solver_create(C.byref(d), C.byref(o), 0, C.byref(h)) == _lib.P3D_ERR_ARG
+    o.restart = 30
+    o.nlevels = 1  # 16^3 coarse level: 107,811 dofs, above the dense limit
+    assert L.p3d_solver_create(C.byref(d), C.byref(o), 0, C.byref(h)) == _lib.P3D_ERR_ARG
+    assert b"dense limit" in L.p3d_last_error()
+    o.nlevels, o.schur_eta = 3, 7
+    assert L.p3d_solver_create(C.byref(d), C.byref(o), 0, C.byref(h)) == _lib.P3D_ERR_ARG
