@@ -329,9 +329,12 @@ def run_b200(args):
     ab = algorithmic_bytes(m)
     achieved = ab / (kern_ms * 1e-3) / 1e9
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        traffic = json.load(open(tf)).get("a11_f64_general_96", None)
+    tf = os.path.join(ROOT, "profiles", "traffic.txt")  # ncu dram__bytes_read+write per launch
+    if os.path.exists(tf) and m == 96 and args.workload == "deformed":
+        for ln in open(tf):
+            f = ln.split()
+            if len(f) == 2 and f[0] == "a11_f64_general_96":
+                traffic = float(f[1])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -377,7 +380,7 @@ def run_b200(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
