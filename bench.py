@@ -221,6 +221,92 @@ def solve_leg(device, m=32, seed=1):
             "oracle_solve": out["ref"]}
 
 
+SERVE_SIZES = (8, 12, 16, 24, 32, 48)
+
+
+def serving_stream(n, seed=7, rate_per_s=200.0):
+    """Independent sinker solves: m^3 elements, m uniform in SERVE_SIZES, 1-12
+    sinkers of radius 0.1, viscosity contrast log-uniform in [1e2, 1e5],
+    density +1 %, Poisson arrivals."""
+    from ptatin3d_b200 import mesh as M
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        m = int(rng.choice(SERVE_SIZES))
+        nsph = int(rng.integers(1, 13))
+        contrast = float(10.0 ** rng.uniform(2.0, 5.0))
+        c = M.uniform_coords(m, m, m)
+        qp = M.qp_coords(c, m, m, m)
+        cen = rng.uniform(0.0, 1.0, size=(nsph, 3))
+        out.append(dict(m=m, coords=c, eta=M.sinker_eta(qp, cen, 0.1, 1.0, contrast),
+                        rho=M.sinker_density(qp, cen, 0.1, 1.0, 1.01), contrast=contrast, nsph=nsph))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate_per_s, size=n))
+    return out, arrivals - arrivals[0]
+
+
+def serve_leg(device, n, max_active=8):
+    """Served stream (mixed precision, rtol 1e-6) against the same solves run
+    one after another with the plain FP64 solver."""
+    import torch
+
+    from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
+    from ptatin3d_b200 import mesh as M
+    from ptatin3d_b200.serving import StokesServer
+    from ptatin3d_b200.solver import StokesSolver, max_levels
+    bits = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
+    reqs, arrivals = serving_stream(n)
+    opts = dict(rtol=1e-6, max_it=1000, schur_eta=SCHUR_ETA_GEOMEAN)
+    # served: continuous admission, concurrent solves
+    S = StokesServer(device=device, hbm_budget=64 << 30, max_active=max_active)
+    for r in reqs[:6]:  # warm the pool shapes (setup of each shape once)
+        S.submit((r["m"],) * 3, bits, r["coords"], r["eta"], r["rho"], nlevels=max_levels(r["m"]),
+                 mg_precision=PREC_F32, **opts)
+    S.wait_all()
+    done, i = [], 0
+    t0 = time.perf_counter()
+    while len(done) < n:
+        now = time.perf_counter() - t0
+        while i < n and arrivals[i] <= now:
+            r = reqs[i]
+            S.submit((r["m"],) * 3, bits, r["coords"], r["eta"], r["rho"], tag=i, nlevels=max_levels(r["m"]),
+                     mg_precision=PREC_F32, **opts)
+            i += 1
+        done += S.poll(timeout_ms=1)
+    served_s = time.perf_counter() - t0
+    st = S.stats()
+    S.close()
+    lat = np.array([d["latency_ms"] for d in done])
+    # sequential plain FP64 solves (solvers reused per mesh size), inputs from and results to the host
+    pool = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    seq_ok = 0
+    for r in reqs:
+        m = r["m"]
+        if m not in pool:
+            pool[m] = StokesSolver(m, m, m, bits, device=device, nlevels=max_levels(m), mg_precision=PREC_F64, **opts)
+        D = pool[m]
+        D.setup(r["coords"], r["eta"])
+        D.set_rhs_body_force(r["rho"])
+        u, p, stt = D.solve(raise_on_noconv=False)
+        u.cpu(), p.cpu()
+        seq_ok += int(stt["converged"])
+    torch.cuda.synchronize()
+    seq_s = time.perf_counter() - t0
+    for D in pool.values():
+        D.destroy()
+    return {"workload": f"{n} independent Stokes solves, m^3 elements with m uniform in {list(SERVE_SIZES)}, 1-12 "
+                        "sinkers r=0.1, eta contrast log-uniform [1e2,1e5], Poisson arrivals 200/s; mixed precision, "
+                        "rtol 1e-6, max 1000 FGMRES iterations",
+            "requests": n, "max_active": max_active, "solves_per_s": n / served_s,
+            "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
+            "converged": int(sum(d["ok"] for d in done)),
+            "sequential_fp64_solves_per_s": n / seq_s, "sequential_fp64_converged": seq_ok,
+            "speedup_vs_sequential_fp64": seq_s / served_s,
+            "peak_device_bytes": st["peak_device_bytes"], "solvers_created": st["solvers_created"],
+            "solvers_reused": st["solvers_reused"]}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -349,6 +435,9 @@ def run_b200(args):
     solve = None
     if rank == 0 and not args.no_solve:
         solve = solve_leg(local)
+    serving = None
+    if rank == 0 and args.serve_requests > 0:
+        serving = serve_leg(local, args.serve_requests)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -369,7 +458,8 @@ def run_b200(args):
                                "hbm_frac": algorithmic_bytes(m, 4) / (f32_ms * 1e-3) / 1e9 / peak},
                 "fp64_alu": {"flop_per_element": REF_FLOPS_PER_EL,
                              "TFLOP/s": REF_FLOPS_PER_EL * m ** 3 / (kern_ms * 1e-3) / 1e12},
-                "solve": solve}
+                "solve": solve,
+                "serving": serving}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -386,6 +476,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-solve", action="store_true", help="skip the FP64 vs mixed-precision Stokes solve leg")
+    ap.add_argument("--serve-requests", type=int, default=32, help="requests of the served-stream leg (0: skip)")
     ap.add_argument("--size", type=int, default=96, help="elements per direction")
     ap.add_argument("--workload", default="deformed", choices=["deformed", "layered"])
     args = ap.parse_args()

@@ -199,6 +199,9 @@ typedef struct p3d_solve_stats {
 } p3d_solve_stats;
 
 int p3d_solver_default_opts(p3d_solver_opts *opts);
+/* Upper estimate of the device memory a solver of this mesh and options
+ * holds after setup (used to admit solves by HBM footprint). */
+int p3d_solver_estimate_bytes(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, int64_t *bytes);
 /* mesh: a whole mesh (p3d_mesh_desc_whole); mx,my,mz divisible by 2^(nlevels-1). */
 int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, int device, p3d_solver **solver);
 /* Device FP64 arrays: coords 3*nn, eta 27*nel.  Builds the hierarchy, the
@@ -217,6 +220,55 @@ int p3d_solver_apply_pc(p3d_solver *s, const double *ru, const double *rp, doubl
  * (0 = coarsest), Dirichlet rows identity (testing the hierarchy). */
 int p3d_solver_level_apply(p3d_solver *s, int level, const double *x_dev, double *y_dev);
 int p3d_solver_destroy(p3d_solver *s);
+
+/* ------------------------------------------------------- solve server --- */
+/* A persistent request loop for independent Stokes solves of uneven mesh
+ * sizes (no counterpart in the reference, which runs one solve per process).
+ * Requests are admitted first-in first-out as soon as one of `max_active`
+ * execution slots and the device memory they need (p3d_solver_estimate_bytes)
+ * are free; admitted solves run concurrently, each on its own stream with its
+ * state resident in HBM.  Solvers are pooled by mesh and options and reused
+ * by later requests of the same shape. */
+typedef struct p3d_server p3d_server;
+
+typedef struct p3d_request {
+  int32_t mx, my, mz;     /* whole mesh, elements per direction                   */
+  uint32_t dirichlet;     /* P3D_BC_BIT mask                                      */
+  const double *coords;   /* host, 3*(2mx+1)(2my+1)(2mz+1)                        */
+  const double *eta;      /* host, 27*mx*my*mz Gauss-point viscosity              */
+  const double *rho;      /* host, 27*mx*my*mz Gauss-point density                */
+  double gx, gy, gz;      /* gravity                                              */
+  double *u, *p;          /* host outputs, 3*nn and 4*nel (valid after the result) */
+  p3d_solver_opts opts;
+  int64_t tag;            /* returned in the result                               */
+} p3d_request;
+
+typedef struct p3d_result {
+  int64_t tag;
+  int32_t status;         /* P3D_OK, P3D_ERR_NOCONV (u, p hold the last iterate), ... */
+  int32_t iterations;
+  double rel_residual;    /* ||r|| / ||r0||                                       */
+  double wait_ms;         /* submit -> admitted                                   */
+  double run_ms;          /* admitted -> solution copied to the host              */
+  double latency_ms;      /* submit -> solution copied to the host                */
+} p3d_result;
+
+typedef struct p3d_server_stats {
+  int64_t submitted, admitted, completed;
+  int32_t active, queued;
+  int64_t device_bytes, peak_device_bytes; /* estimated bytes held by pooled solvers */
+  int32_t solvers_created, solvers_reused;
+} p3d_server_stats;
+
+int p3d_server_create(int device, int64_t hbm_budget_bytes, int32_t max_active, p3d_server **server);
+/* Non-blocking.  The request's host arrays must stay valid until its result
+ * has been returned by p3d_server_poll. */
+int p3d_server_submit(p3d_server *server, const p3d_request *request);
+/* Up to max_results finished solves (waits up to timeout_ms for the first). */
+int p3d_server_poll(p3d_server *server, p3d_result *results, int32_t max_results, int32_t timeout_ms, int32_t *n);
+int p3d_server_get_stats(p3d_server *server, p3d_server_stats *stats);
+/* Finishes every submitted solve, then frees the pool. */
+int p3d_server_destroy(p3d_server *server);
 
 /* -------------------------------------------------------- diagnostics --- */
 /* Last error message of the calling thread (static storage, never NULL). */

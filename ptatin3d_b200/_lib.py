@@ -50,6 +50,24 @@ class SolverOpts(C.Structure):
                 ("schur_eta", C.c_int32)]
 
 
+class Request(C.Structure):
+    _fields_ = [("mx", C.c_int32), ("my", C.c_int32), ("mz", C.c_int32), ("dirichlet", C.c_uint32),
+                ("coords", C.c_void_p), ("eta", C.c_void_p), ("rho", C.c_void_p),
+                ("gx", C.c_double), ("gy", C.c_double), ("gz", C.c_double),
+                ("u", C.c_void_p), ("p", C.c_void_p), ("opts", SolverOpts), ("tag", C.c_int64)]
+
+
+class Result(C.Structure):
+    _fields_ = [("tag", C.c_int64), ("status", C.c_int32), ("iterations", C.c_int32), ("rel_residual", C.c_double),
+                ("wait_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64), ("active", C.c_int32),
+                ("queued", C.c_int32), ("device_bytes", C.c_int64), ("peak_device_bytes", C.c_int64),
+                ("solvers_created", C.c_int32), ("solvers_reused", C.c_int32)]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("r0", C.c_double), ("rfinal", C.c_double),
                 ("setup_ms", C.c_double), ("solve_ms", C.c_double), ("lmax_fine", C.c_double),
@@ -68,6 +86,12 @@ _SIGS = {
     "p3d_solver_apply_pc": ([C.c_void_p] * 5, C.c_int),
     "p3d_solver_destroy": ([C.c_void_p], C.c_int),
     "p3d_solver_level_apply": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_solver_estimate_bytes": ([C.POINTER(MeshDesc), C.POINTER(SolverOpts), C.POINTER(C.c_int64)], C.c_int),
+    "p3d_server_create": ([C.c_int, C.c_int64, C.c_int32, C.POINTER(C.c_void_p)], C.c_int),
+    "p3d_server_submit": ([C.c_void_p, C.POINTER(Request)], C.c_int),
+    "p3d_server_poll": ([C.c_void_p, C.POINTER(Result), C.c_int32, C.c_int32, C.POINTER(C.c_int32)], C.c_int),
+    "p3d_server_get_stats": ([C.c_void_p, C.POINTER(ServerStats)], C.c_int),
+    "p3d_server_destroy": ([C.c_void_p], C.c_int),
     "p3d_last_error": ([], C.c_char_p),
     "p3d_kernel_launch_count": ([], C.c_int64),
     "p3d_version": ([], C.c_char_p),

@@ -25,6 +25,7 @@ struct p3d_op {
   void *kgen = nullptr;   // general path: eta, brick order (NW_GEN)
   void *kaff = nullptr;   // affine path: J^{-1} + eta*w*detJ, brick order (NW_AFF)
   void *hx = nullptr, *hy = nullptr; // host-apply staging
+  unsigned long long *flag = nullptr; // affinity test result (kept: re-setup allocates nothing)
   cudaStream_t stream = nullptr;     // setup / host-apply stream
 };
 

@@ -211,8 +211,8 @@ int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geo
   int ntx, nty, ntz;
   bricks(m, NW_GEN, ntx, nty, ntz);
   size_t ng = (size_t)ntx * nty * ntz * Brick<NW_GEN>::NE * 27;
-  free_dev(op->kgen);
-  if ((rc = dev_alloc(&op->kgen, ng * es, "eta (brick order)"))) return rc;
+  // buffers keep their size for the mesh: a re-setup (new coefficients) allocates and frees nothing
+  if (!op->kgen && (rc = dev_alloc(&op->kgen, ng * es, "eta (brick order)"))) return rc;
   if (op->prec == P3D_PREC_F64)
     pack_eta_kernel<double, NW_GEN><<<grid_for(ng), 256, 0, st>>>(m.mx, m.my, m.mz, ntx, nty, ntz, eta, (double *)op->kgen);
   else
@@ -222,22 +222,21 @@ int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geo
   // affinity
   int mode = geom_mode;
   if (mode == P3D_GEOM_AUTO) {
-    unsigned long long *bad = nullptr, hbad = 0;
-    if ((rc = dev_alloc((void **)&bad, sizeof *bad, "affine flag"))) return rc;
+    unsigned long long hbad = 0;
+    if (!op->flag && (rc = dev_alloc((void **)&op->flag, sizeof *op->flag, "affine flag"))) return rc;
+    unsigned long long *bad = op->flag;
     cudaMemsetAsync(bad, 0, sizeof *bad, st);
     affine_check_kernel<<<grid_for(nel), 256, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz, coords, 1e-13, bad);
     count_launch(1);
     rc = cuda_check(cudaMemcpyAsync(&hbad, bad, sizeof hbad, cudaMemcpyDeviceToHost, st), "affine flag");
     if (!rc) rc = cuda_check(cudaStreamSynchronize(st), "affine sync");
-    cudaFree(bad);
     if (rc) return rc;
     mode = (hbad == 0 && nel > 0) ? P3D_GEOM_AFFINE : P3D_GEOM_GENERAL;
   }
-  free_dev(op->kaff);
   if (mode == P3D_GEOM_AFFINE) {
     bricks(m, NW_AFF, ntx, nty, ntz);
     size_t na = (size_t)ntx * nty * ntz * Brick<NW_AFF>::NE;
-    if ((rc = dev_alloc(&op->kaff, na * 36 * es, "affine geometry"))) return rc;
+    if (!op->kaff && (rc = dev_alloc(&op->kaff, na * 36 * es, "affine geometry"))) return rc;
     if (op->prec == P3D_PREC_F64)
       pack_affine_kernel<double, NW_AFF><<<grid_for(na), 256, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz,
                                                                       ntx, nty, ntz, coords, eta, (double *)op->kaff);
@@ -313,6 +312,7 @@ int p3d_op_destroy(p3d_op *op)
   free_dev(op->kaff);
   free_dev(op->hx);
   free_dev(op->hy);
+  if (op->flag) cudaFree(op->flag);
   if (op->stream) cudaStreamDestroy(op->stream);
   delete op;
   return P3D_OK;

@@ -1,0 +1,334 @@
+// Solve server: a persistent request loop for independent Stokes solves.
+//
+// Requests (a whole mesh, coefficients, density, gravity, solver options)
+// arrive with p3d_server_submit and are admitted first-in first-out as soon
+// as an execution slot and the HBM they need are free.  Each admitted solve
+// runs on one of `max_active` worker threads, on its own CUDA stream, with
+// all of its state (hierarchy, Krylov basis, captured preconditioner graph)
+// resident in device memory; solves that are admitted together overlap on the
+// device.  Finished solvers go back to a pool keyed by mesh and options, so a
+// later request of the same shape reuses the device memory and only uploads
+// new coefficients (no cudaMalloc/cudaFree on the hot path).  Idle pooled
+// solvers are released, least recently used first, when a request needs
+// their memory.
+//
+// No counterpart in the reference (pTatin3d runs one solve per process); the
+// per-request solve is p3d_solver_*.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "p3d_b200.h"
+#include "p3d_internal.h"
+
+namespace p3d {
+
+static double wall_ms()
+{
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Slot {
+  p3d_solver *solver = nullptr;
+  int32_t mx = 0, my = 0, mz = 0;
+  uint32_t dirichlet = 0;
+  p3d_solver_opts opts;
+  int64_t bytes = 0;
+  double *coords = nullptr, *eta = nullptr, *rho = nullptr, *u = nullptr, *p = nullptr;
+  cudaStream_t io = nullptr; // host<->device copies of this slot
+  bool busy = false;
+  bool ready = false; // created (device memory held)
+  uint64_t last_used = 0;
+};
+
+struct Pending {
+  p3d_request req;
+  double t_submit;
+};
+
+static bool same_shape(const Slot &s, const p3d_request &r)
+{
+  return s.mx == r.mx && s.my == r.my && s.mz == r.mz && s.dirichlet == r.dirichlet &&
+         memcmp(&s.opts, &r.opts, sizeof(p3d_solver_opts)) == 0;
+}
+
+static int64_t request_bytes(const p3d_request &r)
+{
+  p3d_mesh_desc d;
+  if (p3d_mesh_desc_whole(r.mx, r.my, r.mz, r.dirichlet, &d)) return -1;
+  int64_t b = 0;
+  if (p3d_solver_estimate_bytes(&d, &r.opts, &b)) return -1;
+  const int64_t nn = (int64_t)(2 * r.mx + 1) * (2 * r.my + 1) * (2 * r.mz + 1), nel = (int64_t)r.mx * r.my * r.mz;
+  return b + 8 * (3 * nn + 27 * nel + 27 * nel + 3 * nn + 4 * nel); // slot buffers
+}
+
+static void release_slot(Slot *s)
+{
+  if (s->solver) p3d_solver_destroy(s->solver);
+  for (double *q : {s->coords, s->eta, s->rho, s->u, s->p})
+    if (q) cudaFree(q);
+  if (s->io) cudaStreamDestroy(s->io);
+  s->solver = nullptr;
+  s->coords = s->eta = s->rho = s->u = s->p = nullptr;
+  s->io = nullptr;
+  s->ready = false;
+}
+
+static int create_slot(Slot *s, int device)
+{
+  p3d_mesh_desc d;
+  int rc = p3d_mesh_desc_whole(s->mx, s->my, s->mz, s->dirichlet, &d);
+  if (!rc) rc = p3d_solver_create(&d, &s->opts, device, &s->solver);
+  const size_t nn = (size_t)(2 * s->mx + 1) * (2 * s->my + 1) * (2 * s->mz + 1), nel = (size_t)s->mx * s->my * s->mz;
+  if (!rc) rc = dev_alloc((void **)&s->coords, 3 * nn * 8, "request coords");
+  if (!rc) rc = dev_alloc((void **)&s->eta, 27 * nel * 8, "request eta");
+  if (!rc) rc = dev_alloc((void **)&s->rho, 27 * nel * 8, "request rho");
+  if (!rc) rc = dev_alloc((void **)&s->u, 3 * nn * 8, "request u");
+  if (!rc) rc = dev_alloc((void **)&s->p, 4 * nel * 8, "request p");
+  if (!rc) rc = cuda_check(cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking), "request stream");
+  if (rc) release_slot(s);
+  else s->ready = true;
+  return rc;
+}
+
+// one solve in slot s; returns the status recorded in the result
+static int run_request(Slot *s, const p3d_request &r, p3d_result &res)
+{
+  const size_t nn = (size_t)(2 * r.mx + 1) * (2 * r.my + 1) * (2 * r.mz + 1), nel = (size_t)r.mx * r.my * r.mz;
+  cudaStream_t io = s->io;
+  int rc = cuda_check(cudaMemcpyAsync(s->coords, r.coords, 3 * nn * 8, cudaMemcpyHostToDevice, io), "h2d coords");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(s->eta, r.eta, 27 * nel * 8, cudaMemcpyHostToDevice, io), "h2d eta");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(s->rho, r.rho, 27 * nel * 8, cudaMemcpyHostToDevice, io), "h2d rho");
+  if (!rc) rc = cuda_check(cudaMemsetAsync(s->u, 0, 3 * nn * 8, io), "zero u");
+  if (!rc) rc = cuda_check(cudaMemsetAsync(s->p, 0, 4 * nel * 8, io), "zero p");
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(io), "h2d sync");
+  if (!rc) rc = p3d_solver_setup(s->solver, s->coords, s->eta);
+  if (!rc) rc = p3d_solver_set_rhs_body_force(s->solver, s->rho, r.gx, r.gy, r.gz);
+  p3d_solve_stats st;
+  memset(&st, 0, sizeof st);
+  int srv = rc ? rc : p3d_solver_solve(s->solver, s->u, s->p, &st);
+  if (!rc && (srv == P3D_OK || srv == P3D_ERR_NOCONV)) {
+    rc = cuda_check(cudaMemcpyAsync(r.u, s->u, 3 * nn * 8, cudaMemcpyDeviceToHost, io), "d2h u");
+    if (!rc) rc = cuda_check(cudaMemcpyAsync(r.p, s->p, 4 * nel * 8, cudaMemcpyDeviceToHost, io), "d2h p");
+    if (!rc) rc = cuda_check(cudaStreamSynchronize(io), "d2h sync");
+  }
+  res.iterations = st.iterations;
+  res.rel_residual = st.r0 > 0 ? st.rfinal / st.r0 : 0.0;
+  return rc ? rc : srv;
+}
+
+} // namespace p3d
+
+using namespace p3d;
+
+struct p3d_server {
+  int device = 0;
+  int64_t budget = 0;
+  int max_active = 1;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Pending> queue;
+  std::vector<Slot *> slots;
+  std::deque<p3d_result> done;
+  std::vector<std::thread> workers;
+  bool stopping = false;
+  int active = 0;
+  int64_t bytes = 0, peak = 0;
+  uint64_t clock = 0;
+  p3d_server_stats st{};
+};
+
+namespace p3d {
+
+// Under the lock: pick (or reserve memory for) a slot for the queue head.
+// Returns the slot, or nullptr when the head must wait.  `evict` collects idle
+// slots to release outside the lock.
+static Slot *admit_head(p3d_server *S, std::vector<Slot *> &evict, bool &fresh, bool &too_big)
+{
+  const p3d_request &r = S->queue.front().req;
+  fresh = false;
+  too_big = false;
+  for (Slot *s : S->slots)
+    if (s->ready && !s->busy && same_shape(*s, r)) return s;
+  const int64_t need = request_bytes(r);
+  if (need < 0 || need > S->budget) {
+    too_big = true;
+    return nullptr;
+  }
+  // release idle slots (least recently used first) until the request fits
+  while (S->bytes + need > S->budget) {
+    Slot *lru = nullptr;
+    for (Slot *s : S->slots)
+      if (s->ready && !s->busy && (!lru || s->last_used < lru->last_used)) lru = s;
+    if (!lru) return nullptr; // wait for a running solve to finish
+    lru->ready = false;
+    S->bytes -= lru->bytes;
+    S->slots.erase(std::find(S->slots.begin(), S->slots.end(), lru));
+    evict.push_back(lru);
+  }
+  Slot *s = new Slot();
+  s->mx = r.mx; s->my = r.my; s->mz = r.mz;
+  s->dirichlet = r.dirichlet;
+  s->opts = r.opts;
+  s->bytes = need;
+  S->bytes += need;
+  S->peak = std::max(S->peak, S->bytes);
+  S->slots.push_back(s);
+  fresh = true;
+  return s;
+}
+
+static void worker(p3d_server *S)
+{
+  cudaSetDevice(S->device);
+  std::unique_lock<std::mutex> lk(S->mu);
+  for (;;) {
+    if (S->queue.empty()) {
+      if (S->stopping) return;
+      S->cv_work.wait(lk);
+      continue;
+    }
+    std::vector<Slot *> evict;
+    bool fresh = false, too_big = false;
+    Slot *slot = admit_head(S, evict, fresh, too_big);
+    if (!slot && !too_big) {
+      if (!evict.empty()) { // memory was given back: release it and look again
+        lk.unlock();
+        for (Slot *e : evict) { release_slot(e); delete e; }
+        lk.lock();
+        continue;
+      }
+      S->cv_work.wait(lk);
+      continue;
+    }
+    Pending job = S->queue.front();
+    S->queue.pop_front();
+    p3d_result res;
+    memset(&res, 0, sizeof res);
+    res.tag = job.req.tag;
+    const double t_admit = wall_ms();
+    res.wait_ms = t_admit - job.t_submit;
+    if (too_big) {
+      res.status = P3D_ERR_NOMEM;
+      res.latency_ms = res.wait_ms;
+      S->done.push_back(res);
+      S->st.completed++;
+      S->cv_done.notify_all();
+      continue;
+    }
+    slot->busy = true;
+    S->active++;
+    S->st.admitted++;
+    if (fresh) S->st.solvers_created++;
+    else S->st.solvers_reused++;
+    S->cv_work.notify_all(); // the next request may fit as well
+    lk.unlock();
+    for (Slot *e : evict) { release_slot(e); delete e; }
+    int rc = fresh ? create_slot(slot, S->device) : P3D_OK;
+    if (!rc) rc = run_request(slot, job.req, res);
+    const double t_end = wall_ms();
+    res.status = rc;
+    res.run_ms = t_end - t_admit;
+    res.latency_ms = t_end - job.t_submit;
+    lk.lock();
+    slot->busy = false;
+    slot->last_used = ++S->clock;
+    if (!slot->ready) { // creation failed: give the memory back
+      S->bytes -= slot->bytes;
+      S->slots.erase(std::find(S->slots.begin(), S->slots.end(), slot));
+      delete slot;
+    }
+    S->active--;
+    S->done.push_back(res);
+    S->st.completed++;
+    S->cv_done.notify_all();
+    S->cv_work.notify_all();
+  }
+}
+
+} // namespace p3d
+
+extern "C" {
+
+int p3d_server_create(int device, int64_t hbm_budget_bytes, int32_t max_active, p3d_server **out)
+{
+  if (!out || hbm_budget_bytes <= 0 || max_active < 1 || max_active > 256)
+    return set_error(P3D_ERR_ARG, "server_create: bad arguments");
+  *out = nullptr;
+  int rc = cuda_check(cudaSetDevice(device), "cudaSetDevice");
+  if (rc) return rc;
+  p3d_server *S = new p3d_server();
+  S->device = device;
+  S->budget = hbm_budget_bytes;
+  S->max_active = max_active;
+  for (int i = 0; i < max_active; i++) S->workers.emplace_back(worker, S);
+  *out = S;
+  return P3D_OK;
+}
+
+int p3d_server_submit(p3d_server *S, const p3d_request *req)
+{
+  if (!S || !req || !req->coords || !req->eta || !req->rho || !req->u || !req->p || req->mx < 1 || req->my < 1 ||
+      req->mz < 1)
+    return set_error(P3D_ERR_ARG, "server_submit: bad request");
+  std::lock_guard<std::mutex> g(S->mu);
+  if (S->stopping) return set_error(P3D_ERR_STATE, "server_submit: server is shutting down");
+  S->queue.push_back(Pending{*req, wall_ms()});
+  S->st.submitted++;
+  S->cv_work.notify_one();
+  return P3D_OK;
+}
+
+int p3d_server_poll(p3d_server *S, p3d_result *results, int32_t max_results, int32_t timeout_ms, int32_t *n)
+{
+  if (!S || !results || !n || max_results < 1) return set_error(P3D_ERR_ARG, "server_poll: bad arguments");
+  std::unique_lock<std::mutex> lk(S->mu);
+  if (S->done.empty() && timeout_ms > 0)
+    S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [S] { return !S->done.empty(); });
+  int k = 0;
+  while (k < max_results && !S->done.empty()) {
+    results[k++] = S->done.front();
+    S->done.pop_front();
+  }
+  *n = k;
+  return P3D_OK;
+}
+
+int p3d_server_get_stats(p3d_server *S, p3d_server_stats *st)
+{
+  if (!S || !st) return set_error(P3D_ERR_ARG, "server_get_stats: null argument");
+  std::lock_guard<std::mutex> g(S->mu);
+  *st = S->st;
+  st->active = S->active;
+  st->queued = (int32_t)S->queue.size();
+  st->device_bytes = S->bytes;
+  st->peak_device_bytes = S->peak;
+  return P3D_OK;
+}
+
+int p3d_server_destroy(p3d_server *S)
+{
+  if (!S) return P3D_OK;
+  {
+    std::lock_guard<std::mutex> g(S->mu);
+    S->stopping = true;
+  }
+  S->cv_work.notify_all();
+  for (auto &t : S->workers) t.join();
+  cudaSetDevice(S->device);
+  for (Slot *s : S->slots) {
+    release_slot(s);
+    delete s;
+  }
+  delete S;
+  return P3D_OK;
+}
+
+} // extern "C"

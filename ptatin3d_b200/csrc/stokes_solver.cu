@@ -51,6 +51,7 @@ struct p3d_solver {
   int nc = 0;
   double *cinv = nullptr;          // dense inverse of the Galerkin coarse operator
   double *cb64 = nullptr, *cx64 = nullptr;
+  double *gj = nullptr;            // Gauss-Jordan pivot row and column
   // Stokes system
   size_t nu = 0, np = 0, N = 0;
   double *Binv = nullptr; // Schur block inverses
@@ -67,6 +68,7 @@ struct p3d_solver {
   double *cg_sc = nullptr; // {rz (2 slots, alternating), pq}
   // preconditioner buffers (fixed for graph capture)
   double *pc_in = nullptr, *pc_out = nullptr, *pc_t = nullptr;
+  double *xsol = nullptr; // [u; p] iterate of a solve
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   bool setup_done = false, rhs_set = false;
@@ -375,9 +377,11 @@ static int build_coarse(p3d_solver *s)
   const int nc = (int)C.nv;
   s->nc = nc;
   const uint32_t dir = level_dir(s);
-  CK(dev_alloc((void **)&s->cinv, (size_t)nc * nc * 8, "coarse operator"));
-  CK(dev_alloc((void **)&s->cb64, (size_t)nc * 8, "coarse vec"));
-  CK(dev_alloc((void **)&s->cx64, (size_t)nc * 8, "coarse vec"));
+  // kept across setups (a solver re-set up with new coefficients allocates nothing)
+  if (!s->cinv) CK(dev_alloc((void **)&s->cinv, (size_t)nc * nc * 8, "coarse operator"));
+  if (!s->cb64) CK(dev_alloc((void **)&s->cb64, (size_t)nc * 8, "coarse vec"));
+  if (!s->cx64) CK(dev_alloc((void **)&s->cx64, (size_t)nc * 8, "coarse vec"));
+  if (!s->gj) CK(dev_alloc((void **)&s->gj, 2 * (size_t)nc * 8, "gauss-jordan"));
   // coarse Dirichlet mask on the host
   std::vector<char> isdir(nc, 0);
   {
@@ -431,19 +435,14 @@ static int build_coarse(p3d_solver *s)
     }
   }
   // Ac is symmetric: columns stored as rows is the same matrix.  Invert in place.
-  double *colk = nullptr, *rowk = nullptr;
-  CK(dev_alloc((void **)&colk, (size_t)nc * 8, "gj"));
-  CK(dev_alloc((void **)&rowk, (size_t)nc * 8, "gj"));
+  double *colk = s->gj, *rowk = s->gj + nc;
   int g = (int)std::min<size_t>(((size_t)nc * nc + 255) / 256, 148 * 16);
   for (int k = 0; k < nc; k++) {
     k_gj_save<<<(nc + 255) / 256, 256, 0, s->st>>>(nc, k, s->cinv, colk, rowk);
     k_gj_step<<<g, 256, 0, s->st>>>(nc, k, s->cinv, colk, rowk);
   }
   count_launch(2 * nc);
-  int rc = cuda_check(cudaStreamSynchronize(s->st), "coarse inverse");
-  cudaFree(colk);
-  cudaFree(rowk);
-  return rc;
+  return cuda_check(cudaStreamSynchronize(s->st), "coarse inverse");
 }
 
 // Galerkin operator of level l from level l+1: Ac = P~^T A P~ (P~ = P with
@@ -682,6 +681,39 @@ int p3d_solver_default_opts(p3d_solver_opts *o)
   return P3D_OK;
 }
 
+int p3d_solver_estimate_bytes(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, int64_t *bytes)
+{
+  if (!mesh || !bytes) return set_error(P3D_ERR_ARG, "estimate_bytes: null argument");
+  p3d_solver_opts o;
+  if (opts) o = *opts;
+  else p3d_solver_default_opts(&o);
+  if (o.nlevels < 1 || o.nlevels > 12 || o.restart < 1) return set_error(P3D_ERR_ARG, "estimate_bytes: bad options");
+  const bool mixed = o.mg_precision == P3D_PREC_F32;
+  double total = 0.0;
+  const double nnf = (double)(2 * mesh->mx + 1) * (2 * mesh->my + 1) * (2 * mesh->mz + 1);
+  const double nu = 3.0 * nnf, np = 4.0 * mesh->mx * mesh->my * mesh->mz, N = nu + np;
+  total += 8.0 * ((2.0 * o.restart + 5.0) * N + nu);     // FGMRES basis, rhs, preconditioner buffers, iterate
+  total += 8.0 * nu * (o.inner_its > 0 ? 4.0 : 1.0);     // velocity-solve vectors
+  for (int l = 0; l < o.nlevels; l++) {
+    const int c = 1 << (o.nlevels - 1 - l);
+    const double mx = mesh->mx / c, my = mesh->my / c, mz = mesh->mz / c;
+    const double nn = (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1), nel = mx * my * mz, nv = 3 * nn;
+    total += 8.0 * 6.0 * nv; // work vectors + inverse diagonal
+    const bool gal = l < o.nlevels - 1 && o.coarse_op == P3D_COARSE_GALERKIN;
+    if (gal) {
+      total += 243.0 * nn * (8.0 + (mixed && l > 0 ? 4.0 : 0.0));
+    } else {
+      total += 8.0 * (3 * nn + 27 * nel);                         // level coordinates + viscosity
+      const double op = 3 * nn + 1.2 * 27 * nel + 1.2 * 36 * nel; // operator: coords, packed eta, affine data
+      total += 8.0 * op + (mixed && l > 0 ? 4.0 * op : 0.0);
+    }
+    if (l == 0) total += 8.0 * (nv * nv + 4 * nv); // dense coarse inverse
+    if (l == o.nlevels - 1) total += 8.0 * 16.0 * nel; // Schur blocks
+  }
+  *bytes = (int64_t)(1.1 * total) + (4 << 20);
+  return P3D_OK;
+}
+
 int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, int device, p3d_solver **out)
 {
   if (!mesh || !out) return set_error(P3D_ERR_ARG, "solver_create: null argument");
@@ -734,6 +766,7 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
   if (!rc) rc = dev_alloc((void **)&s->pc_in, N * 8, "pc in");
   if (!rc) rc = dev_alloc((void **)&s->pc_out, N * 8, "pc out");
   if (!rc) rc = dev_alloc((void **)&s->pc_t, s->nu * 8, "pc t");
+  if (!rc) rc = dev_alloc((void **)&s->xsol, N * 8, "solution");
   s->hs = m + 1;
   if (!rc) rc = dev_alloc((void **)&s->Vptr, (size_t)(m + 2) * sizeof(double *), "V ptrs");
   if (!rc) rc = dev_alloc((void **)&s->part, (size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK * 8, "partials");
@@ -804,16 +837,13 @@ int p3d_solver_solve(p3d_solver *s, double *u, double *p, p3d_solve_stats *stats
   p3d_solve_stats local;
   memset(&local, 0, sizeof local);
   double t0 = now_ms();
-  // x = [u; p] assembled in pc_out scratch? use a dedicated copy in w-sized buffer: reuse pc_in
-  double *x = nullptr;
-  CK(dev_alloc((void **)&x, s->N * 8, "solution"));
+  double *x = s->xsol;
   int rc = cuda_check(cudaMemcpyAsync(x, u, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "x u");
   if (!rc) rc = cuda_check(cudaMemcpyAsync(x + s->nu, p, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "x p");
   if (!rc) rc = fgmres(s, x, &local);
   if (!rc) rc = cuda_check(cudaMemcpyAsync(u, x, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "u out");
   if (!rc) rc = cuda_check(cudaMemcpyAsync(p, x + s->nu, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "p out");
   if (!rc) rc = cuda_check(cudaStreamSynchronize(s->st), "solve sync");
-  cudaFree(x);
   local.solve_ms = now_ms() - t0;
   local.setup_ms = s->setup_ms;
   local.lmax_fine = s->lv.back().lmax;
@@ -855,9 +885,9 @@ int p3d_solver_destroy(p3d_solver *s)
   if (s->gexec) cudaGraphExecDestroy(s->gexec);
   if (s->graph) cudaGraphDestroy(s->graph);
   for (auto &L : s->lv) free_level(L);
-  for (void *p : {(void *)s->cinv, (void *)s->cb64, (void *)s->cx64, (void *)s->Binv, (void *)s->bvec, (void *)s->V,
+  for (void *p : {(void *)s->cinv, (void *)s->cb64, (void *)s->cx64, (void *)s->gj, (void *)s->Binv, (void *)s->bvec, (void *)s->V,
                   (void *)s->Z, (void *)s->w, (void *)s->Vptr, (void *)s->part, (void *)s->hdev, (void *)s->pc_in,
-                  (void *)s->pc_out, (void *)s->pc_t, s->cg_r, s->cg_z, s->cg_p, s->cg_q, (void *)s->cg_ptr,
+                  (void *)s->pc_out, (void *)s->pc_t, (void *)s->xsol, s->cg_r, s->cg_z, s->cg_p, s->cg_q, (void *)s->cg_ptr,
                   (void *)s->cg_sc})
     if (p) cudaFree(p);
   if (s->hhost) cudaFreeHost(s->hhost);

@@ -1,0 +1,94 @@
+"""Solve server (continuous admission, concurrent device-resident solves).
+
+A result must not depend on what else was running: the same request solved
+alone and in a mix of other solves gives the same solution (the solver state
+of concurrent solves is disjoint; the only non-associative step, the atomic
+adds on brick faces, perturbs the iterates at rounding level, well inside the
+tolerance stated here).  Admission must keep the pooled solvers inside the
+device-memory budget, and a request larger than the budget is refused.
+"""
+import numpy as np
+import pytest
+
+from cases import rel
+from ptatin3d_b200 import PREC_F32, SCHUR_ETA_GEOMEAN, P3DError
+from ptatin3d_b200 import _lib
+from ptatin3d_b200 import mesh as M
+from ptatin3d_b200.serving import StokesServer
+from ptatin3d_b200.solver import StokesSolver, max_levels
+
+pytestmark = pytest.mark.gpu
+BITS = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
+OPTS = dict(rtol=1e-9, max_it=3000, schur_eta=SCHUR_ETA_GEOMEAN)
+
+
+def request(m, nsph, contrast, seed):
+    c = M.uniform_coords(m, m, m)
+    qp = M.qp_coords(c, m, m, m)
+    cen, r = M.random_sinkers(nsph, seed, 0.15)
+    return c, M.sinker_eta(qp, cen, r, 1.0, contrast), M.sinker_density(qp, cen, r, 1.0, 1.01)
+
+
+def submit(S, m, arrays, tag, **kw):
+    return S.submit((m, m, m), BITS, *arrays, tag=tag, nlevels=max_levels(m), **OPTS, **kw)
+
+
+def test_result_same_alone_and_in_the_mix(cuda):
+    A = request(16, 2, 1e2, 1)
+    with StokesServer(hbm_budget=8 << 30, max_active=4) as S:
+        submit(S, 16, A, 0, mg_precision=PREC_F32)
+        alone = S.wait_all()[0]
+        submit(S, 16, A, 100, mg_precision=PREC_F32)
+        for t, (m, ns, cst) in enumerate([(8, 1, 1e3), (12, 3, 1e2), (24, 2, 1e2), (16, 4, 10.0), (8, 2, 1e2)]):
+            submit(S, m, request(m, ns, cst, 10 + t), 200 + t, mg_precision=PREC_F32)
+        res = {r["tag"]: r for r in S.wait_all()}
+        st = S.stats()
+    assert alone["ok"] and all(r["ok"] for r in res.values()), [(r["tag"], r["status"]) for r in res.values()]
+    mixed = res[100]
+    assert rel(mixed["u"], alone["u"]) <= 1e-7
+    assert rel(mixed["p"], alone["p"]) <= 1e-6
+    assert st["completed"] == 7 and st["solvers_reused"] >= 1
+    # and the same as a direct solve of the request through the solver API
+    D = StokesSolver(16, 16, 16, BITS, nlevels=max_levels(16), mg_precision=PREC_F32, **OPTS)
+    D.setup(A[0], A[1])
+    D.set_rhs_body_force(A[2])
+    u, p, _ = D.solve()
+    assert rel(alone["u"], u.cpu().numpy()) <= 1e-7
+
+
+def test_admission_respects_memory_budget(cuda):
+    L = _lib.lib()
+    import ctypes as C
+    from ptatin3d_b200.solver import default_opts
+    est = {}
+    for m in (8, 16, 24):
+        d = _lib.MeshDesc()
+        L.p3d_mesh_desc_whole(m, m, m, BITS, C.byref(d))
+        b = C.c_int64()
+        _lib.check(L.p3d_solver_estimate_bytes(C.byref(d), C.byref(default_opts(nlevels=max_levels(m), **OPTS)),
+                                               C.byref(b)))
+        est[m] = b.value
+    budget = int(1.3 * est[24])  # one 24^3 solve at a time, or a few small ones
+    with StokesServer(hbm_budget=budget, max_active=4) as S:
+        for t, m in enumerate([24, 8, 16, 24, 8, 16]):
+            submit(S, m, request(m, 2, 1e2, t), t)
+        res = S.wait_all()
+        st = S.stats()
+    assert all(r["ok"] for r in res)
+    assert st["peak_device_bytes"] <= budget
+    assert st["completed"] == 6
+
+
+def test_request_larger_than_budget_is_refused(cuda):
+    with StokesServer(hbm_budget=32 << 20, max_active=2) as S:
+        submit(S, 24, request(24, 1, 10.0, 0), 7)
+        r = S.wait_all()[0]
+    assert r["status"] == _lib.P3D_ERR_NOMEM
+
+
+def test_bad_requests_raise(cuda):
+    with StokesServer(hbm_budget=1 << 30, max_active=1) as S:
+        with pytest.raises(ValueError):
+            S.submit((4, 4, 4), BITS, np.zeros(3), np.zeros(27 * 64), np.zeros(27 * 64))
+    with pytest.raises(P3DError):
+        StokesServer(hbm_budget=0)
