@@ -12,9 +12,10 @@ steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
-Under torchrun each rank applies its own replica of the mesh (independent
-operators, no collective on the data path) and `value` is the total dof
-throughput of all ranks, timed as the max over ranks.  `--impl reference`
+Under torchrun (N GPUs) the mesh is m x m x (m*N) elements cut into z-slabs
+of m^3 elements, one per rank (weak scaling); a step applies every slab and
+exchanges the node plane shared with each neighbour over NCCL, and `value`
+is the dof throughput of the whole mesh, timed as the max over ranks.  `--impl reference`
 times the reference's own CPU implementation of the same apply
 (MFStokesWrapper_A11_AVX compiled from the pTatin3d sources into
 oracle/_ref, all host threads) on rank 0.
@@ -338,6 +339,14 @@ def run_b200(args):
 
     rank, world, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
+    if world > 1:
+        return run_slabs(args, rank, world, local)
+    if args.slabs:  # the multi-GPU code path on one rank (no neighbour exchange)
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="tcp://127.0.0.1:29531", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=120))
+        return run_slabs(args, 0, 1, local)
     wl = workload(args.size, kind=args.workload)
     m = wl["m"]
     ndof = wl["x"].size
@@ -467,6 +476,99 @@ def run_b200(args):
     return 0
 
 
+def run_slabs(args, rank, world, local):
+    """N GPUs: one mesh of m x m x (m*N) elements cut into z-slabs of m^3
+    elements, one per rank (weak scaling).  A step is one A11 MatMult of the
+    whole mesh: every rank applies its slab, then the node plane shared with
+    each neighbour is exchanged point-to-point over NCCL and added
+    (DMLocalToGlobal(ADD) of a 1-D decomposition)."""
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    from ptatin3d_b200 import PREC_F64, launch_count
+    from ptatin3d_b200 import mesh as M
+    from ptatin3d_b200._lib import BC_MATMULT, check, lib
+    from ptatin3d_b200.slabs import SlabExchange, device_slab_operator, slab_range
+    m = args.size
+    mzg = m * world
+    z0, z1 = slab_range(mzg, rank, world)
+    coords = M.slab_coords(m, m, mzg, z0, z1, frac=0.2, seed=4)
+    eta = M.lognormal_grf_eta(m, m, z1 - z0, seed=4 + 1000 * rank, sigma_decades=2.0, corr_len=0.1)
+    op = device_slab_operator(m, m, mzg, M.FREE_SLIP, coords, eta, rank, world, PREC_F64, local)
+    L = lib()
+    check(L.p3d_op_set_bc_mode(op.h, BC_MATMULT))
+    ex = SlabExchange(m, m, mzg, M.FREE_SLIP, rank, world, device=torch.device("cuda", local))
+    rng = np.random.default_rng(100 + rank)
+    x = torch.tensor(rng.uniform(-1.0, 1.0, size=ex.n_local), dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(x)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    xp, yp = C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())
+
+    def step():
+        check(L.p3d_a11_apply(op.h, xp, yp, sp))
+        ex.add_shared(x, y)
+
+    dist.barrier()
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    n0 = launch_count()
+    with ClockSampler(local) as clk:
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+    launches = launch_count() - n0
+    step_ms = reduce_max(t0.elapsed_time(t1) / args.steps, world)
+    ndof = 3 * (2 * m + 1) ** 2 * (2 * mzg + 1)  # unique dofs of the whole mesh
+    value = ndof / (step_ms * 1e-3) / 1e9
+    # end to end: the slab's x from pinned host memory in, y out, every step
+    xh = x.cpu().pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    ne = max(3, args.steps // 10)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ne):
+        x.copy_(xh, non_blocking=True)
+        step()
+        yh.copy_(y, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(e0.elapsed_time(e1) / ne, world)
+    peak, peak_kind = load_peaks()
+    ab = world * algorithmic_bytes(m)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"A11 MatMult, Q2 {m}x{m}x{mzg} deformed mesh (interior nodes +-0.2h), "
+                                       "log-normal eta, free-slip walls; z-slabs of m^3 elements per GPU with a "
+                                       "shared-plane exchange over NCCL every step",
+                           "elements": m * m * mzg, "dofs": ndof, "parallelism": f"z-slabs x{world}",
+                           "l2": "inputs > L2 per GPU, no flush"},
+                "roofline": {"bound": "hbm", "achieved": ab / world / (step_ms * 1e-3) / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": ab / world / (step_ms * 1e-3) / 1e9 / peak, "traffic": None,
+                             "peak_kind": peak_kind, "note": "per GPU, step time including the exchange"},
+                "cpu_baseline": None,
+                "e2e": {"value": ndof / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+                        "h2d_bytes_per_step": 8 * ex.n_local * world, "d2h_bytes_per_step": 8 * ex.n_local * world},
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    del op
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -477,6 +579,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-solve", action="store_true", help="skip the FP64 vs mixed-precision Stokes solve leg")
     ap.add_argument("--serve-requests", type=int, default=32, help="requests of the served-stream leg (0: skip)")
+    ap.add_argument("--slabs", action="store_true", help="run the multi-GPU z-slab path on a single rank")
     ap.add_argument("--size", type=int, default=96, help="elements per direction")
     ap.add_argument("--workload", default="deformed", choices=["deformed", "layered"])
     args = ap.parse_args()

@@ -101,14 +101,7 @@ template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t 
     if (nbricks_t(a) == 0) return P3D_OK;
     kern<<<nbricks_t(a), 32 * NW_AFF, smem, st>>>(a);
   } else {
-    TileArgs<T> a = tile_args<T>(op, NW_GEN);
-    a.x = x; a.y = y; a.kdat = reinterpret_cast<const T *>(op->kgen);
-    auto kern = stokes_general_kernel<T, NW_GEN, true, false, false>;
-    size_t smem = GeneralSmem<T, NW_GEN, true, false, false>::BYTES;
-    int rc = prep_kernel(kern, smem);
-    if (rc) return rc;
-    if (nbricks_t(a) == 0) return P3D_OK;
-    kern<<<nbricks_t(a), 32 * NW_GEN, smem, st>>>(a);
+    return launch_general<T, true, false, false>(op, x, nullptr, y, nullptr, st);
   }
   count_launch(1);
   return cuda_check(cudaGetLastError(), "a11 launch");
@@ -119,8 +112,11 @@ int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_
 {
   TileArgs<T> a = tile_args<T>(op, NW_GEN);
   a.x = u; a.y = yu; a.p = p; a.yp = yp; a.kdat = reinterpret_cast<const T *>(op->kgen);
-  auto kern = stokes_general_kernel<T, NW_GEN, DA11, DA12, DA21>;
-  size_t smem = GeneralSmem<T, NW_GEN, DA11, DA12, DA21>::BYTES;
+  // FP64: Jacobian columns exchanged by warp shuffles; FP32: per-element geometry table
+  auto kern = sizeof(T) == 8 ? stokes_general_kernel<T, NW_GEN, DA11, DA12, DA21>
+                             : stokes_general_tab_kernel<T, NW_GEN, DA11, DA12, DA21>;
+  size_t smem = sizeof(T) == 8 ? GeneralSmem<T, NW_GEN, DA11, DA12, DA21>::BYTES
+                               : GeneralTabSmem<T, NW_GEN, DA11, DA12, DA21>::BYTES;
   int rc = prep_kernel(kern, smem);
   if (rc) return rc;
   if (nbricks_t(a) == 0) return P3D_OK;

@@ -217,11 +217,206 @@ __global__ void __launch_bounds__(32 * NW, 4) a11_affine_kernel(TileArgs<T> A)
 }
 
 // ------------------------------------------------------- general geometry
+// The Jacobian is recomputed at every Gauss point.  Lane f owns column f of
+// M = [dx_l/dxi_d] (d = row); at each point it fetches the element's other two
+// columns by warp shuffle and forms the adjugate rows in registers:
+//   row_f(M^{-1}) = (col_{f+1} x col_{f+2}) / det,   det = col_f . (col_{f+1} x col_{f+2}),
+// rotated so that row 0 belongs to direction f (the rotation makes the strain
+// exchange a uniform pair of shuffles).  The 1/det factors of the gradient
+// and of the pulled-back stress combine into one scale eta*w/det per point,
+// so the action runs on the unscaled adjugate.  Gauss-point coordinates are
+// interpolated once per element into shared memory and read one point plane
+// (9 points) at a time.  The register cap (6 CTAs of 64 threads per SM, 168
+// registers) trades a few hundred bytes of spills for 50 % more resident warps,
+// which this latency-bound kernel converts into speed (measured at 96^3:
+// 1.65 ms uncapped, 1.45 ms capped; 128 registers: 1.52 ms).
+template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSmem {
+  using BK = Brick<NW>;
+  static constexpr bool NEEDX = DA11 || DA21;
+  static constexpr bool NEEDY = DA11 || DA12;
+  static constexpr int CT = align16(3 * BK::NN, sizeof(T));  // coordinate tile / accumulator
+  static constexpr int CQ = align16(BK::NE * 81, sizeof(T)); // Gauss-point coordinates
+  static constexpr int OX = 0;
+  static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OC = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OK = OC + (CT > CQ ? CT : CQ);
+  static constexpr int TOTAL = OK + align16(BK::NE * 27, sizeof(T));
+  static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
+};
+
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> A)
+{
+  using BK = Brick<NW>;
+  using SM = GeneralSmem<T, NW, DA11, DA12, DA21>;
+  constexpr bool PB = DA12 || DA21;
+  constexpr bool NEEDY = SM::NEEDY;
+  extern __shared__ __align__(16) unsigned char p3d_smem[];
+  T *sm = reinterpret_cast<T *>(p3d_smem);
+  T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_c = sm + SM::OC, *s_k = sm + SM::OK;
+  const BrickPos b = brick_pos<T, NW>(A);
+  if (SM::NEEDX) stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
+  stage_nodes<T, NW>(A, b, A.coords, s_c, false);
+  stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  if (NEEDY) stage_nodes<T, NW>(A, b, A.y, s_y, false);
+  cp_async_wait_all();
+  __syncthreads();
+
+  const LaneMap L = lane_map();
+  const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
+  // coordinates at the Gauss points (lane f: coordinate f) and the pressure-basis scaling
+  T avg = (T)0, rL = (T)1;
+  {
+    T xq[27];
+#pragma unroll
+    for (int n = 0; n < 27; n++) xq[n] = s_c[3 * brick_node<NW>(L.a, L.b, L.c, n) + L.f];
+    if (!valid) { // a unit cube stands in for a slot outside the mesh (its result is never written)
+#pragma unroll
+      for (int n = 0; n < 27; n++) {
+        const int a3 = (L.f == 0) ? n % 3 : ((L.f == 1) ? (n / 3) % 3 : n / 9);
+        xq[n] = (T)(0.5 * a3);
+      }
+    }
+    if (PB) {
+#pragma unroll
+      for (int n = 0; n < 27; n++) avg += xq[n];
+      avg *= cst<T>(1.0 / 27.0);
+      T Lf = (L.f == 0) ? xq[14] - xq[12] : ((L.f == 1) ? xq[16] - xq[10] : xq[22] - xq[4]);
+      rL = (T)1 / Lf;
+    }
+    interp27(xq);
+    __syncthreads(); // every warp has read the coordinate tile: reuse it for the Gauss-point coordinates
+    if (L.active) {
+#pragma unroll
+      for (int n = 0; n < 27; n++) s_c[L.slot * 81 + L.f * 27 + n] = xq[n];
+    }
+  }
+  __syncwarp();
+  const T *X = s_c + L.slot * 81 + L.f * 27;
+  const T *eta_e = s_k + L.slot * 27;
+
+  const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
+  const size_t eg = (size_t)(b.e0x + L.a) + (size_t)A.mx * ((size_t)(b.e0y + L.b) + (size_t)A.my * (b.e0z + L.c));
+  T uq[27], r[27];
+  if (SM::NEEDX) load_interp<T, NW>(s_x, L, uq);
+#pragma unroll
+  for (int n = 0; n < 27; n++) r[n] = (T)0;
+  // pressure dofs rotated to the lane's direction: pr[0] constant, pr[1+m] multiplies hat_{f+m}
+  T pr0 = 0, pr1 = 0, pr2 = 0, pr3 = 0;
+  if (DA12 && valid) {
+    const T p0 = A.p[4 * eg], p1 = A.p[4 * eg + 1], p2 = A.p[4 * eg + 2], p3 = A.p[4 * eg + 3];
+    pr0 = p0;
+    pr1 = L.f == 0 ? p1 : (L.f == 1 ? p2 : p3);
+    pr2 = L.f == 0 ? p2 : (L.f == 1 ? p3 : p1);
+    pr3 = L.f == 0 ? p3 : (L.f == 1 ? p1 : p2);
+  }
+  T ap0 = 0, ap1 = 0, ap2 = 0, ap3 = 0; // A21: [1, hat_f, hat_{f+1}, hat_{f+2}] moments
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    // ---- plane k: column f of M at the plane's 9 points
+    T c0[9], c1[9], c2[9], hat[9];
+    {
+      T xp[27];
+#pragma unroll
+      for (int n = 0; n < 27; n++) xp[n] = X[n];
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          const int q9 = i + 3 * j;
+          c0[q9] = dcol(i, xp[3 * j + 9 * k], xp[1 + 3 * j + 9 * k], xp[2 + 3 * j + 9 * k]);
+          c1[q9] = dcol(j, xp[i + 9 * k], xp[i + 3 + 9 * k], xp[i + 6 + 9 * k]);
+          c2[q9] = dcol(k, xp[i + 3 * j], xp[i + 3 * j + 9], xp[i + 3 * j + 18]);
+          if (PB) hat[q9] = (xp[q9 + 9 * k] - avg) * rL;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const int q9 = i + 3 * j;
+        // the element's other two columns: a = col_{f+1}, bb = col_{f+2}
+        const T a0 = __shfl_sync(0xffffffffu, c0[q9], src1), a1 = __shfl_sync(0xffffffffu, c1[q9], src1),
+                a2 = __shfl_sync(0xffffffffu, c2[q9], src1);
+        const T b0 = __shfl_sync(0xffffffffu, c0[q9], src2), b1 = __shfl_sync(0xffffffffu, c1[q9], src2),
+                b2 = __shfl_sync(0xffffffffu, c2[q9], src2);
+        const T cc0 = c0[q9], cc1 = c1[q9], cc2 = c2[q9];
+        // unscaled rows of M^{-1}: R0 (direction f) = a x b, R1 = b x c, R2 = c x a
+        T Jr[9];
+        Jr[0] = a1 * b2 - a2 * b1; Jr[1] = a2 * b0 - a0 * b2; Jr[2] = a0 * b1 - a1 * b0;
+        Jr[3] = b1 * cc2 - b2 * cc1; Jr[4] = b2 * cc0 - b0 * cc2; Jr[5] = b0 * cc1 - b1 * cc0;
+        Jr[6] = cc1 * a2 - cc2 * a1; Jr[7] = cc2 * a0 - cc0 * a2; Jr[8] = cc0 * a1 - cc1 * a0;
+        const T det = cc0 * Jr[0] + cc1 * Jr[1] + cc2 * Jr[2];
+        const T wq = cst<T>(w1d(i) * w1d(j) * w1d(k));
+        T ro0 = 0, ro1 = 0, ro2 = 0, D0 = 0;
+        if (SM::NEEDX) {
+          P3D_GRAD(uq, i, j, k, g0, g1, g2)
+          if (DA11) {
+            // eta*w*det * (D + D^T) pulled back with M^{-T}: with unscaled rows the
+            // factors of det leave eta*w/det
+            const T sc = (valid ? eta_e[q9 + 9 * k] : (T)0) * wq / det;
+            qp_action(Jr, sc, g0, g1, g2, src1, src2, D0, ro0, ro1, ro2);
+          } else {
+            D0 = Jr[0] * g0 + Jr[1] * g1 + Jr[2] * g2;
+          }
+        }
+        if (PB) {
+          // hats of the element's three lanes, rotated: h0 = hat_f, h1 = hat_{f+1}, h2 = hat_{f+2}
+          const T h0 = hat[q9], h1 = __shfl_sync(0xffffffffu, h0, src1), h2 = __shfl_sync(0xffffffffu, h0, src2);
+          if (DA12) {
+            // -w detJ p_q grad(N) = -w p_q * (adjugate row f) (det cancels)
+            const T t = valid ? -wq * (pr0 + pr1 * h0 + pr2 * h1 + pr3 * h2) : (T)0;
+            ro0 += t * Jr[0]; ro1 += t * Jr[1]; ro2 += t * Jr[2];
+          }
+          if (DA21) {
+            // -w detJ Np du_f/dx_f = -w Np (adjugate row f . grad)
+            const T t = valid ? -wq * D0 : (T)0;
+            ap0 += t; ap1 += t * h0; ap2 += t * h1; ap3 += t * h2;
+          }
+        }
+        if (NEEDY) { P3D_SCATTER(r, i, j, k, ro0, ro1, ro2) }
+      }
+  }
+  if (DA21) {
+    // moments of the three lanes, back to the basis order [1, xh, yh, zh]:
+    // lane f holds [t, t*hat_f, t*hat_{f+1}, t*hat_{f+2}] summed over its own t
+    const T s0 = ap0 + __shfl_sync(0xffffffffu, ap0, src1) + __shfl_sync(0xffffffffu, ap0, src2);
+    // component m of the basis: lane f stores it in slot 1 + (m - f) mod 3
+    T mom[3];
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+      const int sl0 = (m - L.f + 3) % 3;                 // this lane's slot for basis m
+      const int sl1 = (m - (L.f + 1) % 3 + 3) % 3;       // lane src1's slot
+      const int sl2 = (m - (L.f + 2) % 3 + 3) % 3;       // lane src2's slot
+      const T v0 = sl0 == 0 ? ap1 : (sl0 == 1 ? ap2 : ap3);
+      const T w1 = __shfl_sync(0xffffffffu, ap1, src1), w2 = __shfl_sync(0xffffffffu, ap2, src1),
+              w3 = __shfl_sync(0xffffffffu, ap3, src1);
+      const T u1 = __shfl_sync(0xffffffffu, ap1, src2), u2 = __shfl_sync(0xffffffffu, ap2, src2),
+              u3 = __shfl_sync(0xffffffffu, ap3, src2);
+      mom[m] = v0 + (sl1 == 0 ? w1 : (sl1 == 1 ? w2 : w3)) + (sl2 == 0 ? u1 : (sl2 == 1 ? u2 : u3));
+    }
+    if (L.active && valid && L.f == 0) {
+      A.yp[4 * eg] += s0; A.yp[4 * eg + 1] += mom[0]; A.yp[4 * eg + 2] += mom[1]; A.yp[4 * eg + 3] += mom[2];
+    }
+  }
+  if (NEEDY) {
+    interp27T(r);
+    __syncthreads(); // every warp is done with the Gauss-point coordinates: reuse as the accumulator
+    T *s_acc = s_c;
+    for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
+    __syncthreads();
+    accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
+    write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
+  }
+}
+
+// ---------------------------------------- general geometry, table variant
+// Used for FP32, where the table costs less than the shuffle exchange.
 // Geometry is built one Gauss-point plane (9 points, fixed k) at a time: the
 // interpolated coordinates of each element stay in shared memory and every
 // lane inverts 3 of the plane's 9 Jacobians, so the per-element geometry table
 // holds 9 points instead of 27 (3x less shared memory, more CTAs per SM).
-template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSmem {
+template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralTabSmem {
   using BK = Brick<NW>;
   static constexpr bool NEEDX = DA11 || DA21;
   static constexpr bool NEEDY = DA11 || DA12;
@@ -238,10 +433,10 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSme
 };
 
 template <typename T, int NW, bool DA11, bool DA12, bool DA21>
-__global__ void __launch_bounds__(32 * NW) stokes_general_kernel(TileArgs<T> A)
+__global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T> A)
 {
   using BK = Brick<NW>;
-  using SM = GeneralSmem<T, NW, DA11, DA12, DA21>;
+  using SM = GeneralTabSmem<T, NW, DA11, DA12, DA21>;
   constexpr int GQ = SM::GQ;
   constexpr bool PB = DA12 || DA21;
   constexpr bool NEEDY = SM::NEEDY;

@@ -76,6 +76,35 @@ def perturb_interior(coords, mx, my, mz, frac=0.2, seed=0):
     return c.reshape(-1)
 
 
+def _hash_uniform(idx, seed):
+    """Counter-based U[-1, 1) from integer indices (splitmix64 finaliser)."""
+    with np.errstate(over="ignore"):
+        z = (idx.astype(np.uint64) + np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15)) * np.uint64(0xBF58476D1CE4E5B9)
+        z ^= z >> np.uint64(27)
+        z *= np.uint64(0x94D049BB133111EB)
+        z ^= z >> np.uint64(31)
+    return (z >> np.uint64(11)).astype(np.float64) * (2.0 / 9007199254740992.0) - 1.0
+
+
+def slab_coords(mx, my, mz_global, z0, z1, frac=0.2, seed=0):
+    """Coordinates of element layers [z0, z1) of an mx*my*mz_global unit-cube
+    mesh whose interior lattice nodes are moved by U[-frac*h, frac*h] per
+    coordinate.  The displacement of a node is a hash of its global lattice
+    index, so slabs of different ranks agree on the node planes they share
+    and the union of all slabs is one consistent mesh."""
+    nx, ny, nzg = 2 * mx + 1, 2 * my + 1, 2 * mz_global + 1
+    k = np.arange(2 * z0, 2 * z1 + 1)
+    K, J, I = np.meshgrid(k, np.arange(ny), np.arange(nx), indexing="ij")
+    h = np.array([1.0 / (nx - 1), 1.0 / (ny - 1), 1.0 / (nzg - 1)])
+    c = np.stack([I * h[0], J * h[1], K * h[2]], axis=-1)
+    g = (I + nx * (J + ny * K.astype(np.int64))).astype(np.int64)
+    interior = (I > 0) & (I < nx - 1) & (J > 0) & (J < ny - 1) & (K > 0) & (K < nzg - 1)
+    for l in range(3):
+        d = _hash_uniform(3 * g + l, seed) * frac * h[l]
+        c[..., l] += np.where(interior, d, 0.0)
+    return c.reshape(-1)
+
+
 def qp_coords(coords, mx, my, mz):
     """Physical coordinates of the 27 Gauss points of every element: (nel, 27, 3)."""
     nz, ny, nx = lattice_shape(mx, my, mz)

@@ -109,3 +109,22 @@ def test_slab_ranges_cover_mesh():
             assert rs[0][0] == 0 and rs[-1][1] == mz
             assert all(a[1] == b[0] for a, b in zip(rs, rs[1:]))
             assert max(b - a for a, b in rs) - min(b - a for a, b in rs) <= 1
+
+
+def test_slab_coords_agree_on_shared_planes():
+    """Hash-perturbed slabs form one mesh: shared planes match, the union is the global mesh."""
+    mx, my, mzg = 3, 2, 7
+    full = M.slab_coords(mx, my, mzg, 0, mzg, frac=0.2, seed=5).reshape(2 * mzg + 1, -1)
+    P = 3 * (2 * mx + 1) * (2 * my + 1)
+    for world in (2, 3):
+        for r in range(world):
+            z0, z1 = slab_range(mzg, r, world)
+            s = M.slab_coords(mx, my, mzg, z0, z1, frac=0.2, seed=5).reshape(2 * (z1 - z0) + 1, -1)
+            assert np.array_equal(s, full[2 * z0:2 * z1 + 1])
+    # boundary nodes are not moved, interior nodes are, by at most 0.2 h
+    u = M.uniform_coords(mx, my, mzg).reshape(2 * mzg + 1, -1)
+    d = np.abs(full - u).reshape(2 * mzg + 1, 2 * my + 1, 2 * mx + 1, 3)
+    assert d[0].max() == 0 and d[-1].max() == 0 and d[:, 0].max() == 0 and d[:, :, -1].max() == 0
+    h = (1 / (2 * mx), 1 / (2 * my), 1 / (2 * mzg))
+    for l in range(3):
+        assert 0 < d[..., l].max() <= 0.2 * h[l] + 1e-15
