@@ -361,8 +361,8 @@ def run_b200(args):
     sp = C.c_void_p(stream.cuda_stream)
     xp, yp = C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())
 
-    def step():
-        check(L.p3d_a11_apply(op.h, xp, yp, sp))
+    def step():  # MatMult_MFStokes_A11: y = A11 x
+        check(L.p3d_a11_mult(op.h, xp, yp, sp))
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -394,11 +394,11 @@ def run_b200(args):
     check(L.p3d_op_set_bc_mode(op32.h, BC_MATMULT))
     x32, y32 = x.float(), torch.zeros(ndof, dtype=torch.float32, device="cuda")
     for _ in range(3):
-        check(L.p3d_a11_apply(op32.h, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), sp))
+        check(L.p3d_a11_mult(op32.h, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), sp))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        check(L.p3d_a11_apply(op32.h, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), sp))
+        check(L.p3d_a11_mult(op32.h, C.c_void_p(x32.data_ptr()), C.c_void_p(y32.data_ptr()), sp))
     e1.record(stream)
     torch.cuda.synchronize()
     f32_ms = e0.elapsed_time(e1) / args.steps
@@ -507,8 +507,8 @@ def run_slabs(args, rank, world, local):
     sp = C.c_void_p(stream.cuda_stream)
     xp, yp = C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())
 
-    def step():
-        check(L.p3d_a11_apply(op.h, xp, yp, sp))
+    def step():  # slab MatMult, then the shared planes' partial sums
+        check(L.p3d_a11_mult(op.h, xp, yp, sp))
         ex.add_shared(x, y)
 
     dist.barrier()

@@ -104,6 +104,10 @@ int p3d_op_sizes(const p3d_op *op, int64_t *n_velocity, int64_t *n_pressure);
  * src/stokes_operators.c:1181); with P3D_BC_MATMULT the Dirichlet rows are
  * overwritten with x instead. */
 int p3d_a11_apply(p3d_op *op, const void *x, void *y, void *stream);
+/* MatMult contract, y = A11 x (MatMult_MFStokes_A11, src/stokes_operators.c:1142-1205,
+ * which zeroes Yu and then adds): y is overwritten and never read, which
+ * saves the read of y that the "+=" form needs. */
+int p3d_a11_mult(p3d_op *op, const void *x, void *y, void *stream);
 int p3d_a11_diagonal(p3d_op *op, void *d, void *stream);           /* d += diag(A11); Dirichlet slots = 1 with MATMULT */
 int p3d_a12_apply(p3d_op *op, const void *p, void *yu, void *stream);  /* yu += A12 p; Dirichlet rows 0 with MATMULT */
 int p3d_a21_apply(p3d_op *op, const void *u, void *yp, void *stream);  /* yp += A21 u; Dirichlet columns zeroed with MATMULT */

@@ -30,8 +30,9 @@ struct p3d_op {
 };
 
 namespace p3d {
-template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st);
+// overwrite: y is zero on entry and is not read (y = A x); otherwise y += A x
+template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st, bool overwrite = false);
 template <typename T> int launch_diag(p3d_op *op, T *d, cudaStream_t st);
 template <typename T, bool DA11, bool DA12, bool DA21>
-int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st);
+int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st, bool overwrite = false);
 } // namespace p3d

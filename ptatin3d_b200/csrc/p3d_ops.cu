@@ -89,11 +89,12 @@ template <typename K> static int prep_kernel(K kernel, size_t smem)
 template <typename T> static int nbricks_t(const TileArgs<T> &a) { return a.ntx * a.nty * a.ntz; }
 
 // ------------------------------------------------------------- launches ---
-template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st)
+template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st, bool overwrite)
 {
   if (op->geom == P3D_GEOM_AFFINE) {
     TileArgs<T> a = tile_args<T>(op, NW_AFF);
     a.x = x; a.y = y; a.kdat = reinterpret_cast<const T *>(op->kaff);
+    a.overwrite = overwrite ? 1 : 0;
     auto kern = a11_affine_kernel<T, NW_AFF>;
     size_t smem = AffineSmem<T, NW_AFF>::BYTES;
     int rc = prep_kernel(kern, smem);
@@ -101,17 +102,18 @@ template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t 
     if (nbricks_t(a) == 0) return P3D_OK;
     kern<<<nbricks_t(a), 32 * NW_AFF, smem, st>>>(a);
   } else {
-    return launch_general<T, true, false, false>(op, x, nullptr, y, nullptr, st);
+    return launch_general<T, true, false, false>(op, x, nullptr, y, nullptr, st, overwrite);
   }
   count_launch(1);
   return cuda_check(cudaGetLastError(), "a11 launch");
 }
 
 template <typename T, bool DA11, bool DA12, bool DA21>
-int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st)
+int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st, bool overwrite)
 {
   TileArgs<T> a = tile_args<T>(op, NW_GEN);
   a.x = u; a.y = yu; a.p = p; a.yp = yp; a.kdat = reinterpret_cast<const T *>(op->kgen);
+  a.overwrite = overwrite ? 1 : 0;
   // FP64: Jacobian columns exchanged by warp shuffles; FP32: per-element geometry table
   auto kern = sizeof(T) == 8 ? stokes_general_kernel<T, NW_GEN, DA11, DA12, DA21>
                              : stokes_general_tab_kernel<T, NW_GEN, DA11, DA12, DA21>;
@@ -139,16 +141,16 @@ template <typename T> int launch_diag(p3d_op *op, T *d, cudaStream_t st)
   return cuda_check(cudaGetLastError(), "diag launch");
 }
 
-template int launch_a11<double>(p3d_op *, const double *, double *, cudaStream_t);
-template int launch_a11<float>(p3d_op *, const float *, float *, cudaStream_t);
+template int launch_a11<double>(p3d_op *, const double *, double *, cudaStream_t, bool);
+template int launch_a11<float>(p3d_op *, const float *, float *, cudaStream_t, bool);
 template int launch_diag<double>(p3d_op *, double *, cudaStream_t);
 template int launch_diag<float>(p3d_op *, float *, cudaStream_t);
-template int launch_general<double, true, true, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t);
-template int launch_general<float, true, true, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t);
-template int launch_general<double, false, true, false>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t);
-template int launch_general<double, false, false, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t);
-template int launch_general<float, false, true, false>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t);
-template int launch_general<float, false, false, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t);
+template int launch_general<double, true, true, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool);
+template int launch_general<float, true, true, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool);
+template int launch_general<double, false, true, false>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool);
+template int launch_general<double, false, false, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool);
+template int launch_general<float, false, true, false>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool);
+template int launch_general<float, false, false, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool);
 
 // --------------------------------------------------------------- setup ---
 static void free_dev(void *&p)
@@ -375,6 +377,19 @@ int p3d_a11_apply(p3d_op *op, const void *x, void *y, void *stream)
   cudaStream_t st = (cudaStream_t)stream;
   if (op->prec == P3D_PREC_F64) return launch_a11<double>(op, (const double *)x, (double *)y, st);
   return launch_a11<float>(op, (const float *)x, (float *)y, st);
+}
+
+int p3d_a11_mult(p3d_op *op, const void *x, void *y, void *stream)
+{
+  P3D_REQUIRE_SETUP(op);
+  if (!x || !y) return set_error(P3D_ERR_ARG, "a11_mult: null vector");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = 3ull * op->m.gx * op->m.gy * op->m.gz, es = op->prec == P3D_PREC_F64 ? 8 : 4;
+  // y is zeroed (brick-face nodes are accumulated atomically) and never read by the kernel
+  int rc = cuda_check(cudaMemsetAsync(y, 0, n * es, st), "a11_mult memset");
+  if (rc) return rc;
+  if (op->prec == P3D_PREC_F64) return launch_a11<double>(op, (const double *)x, (double *)y, st, true);
+  return launch_a11<float>(op, (const float *)x, (float *)y, st, true);
 }
 
 int p3d_a11_diagonal(p3d_op *op, void *d, void *stream)

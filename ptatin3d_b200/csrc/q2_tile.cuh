@@ -127,6 +127,7 @@ template <typename T> struct TileArgs {
   const T *__restrict__ p;    // pressure in  (A12)
   T *__restrict__ yp;         // pressure out (A21)
   int diag;                   // diagonal kernel: 1 -> Dirichlet slots = 1
+  int overwrite;              // 1: y is zero on entry and not read (y = A x); 0: y += A x
 };
 
 __device__ __forceinline__ bool is_dirichlet(uint32_t m, int ix, int iy, int iz, int ox, int oy, int oz, int ex,
@@ -148,6 +149,8 @@ template <int NW> struct Brick {
   static constexpr int NX = 2 * TX + 1, NY = 2 * TY + 1, NZ = 2 * NW + 1;
   static constexpr int NN = NX * NY * NZ;
   static constexpr int NE = TX * TY * NW;
+  static constexpr int PL = 3 * NX * NY;          // values of one node plane
+  static constexpr int BOT = (NW - 1) * PL;       // bottom planes of warps 1..NW-1 (accumulation)
 };
 
 // Brick geometry for blockIdx.x
@@ -234,25 +237,38 @@ template <typename T> __device__ __forceinline__ void stage_block(const T *__res
 }
 
 // Add the lane's 27 nodal contributions r[] into the brick's node tile s_acc
-// (zeroed by the caller).  Elements whose (a,b,c) parities agree share no node,
-// so the 8 parity classes take turns and every update is a plain shared-memory
-// read-modify-write.  Must be reached by every thread of the CTA.
+// (zeroed by the caller, with the Brick::BOT values after it).  Warp c owns
+// element layer c, i.e. node planes 2c..2c+2; plane 2c+2 is also the bottom
+// plane of warp c+1, so warps c >= 1 put their bottom plane into a private
+// buffer (s_acc + 3*NN) that is folded in after one CTA barrier.  Inside a
+// warp, elements whose (a,b) parities agree share no node: 4 parity classes
+// take turns, separated by __syncwarp, and every update is a plain
+// shared-memory read-modify-write.  Must be reached by every thread.
 template <typename T, int NW>
 __device__ __forceinline__ void accumulate_phases(T *s_acc, const T r[27], int a, int bb, int c, int f, bool doit)
 {
   using BK = Brick<NW>;
-  const int par = (a & 1) | ((bb & 1) << 1) | ((c & 1) << 2);
+  T *s_bot = s_acc + 3 * BK::NN;
+  const int par = (a & 1) | ((bb & 1) << 1);
   T *base = s_acc + 3 * (2 * a + BK::NX * (2 * bb + BK::NY * 2 * c)) + f;
-  for (int ph = 0; ph < 8; ph++) {
+  T *bot = c > 0 ? s_bot + (c - 1) * BK::PL + 3 * (2 * a + BK::NX * 2 * bb) + f : base;
+  for (int ph = 0; ph < 4; ph++) {
     if (doit && ph == par) {
 #pragma unroll
       for (int n = 0; n < 27; n++) {
-        const int off = 3 * ((n % 3) + BK::NX * (((n / 3) % 3) + BK::NY * (n / 9)));
-        base[off] += r[n];
+        const int off = 3 * ((n % 3) + BK::NX * ((n / 3) % 3));
+        if (n / 9 == 0) bot[off] += r[n];
+        else base[off + (n / 9) * BK::PL] += r[n];
       }
     }
-    __syncthreads();
+    __syncwarp();
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < BK::BOT; i += blockDim.x) {
+    const int cz = i / BK::PL + 1;
+    s_acc[2 * cz * BK::PL + (i - (cz - 1) * BK::PL)] += s_bot[i];
+  }
+  __syncthreads();
 }
 
 // Write the accumulated brick tile into y: y = y_staged + acc for nodes no
@@ -295,7 +311,7 @@ __device__ __forceinline__ void write_tile(const TileArgs<T> &A, const BrickPos 
       }
       const T v = s_acc[row * ROWLEN + col];
       if (rs || (k ? xs1 : xs0)) atomicAdd(A.y + g, v);
-      else A.y[g] = s_y[row * ROWLEN + col] + v;
+      else A.y[g] = A.overwrite ? v : s_y[row * ROWLEN + col] + v;
     }
   }
 }

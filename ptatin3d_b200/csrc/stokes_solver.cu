@@ -100,7 +100,7 @@ template <typename T> static int a11(p3d_solver *s, Level &L, const T *x, T *y)
   }
   CU(cudaMemsetAsync(y, 0, L.nv * sizeof(T), s->st), "memset");
   p3d_op *op = sizeof(T) == 8 ? L.op64 : L.op32;
-  return launch_a11<T>(op, x, y, s->st);
+  return launch_a11<T>(op, x, y, s->st, true);
 }
 
 // Chebyshev smoothing on level l: x <- x + K steps for A x = b (zero_guess: x = 0 on entry)
@@ -244,7 +244,7 @@ static int stokes_op(p3d_solver *s, const double *x, double *y)
 {
   CU(cudaMemsetAsync(y, 0, s->N * 8, s->st), "memset");
   Level &F = s->lv.back();
-  return launch_general<double, true, true, true>(F.op64, x, x + s->nu, y, y + s->nu, s->st);
+  return launch_general<double, true, true, true>(F.op64, x, x + s->nu, y, y + s->nu, s->st, true);
 }
 
 // ||v||_2 (FP64)

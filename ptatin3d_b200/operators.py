@@ -112,10 +112,9 @@ class MatA11MF(_Op):
 
     def mult(self, x: torch.Tensor, y: torch.Tensor):
         """MatMult_MFStokes_A11: y = A11 x with Dirichlet columns zeroed and rows y_k = x_k."""
-        y.zero_()
         self._bc(BC_MATMULT)
-        check(lib().p3d_a11_apply(self.h, self._vec(x, self.n_velocity, "x"),
-                                  self._vec(y, self.n_velocity, "y"), _stream()))
+        check(lib().p3d_a11_mult(self.h, self._vec(x, self.n_velocity, "x"),
+                                 self._vec(y, self.n_velocity, "y"), _stream()))
 
     def mult_add(self, x: torch.Tensor, y: torch.Tensor):
         """y += A11 x with the MatMult boundary convention (Dirichlet rows overwritten)."""

@@ -65,7 +65,7 @@ def test_a11_auto_detects_affine(cuda):
 def test_a11_matmult_sinker(cuda, restatement, deform):
     case = sinker_case(12, deform=deform)
     op = make_op(case)
-    y = torch.empty(case["x"].size, dtype=torch.float64, device="cuda")
+    y = torch.full((case["x"].size,), float("nan"), dtype=torch.float64, device="cuda")  # overwritten, never read
     op.mult(T(case["x"]), y)
     d, c, e = case["dims"], case["coords"], case["eta"].reshape(-1)
     ref = matmult_a11(lambda v: restatement.a11_raw(d, c, e, v), case["x"], case["mask"])
