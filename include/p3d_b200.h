@@ -119,6 +119,10 @@ int p3d_stokes_apply(p3d_op *op, const void *u, const void *p, void *yu, void *y
  * CopyFrom_A11_CUDA does; its caller has zeroed Yu, so this equals the
  * SpMVOp "+=" contract), and returns when y is complete. */
 int p3d_a11_apply_host(p3d_op *op, const double *x_host, double *y_host);
+/* Split p3d_a11_apply_host into `chunks` z-ranges of brick layers (0 =
+ * automatic: 16 for meshes of 4M dofs and more, else 1) whose host->device
+ * copies, applies and device->host copies overlap on three streams. */
+int p3d_op_set_host_chunks(p3d_op *op, int chunks);
 
 /* Same result as p3d_a11_apply_host, without allocating any device memory
  * (no counterpart in the reference).  For callers that may not call

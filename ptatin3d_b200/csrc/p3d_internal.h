@@ -26,13 +26,21 @@ struct p3d_op {
   void *kaff = nullptr;   // affine path: J^{-1} + eta*w*detJ, brick order (NW_AFF)
   void *hx = nullptr, *hy = nullptr; // host-apply staging
   unsigned long long *flag = nullptr; // affinity test result (kept: re-setup allocates nothing)
+  cudaStream_t s_h2d = nullptr, s_d2h = nullptr; // host-apply copy streams
+  cudaEvent_t ev[32] = {};                      // host-apply chunk events (16 chunks x {x in, y done})
+  int host_chunks = 0;                           // 0: automatic
   cudaStream_t stream = nullptr;     // setup / host-apply stream
 };
 
 namespace p3d {
-// overwrite: y is zero on entry and is not read (y = A x); otherwise y += A x
-template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st, bool overwrite = false);
+// overwrite: y is zero on entry and is not read (y = A x); otherwise y += A x.
+// [tzb, tze): range of brick layers along z to apply (tze < 0: all).
+template <typename T>
+int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st, bool overwrite = false, int tzb = 0, int tze = -1);
 template <typename T> int launch_diag(p3d_op *op, T *d, cudaStream_t st);
 template <typename T, bool DA11, bool DA12, bool DA21>
-int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st, bool overwrite = false);
+int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st, bool overwrite = false,
+                   int tzb = 0, int tze = -1);
+// brick layer height along z of the A11 path the operator uses
+int a11_brick_height(const p3d_op *op);
 } // namespace p3d

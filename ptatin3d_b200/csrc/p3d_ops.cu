@@ -1,6 +1,7 @@
 // Operator objects and the C-ABI of libp3d_b200.so (see include/p3d_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -89,7 +90,18 @@ template <typename K> static int prep_kernel(K kernel, size_t smem)
 template <typename T> static int nbricks_t(const TileArgs<T> &a) { return a.ntx * a.nty * a.ntz; }
 
 // ------------------------------------------------------------- launches ---
-template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st, bool overwrite)
+// bricks of the layer range [tzb, tze) (tze < 0: all layers); sets a.brick0
+template <typename T> static int brick_range(TileArgs<T> &a, int tzb, int tze)
+{
+  if (tze < 0 || tze > a.ntz) tze = a.ntz;
+  if (tzb < 0) tzb = 0;
+  a.brick0 = tzb * a.ntx * a.nty;
+  return tze > tzb ? (tze - tzb) * a.ntx * a.nty : 0;
+}
+
+int a11_brick_height(const p3d_op *op) { return op->geom == P3D_GEOM_AFFINE ? NW_AFF : NW_GEN; }
+
+template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st, bool overwrite, int tzb, int tze)
 {
   if (op->geom == P3D_GEOM_AFFINE) {
     TileArgs<T> a = tile_args<T>(op, NW_AFF);
@@ -99,17 +111,18 @@ template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t 
     size_t smem = AffineSmem<T, NW_AFF>::BYTES;
     int rc = prep_kernel(kern, smem);
     if (rc) return rc;
-    if (nbricks_t(a) == 0) return P3D_OK;
-    kern<<<nbricks_t(a), 32 * NW_AFF, smem, st>>>(a);
+    const int nb = brick_range(a, tzb, tze);
+    if (nb == 0) return P3D_OK;
+    kern<<<nb, 32 * NW_AFF, smem, st>>>(a);
   } else {
-    return launch_general<T, true, false, false>(op, x, nullptr, y, nullptr, st, overwrite);
+    return launch_general<T, true, false, false>(op, x, nullptr, y, nullptr, st, overwrite, tzb, tze);
   }
   count_launch(1);
   return cuda_check(cudaGetLastError(), "a11 launch");
 }
 
 template <typename T, bool DA11, bool DA12, bool DA21>
-int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st, bool overwrite)
+int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st, bool overwrite, int tzb, int tze)
 {
   TileArgs<T> a = tile_args<T>(op, NW_GEN);
   a.x = u; a.y = yu; a.p = p; a.yp = yp; a.kdat = reinterpret_cast<const T *>(op->kgen);
@@ -121,8 +134,9 @@ int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_
                                : GeneralTabSmem<T, NW_GEN, DA11, DA12, DA21>::BYTES;
   int rc = prep_kernel(kern, smem);
   if (rc) return rc;
-  if (nbricks_t(a) == 0) return P3D_OK;
-  kern<<<nbricks_t(a), 32 * NW_GEN, smem, st>>>(a);
+  const int nb = brick_range(a, tzb, tze);
+  if (nb == 0) return P3D_OK;
+  kern<<<nb, 32 * NW_GEN, smem, st>>>(a);
   count_launch(1);
   return cuda_check(cudaGetLastError(), "stokes launch");
 }
@@ -141,16 +155,16 @@ template <typename T> int launch_diag(p3d_op *op, T *d, cudaStream_t st)
   return cuda_check(cudaGetLastError(), "diag launch");
 }
 
-template int launch_a11<double>(p3d_op *, const double *, double *, cudaStream_t, bool);
-template int launch_a11<float>(p3d_op *, const float *, float *, cudaStream_t, bool);
+template int launch_a11<double>(p3d_op *, const double *, double *, cudaStream_t, bool, int, int);
+template int launch_a11<float>(p3d_op *, const float *, float *, cudaStream_t, bool, int, int);
 template int launch_diag<double>(p3d_op *, double *, cudaStream_t);
 template int launch_diag<float>(p3d_op *, float *, cudaStream_t);
-template int launch_general<double, true, true, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool);
-template int launch_general<float, true, true, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool);
-template int launch_general<double, false, true, false>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool);
-template int launch_general<double, false, false, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool);
-template int launch_general<float, false, true, false>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool);
-template int launch_general<float, false, false, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool);
+template int launch_general<double, true, true, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool, int, int);
+template int launch_general<float, true, true, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool, int, int);
+template int launch_general<double, false, true, false>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool, int, int);
+template int launch_general<double, false, false, true>(p3d_op *, const double *, const double *, double *, double *, cudaStream_t, bool, int, int);
+template int launch_general<float, false, true, false>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool, int, int);
+template int launch_general<float, false, false, true>(p3d_op *, const float *, const float *, float *, float *, cudaStream_t, bool, int, int);
 
 // --------------------------------------------------------------- setup ---
 static void free_dev(void *&p)
@@ -311,6 +325,10 @@ int p3d_op_destroy(p3d_op *op)
   free_dev(op->hx);
   free_dev(op->hy);
   if (op->flag) cudaFree(op->flag);
+  for (auto &e : op->ev)
+    if (e) cudaEventDestroy(e);
+  if (op->s_h2d) cudaStreamDestroy(op->s_h2d);
+  if (op->s_d2h) cudaStreamDestroy(op->s_d2h);
   if (op->stream) cudaStreamDestroy(op->stream);
   delete op;
   return P3D_OK;
@@ -432,22 +450,64 @@ int p3d_stokes_apply(p3d_op *op, const void *u, const void *p, void *yu, void *y
   return launch_general<float, true, true, true>(op, (const float *)u, (const float *)p, (float *)yu, (float *)yp, st);
 }
 
+int p3d_op_set_host_chunks(p3d_op *op, int chunks)
+{
+  if (!op || chunks < 0 || chunks > 16) return set_error(P3D_ERR_ARG, "set_host_chunks: chunks in [0,16]");
+  op->host_chunks = chunks;
+  return P3D_OK;
+}
+
 int p3d_a11_apply_host(p3d_op *op, const double *xh, double *yh)
 {
   P3D_REQUIRE_SETUP(op);
   if (!xh || !yh) return set_error(P3D_ERR_ARG, "a11_apply_host: null vector");
   if (op->prec != P3D_PREC_F64) return set_error(P3D_ERR_ARG, "a11_apply_host: FP64 operators only");
   cudaSetDevice(op->device);
-  size_t n = 3ull * op->m.gx * op->m.gy * op->m.gz;
+  const p3d_mesh_desc &m = op->m;
+  const size_t P = 3ull * m.gx * m.gy, n = P * m.gz; // doubles per lattice plane, in total
   int rc;
   if (!op->hx && (rc = dev_alloc(&op->hx, n * 8, "host-apply x"))) return rc;
   if (!op->hy && (rc = dev_alloc(&op->hy, n * 8, "host-apply y"))) return rc;
-  cudaStream_t st = op->stream;
-  if ((rc = cuda_check(cudaMemcpyAsync(op->hx, xh, n * 8, cudaMemcpyHostToDevice, st), "H2D x"))) return rc;
-  if ((rc = cuda_check(cudaMemsetAsync(op->hy, 0, n * 8, st), "zero y"))) return rc;
-  if ((rc = launch_a11<double>(op, (const double *)op->hx, (double *)op->hy, st))) return rc;
-  if ((rc = cuda_check(cudaMemcpyAsync(yh, op->hy, n * 8, cudaMemcpyDeviceToHost, st), "D2H y"))) return rc;
-  return cuda_check(cudaStreamSynchronize(st), "host apply sync");
+  if (!op->s_h2d) {
+    if ((rc = cuda_check(cudaStreamCreateWithFlags(&op->s_h2d, cudaStreamNonBlocking), "h2d stream"))) return rc;
+    if ((rc = cuda_check(cudaStreamCreateWithFlags(&op->s_d2h, cudaStreamNonBlocking), "d2h stream"))) return rc;
+    for (auto &e : op->ev)
+      if ((rc = cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) return rc;
+  }
+  // Pipeline along z: chunk k's x planes go in on s_h2d while chunk k-1 is
+  // applied on the compute stream, and the y planes no later chunk touches go
+  // out on s_d2h.  A chunk is a range of whole brick layers; elements of
+  // layers [z0, z1) read node planes oz+2z0 .. oz+2z1 and write the same, and
+  // plane oz+2z1 also receives the next chunk's (atomic) contributions.
+  const int H = a11_brick_height(op), ntz = (m.mz + H - 1) / H;
+  int K = op->host_chunks > 0 ? op->host_chunks : (n >= (size_t)4 << 20 ? 16 : 1);
+  if (K > ntz) K = ntz < 1 ? 1 : ntz;
+  cudaStream_t cs = op->stream;
+  double *dx = (double *)op->hx, *dy = (double *)op->hy;
+  if ((rc = cuda_check(cudaMemsetAsync(dy, 0, n * 8, cs), "zero y"))) return rc;
+  size_t p0 = 0, q0 = 0; // next x plane to send, next y plane to return
+  for (int k = 0; k < K; k++) {
+    const int tzb = (int)((long long)k * ntz / K), tze = (int)((long long)(k + 1) * ntz / K);
+    const int z1 = std::min(tze * H, m.mz);
+    const size_t p1 = k == K - 1 ? (size_t)m.gz : (size_t)(m.oz + 2 * z1 + 1); // x planes [p0, p1)
+    const size_t q1 = k == K - 1 ? (size_t)m.gz : (size_t)(m.oz + 2 * z1);     // final y planes [q0, q1)
+    cudaEvent_t ex = op->ev[2 * k], ec = op->ev[2 * k + 1];
+    if (p1 > p0 && (rc = cuda_check(cudaMemcpyAsync(dx + p0 * P, xh + p0 * P, (p1 - p0) * P * 8, cudaMemcpyHostToDevice,
+                                                    op->s_h2d), "H2D x")))
+      return rc;
+    p0 = std::max(p0, p1);
+    if ((rc = cuda_check(cudaEventRecord(ex, op->s_h2d), "record"))) return rc;
+    if ((rc = cuda_check(cudaStreamWaitEvent(cs, ex, 0), "wait"))) return rc;
+    if ((rc = launch_a11<double>(op, dx, dy, cs, true, tzb, tze))) return rc;
+    if ((rc = cuda_check(cudaEventRecord(ec, cs), "record"))) return rc;
+    if ((rc = cuda_check(cudaStreamWaitEvent(op->s_d2h, ec, 0), "wait"))) return rc;
+    if (q1 > q0 && (rc = cuda_check(cudaMemcpyAsync(yh + q0 * P, dy + q0 * P, (q1 - q0) * P * 8, cudaMemcpyDeviceToHost,
+                                                    op->s_d2h), "D2H y")))
+      return rc;
+    q0 = std::max(q0, q1);
+  }
+  if ((rc = cuda_check(cudaStreamSynchronize(op->s_d2h), "host apply sync"))) return rc;
+  return cuda_check(cudaStreamSynchronize(cs), "host apply sync");
 }
 
 } // extern "C"

@@ -128,6 +128,7 @@ template <typename T> struct TileArgs {
   T *__restrict__ yp;         // pressure out (A21)
   int diag;                   // diagonal kernel: 1 -> Dirichlet slots = 1
   int overwrite;              // 1: y is zero on entry and not read (y = A x); 0: y += A x
+  int brick0;                 // first brick of the launch (z-chunked launches)
 };
 
 __device__ __forceinline__ bool is_dirichlet(uint32_t m, int ix, int iy, int iz, int ox, int oy, int oz, int ex,
@@ -164,7 +165,7 @@ struct BrickPos {
 template <typename T, int NW> __device__ __forceinline__ BrickPos brick_pos(const TileArgs<T> &A)
 {
   BrickPos b;
-  int t = blockIdx.x;
+  int t = blockIdx.x + A.brick0;
   b.tx = t % A.ntx;
   b.ty = (t / A.ntx) % A.nty;
   b.tz = t / (A.ntx * A.nty);

@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(32 * NW, 4) a11_affine_kernel(TileArgs<T> A)
   T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_k = sm + SM::OK, *s_acc = sm + SM::OA;
   const BrickPos b = brick_pos<T, NW>(A);
   stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
-  stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * SM::KS, s_k, BK::NE * SM::KS);
+  stage_block(A.kdat + (size_t)(blockIdx.x + A.brick0) * BK::NE * SM::KS, s_k, BK::NE * SM::KS);
   if (!A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
   for (int i = threadIdx.x; i < 3 * BK::NN + BK::BOT; i += blockDim.x) s_acc[i] = (T)0;
   cp_async_wait_all();
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
   const BrickPos b = brick_pos<T, NW>(A);
   if (SM::NEEDX) stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
   stage_nodes<T, NW>(A, b, A.coords, s_c, false);
-  stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  stage_block(A.kdat + (size_t)(blockIdx.x + A.brick0) * BK::NE * 27, s_k, BK::NE * 27);
   if (NEEDY && !A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
   cp_async_wait_all();
   __syncthreads();
@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
   const BrickPos b = brick_pos<T, NW>(A);
   if (SM::NEEDX) stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
   stage_nodes<T, NW>(A, b, A.coords, s_c, false);
-  stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  stage_block(A.kdat + (size_t)(blockIdx.x + A.brick0) * BK::NE * 27, s_k, BK::NE * 27);
   if (NEEDY && !A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
   cp_async_wait_all();
   __syncthreads();
@@ -613,7 +613,7 @@ __global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
   T *s_y = sm + SM::OY, *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
   const BrickPos b = brick_pos<T, NW>(A);
   stage_nodes<T, NW>(A, b, A.coords, s_c, false);
-  stage_block(A.kdat + (size_t)blockIdx.x * BK::NE * 27, s_k, BK::NE * 27);
+  stage_block(A.kdat + (size_t)(blockIdx.x + A.brick0) * BK::NE * 27, s_k, BK::NE * 27);
   stage_nodes<T, NW>(A, b, A.y, s_y, false);
   cp_async_wait_all();
   __syncthreads();
