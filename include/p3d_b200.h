@@ -187,8 +187,15 @@ typedef struct p3d_solver_opts {
                            quadrature point, the reference's ScaledMassMatrix) or
                            P3D_SCHUR_ETA_GEOMEAN (1/eta_e, eta_e the element's
                            geometric-mean viscosity)                              */
+  int32_t coarse_eta;   /* Gauss-point viscosity of rediscretised coarse levels:
+                           P3D_COARSE_ETA_GEOMEAN (geometric mean of the nearest
+                           finer Gauss points) or P3D_COARSE_ETA_Q1 (the
+                           reference's Q1 projection hierarchy: nodal projection,
+                           scaled restriction, clamped interpolation)            */
 } p3d_solver_opts;
 
+#define P3D_COARSE_ETA_GEOMEAN 0
+#define P3D_COARSE_ETA_Q1 1
 #define P3D_SCHUR_ETA_QP 0
 #define P3D_SCHUR_ETA_GEOMEAN 1
 #define P3D_COARSE_GALERKIN 0

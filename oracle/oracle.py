@@ -90,6 +90,25 @@ class Restatement:
         self.L.o_a11_element_matrix(_p(np.ascontiguousarray(elcoords, dtype=np.float64)), _p(np.ascontiguousarray(eta_e, dtype=np.float64)), _p(K))
         return K.reshape(81, 81)
 
+    def eta_hierarchy(self, dims, eta, nlevels):
+        """Gauss-point viscosity of every level, finest first, by the reference's
+        Q1 projection hierarchy (src/material_point_utils.c:1267-1420)."""
+        for f, n in (("o_eta_project_nodes", 4), ("o_eta_restrict_nodes", 5), ("o_eta_nodes_to_qp", 5)):
+            getattr(self.L, f).argtypes = [C.c_int] * 3 + [_dp] * 2
+        mx, my, mz = dims
+        v = np.zeros((2 * mx + 1) * (2 * my + 1) * (2 * mz + 1))
+        self.L.o_eta_project_nodes(mx, my, mz, _p(np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)), _p(v))
+        out = [np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)]
+        for _ in range(nlevels - 1):
+            mx, my, mz = mx // 2, my // 2, mz // 2
+            vc = np.zeros((2 * mx + 1) * (2 * my + 1) * (2 * mz + 1))
+            self.L.o_eta_restrict_nodes(2 * mx + 1, 2 * my + 1, 2 * mz + 1, _p(v), _p(vc))
+            e = np.zeros(27 * mx * my * mz)
+            self.L.o_eta_nodes_to_qp(mx, my, mz, _p(vc), _p(e))
+            out.append(e)
+            v = vc
+        return out
+
     def prolong(self, cn, ndof, xc):
         fn = [2 * c - 1 for c in cn]
         xf = np.zeros(fn[0] * fn[1] * fn[2] * ndof)

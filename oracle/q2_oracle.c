@@ -442,6 +442,95 @@ void o_restrict(int cnx, int cny, int cnz, int ndof, const double *xf, double *x
       }
 }
 
+/* ------------------------------------------- coefficient hierarchy --- */
+/* The reference's coefficient hierarchy for Gauss-point viscosity
+ * (SwarmUpdateGaussPropertiesLocalL2Projection_Q1_MPntPStokes_Hierarchy,
+ * src/material_point_utils.c:1267-1420, projection types -1/0 with
+ * -mp_hierarchy_projection_type 0).  The Q2 node lattice is treated as a Q1
+ * lattice with one scalar per node. */
+
+/* Q1 shape functions of the element at reference point xi (element_utils_q1.c:32-47),
+ * mapped to the element's Q2 corner nodes 0,2,6,8,18,20,24,26 */
+static void o_q1_corner_weights(const double xi[3], double w[27])
+{
+  for (int n = 0; n < 27; n++) w[n] = 0.0;
+  for (int c = 0; c < 2; c++)
+    for (int b = 0; b < 2; b++)
+      for (int a = 0; a < 2; a++)
+        w[2 * a + 3 * (2 * b) + 9 * (2 * c)] = 0.125 * (a ? 1.0 + xi[0] : 1.0 - xi[0]) *
+                                               (b ? 1.0 + xi[1] : 1.0 - xi[1]) * (c ? 1.0 + xi[2] : 1.0 - xi[2]);
+}
+
+/* fine level: nodal field v = A / B with, per element and Gauss point q,
+ * A_n += N_n(q) eta_q, B_n += N_n(q); N = the Q1 corner weights at the corners
+ * and 1 at the 19 other Q2 nodes
+ * (_BuildQ1CoefficientProjection_QuadraturePoints_MPntPStokes_FineGrid, :1138-1257) */
+void o_eta_project_nodes(int mx, int my, int mz, const double *eta, double *v)
+{
+  o_tables();
+  o_mesh m = {mx, my, mz};
+  long nx = 2 * mx + 1, ny = 2 * my + 1, nn = nx * ny * (2 * mz + 1);
+  double *B = (double *)calloc((size_t)nn, sizeof(double));
+  memset(v, 0, sizeof(double) * (size_t)nn);
+  long nel = (long)mx * my * mz;
+  for (long e = 0; e < nel; e++) {
+    long nid[27];
+    o_element_nodes(&m, e, nid);
+    for (int q = 0; q < 27; q++) {
+      double xi[3] = {GP[q % 3], GP[(q / 3) % 3], GP[q / 9]}, w[27];
+      o_q1_corner_weights(xi, w);
+      for (int n = 0; n < 27; n++) {
+        const int corner = (n % 3 != 1) && ((n / 3) % 3 != 1) && (n / 9 != 1);
+        const double N = corner ? w[n] : 1.0;
+        v[nid[n]] += N * eta[27 * e + q];
+        B[nid[n]] += N;
+      }
+    }
+  }
+  for (long i = 0; i < nn; i++) v[i] /= B[i];
+  free(B);
+}
+
+/* next coarser level: vc = (P^T vf) ./ (P^T 1) (MatRestrict with DMCreateInterpolationScale, :1379-1394) */
+void o_eta_restrict_nodes(int cnx, int cny, int cnz, const double *vf, double *vc)
+{
+  long fn = (long)(2 * cnx - 1) * (2 * cny - 1) * (2 * cnz - 1), cn = (long)cnx * cny * cnz;
+  double *ones = (double *)malloc(sizeof(double) * (size_t)fn), *den = (double *)malloc(sizeof(double) * (size_t)cn);
+  for (long i = 0; i < fn; i++) ones[i] = 1.0;
+  o_restrict(cnx, cny, cnz, 1, vf, vc);
+  o_restrict(cnx, cny, cnz, 1, ones, den);
+  for (long i = 0; i < cn; i++) vc[i] /= den[i];
+  free(ones);
+  free(den);
+}
+
+/* Gauss-point values of a level from its nodal field: Q1 interpolation of the
+ * 8 corner values, clamped to the range of the element's 27 nodal values
+ * (_SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_InterpolateToQuadratePoints, :894-1030) */
+void o_eta_nodes_to_qp(int mx, int my, int mz, const double *v, double *eta)
+{
+  o_tables();
+  o_mesh m = {mx, my, mz};
+  long nel = (long)mx * my * mz;
+  for (long e = 0; e < nel; e++) {
+    long nid[27];
+    o_element_nodes(&m, e, nid);
+    double lo = 1e32, hi = -1e32;
+    for (int n = 0; n < 27; n++) {
+      if (v[nid[n]] < lo) lo = v[nid[n]];
+      if (v[nid[n]] > hi) hi = v[nid[n]];
+    }
+    for (int q = 0; q < 27; q++) {
+      double xi[3] = {GP[q % 3], GP[(q / 3) % 3], GP[q / 9]}, w[27], s = 0.0;
+      o_q1_corner_weights(xi, w);
+      for (int n = 0; n < 27; n++) s += w[n] * v[nid[n]];
+      if (s < lo) s = lo;
+      if (s > hi) s = hi;
+      eta[27 * e + q] = s;
+    }
+  }
+}
+
 /* --------------------------------------------- Dirichlet conventions --- */
 /* x_local[k] = 0 where mask[k] (src/dmda_bcs.c:500-526) */
 void o_bc_zero(long n, const uint8_t *mask, double *x)

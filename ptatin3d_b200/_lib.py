@@ -18,6 +18,7 @@ P3D_ERR_ARG, P3D_ERR_CUDA, P3D_ERR_STATE, P3D_ERR_NOMEM, P3D_ERR_NOCONV, P3D_ERR
 PREC_F64, PREC_F32 = 64, 32
 COARSE_GALERKIN, COARSE_REDISC = 0, 1
 SCHUR_ETA_QP, SCHUR_ETA_GEOMEAN = 0, 1
+COARSE_ETA_GEOMEAN, COARSE_ETA_Q1 = 0, 1
 MAX_RESTART = 120
 COARSE_MAX_DOFS = 16384
 GEOM_AUTO, GEOM_GENERAL, GEOM_AFFINE = 0, 1, 2
@@ -47,7 +48,7 @@ class SolverOpts(C.Structure):
                 ("esteig_its", C.c_int32), ("mg_precision", C.c_int32), ("restart", C.c_int32),
                 ("max_it", C.c_int32), ("rtol", C.c_double), ("atol", C.c_double), ("use_graph", C.c_int32),
                 ("verbose", C.c_int32), ("inner_its", C.c_int32), ("coarse_op", C.c_int32),
-                ("schur_eta", C.c_int32)]
+                ("schur_eta", C.c_int32), ("coarse_eta", C.c_int32)]
 
 
 class Request(C.Structure):

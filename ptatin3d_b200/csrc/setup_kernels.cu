@@ -11,6 +11,9 @@
 //   s_restrict_eta : Gauss-point viscosity of a coarse level from the next finer
 //                    one (geometric mean over the fine points nearest each coarse
 //                    point; keeps eta positive across contrasts of 1e5)
+//   s_eta_project / s_eta_to_qp: the reference's Q1 projection hierarchy of
+//                    Gauss-point viscosity (nodal projection, scaled
+//                    restriction, clamped interpolation back to Gauss points)
 //   s_inject_coords: coarse coordinates by injection on the node lattice
 //                    (src/dmda_project_coords.c:73-95)
 #include <cuda_runtime.h>
@@ -195,6 +198,104 @@ __global__ void k_inject(int cnx, int cny, int cnz, const double *__restrict__ c
     size_t f = (size_t)(2 * I) + (size_t)fnx * ((size_t)(2 * J) + (size_t)fny * (2 * K));
     for (int l = 0; l < 3; l++) cc[3 * i + l] = cf[3 * f + l];
   }
+}
+
+// ---- the reference's Q1 projection hierarchy of Gauss-point viscosity
+// (src/material_point_utils.c:1138-1257, 1379-1394, 894-1030)
+__device__ __forceinline__ double q1w(int corner, double xi, double eta, double zeta)
+{
+  const int a = corner & 1, b = (corner >> 1) & 1, c = corner >> 2;
+  return 0.125 * (a ? 1.0 + xi : 1.0 - xi) * (b ? 1.0 + eta : 1.0 - eta) * (c ? 1.0 + zeta : 1.0 - zeta);
+}
+__device__ __forceinline__ double gp1(int i) { return i == 0 ? -0.77459666924148337704 : (i == 1 ? 0.0 : 0.77459666924148337704); }
+
+// A_n += N_n(q) eta_q, B_n += N_n(q): Q1 corner weights at the 8 corners, 1 at the other Q2 nodes
+__global__ void k_eta_project(int mx, int my, int mz, const double *__restrict__ eta, double *__restrict__ A,
+                              double *__restrict__ B)
+{
+  const size_t nel = (size_t)mx * my * mz;
+  const int nx = 2 * mx + 1, ny = 2 * my + 1;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nel; e += (size_t)gridDim.x * blockDim.x) {
+    const int ex = e % mx, ey = (e / mx) % my, ez = e / ((size_t)mx * my);
+    double sc[8] = {}, wc[8] = {}, se = 0.0;
+    for (int q = 0; q < 27; q++) {
+      const double v = eta[27 * e + q], xi = gp1(q % 3), et = gp1((q / 3) % 3), ze = gp1(q / 9);
+      se += v;
+      for (int c = 0; c < 8; c++) {
+        const double w = q1w(c, xi, et, ze);
+        sc[c] += w * v;
+        wc[c] += w;
+      }
+    }
+    for (int n = 0; n < 27; n++) {
+      const int a = n % 3, b = (n / 3) % 3, c = n / 9;
+      const size_t g = (size_t)(2 * ex + a) + (size_t)nx * ((size_t)(2 * ey + b) + (size_t)ny * (2 * ez + c));
+      if (a != 1 && b != 1 && c != 1) {
+        const int corner = (a >> 1) | ((b >> 1) << 1) | ((c >> 1) << 2);
+        atomicAdd(A + g, sc[corner]);
+        atomicAdd(B + g, wc[corner]);
+      } else {
+        atomicAdd(A + g, se);
+        atomicAdd(B + g, 27.0);
+      }
+    }
+  }
+}
+__global__ void k_divide(size_t n, double *__restrict__ a, const double *__restrict__ b)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) a[i] /= b[i];
+}
+// Gauss-point values from the nodal field: Q1 interpolation of the corners, clamped to the element's nodal range
+__global__ void k_eta_to_qp(int mx, int my, int mz, const double *__restrict__ v, double *__restrict__ eta)
+{
+  const size_t nel = (size_t)mx * my * mz;
+  const int nx = 2 * mx + 1, ny = 2 * my + 1;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nel; e += (size_t)gridDim.x * blockDim.x) {
+    const int ex = e % mx, ey = (e / mx) % my, ez = e / ((size_t)mx * my);
+    double lo = 1e32, hi = -1e32, vc[8];
+    for (int n = 0; n < 27; n++) {
+      const int a = n % 3, b = (n / 3) % 3, c = n / 9;
+      const double x = v[(size_t)(2 * ex + a) + (size_t)nx * ((size_t)(2 * ey + b) + (size_t)ny * (2 * ez + c))];
+      lo = fmin(lo, x);
+      hi = fmax(hi, x);
+      if (a != 1 && b != 1 && c != 1) vc[(a >> 1) | ((b >> 1) << 1) | ((c >> 1) << 2)] = x;
+    }
+    for (int q = 0; q < 27; q++) {
+      const double xi = gp1(q % 3), et = gp1((q / 3) % 3), ze = gp1(q / 9);
+      double s = 0.0;
+      for (int c = 0; c < 8; c++) s += q1w(c, xi, et, ze) * vc[c];
+      eta[27 * e + q] = fmin(fmax(s, lo), hi);
+    }
+  }
+}
+
+void s_eta_project(int mx, int my, int mz, const double *eta, double *A, double *B, cudaStream_t s)
+{
+  const size_t nn = (size_t)(2 * mx + 1) * (2 * my + 1) * (2 * mz + 1);
+  cudaMemsetAsync(A, 0, nn * 8, s);
+  cudaMemsetAsync(B, 0, nn * 8, s);
+  k_eta_project<<<sgrid((size_t)mx * my * mz), 128, 0, s>>>(mx, my, mz, eta, A, B);
+  k_divide<<<sgrid(nn), 128, 0, s>>>(nn, A, B);
+  count_launch(2);
+}
+__global__ void k_fill(size_t n, double v, double *__restrict__ a)
+{
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) a[i] = v;
+}
+void s_fill(size_t n, double v, double *a, cudaStream_t s)
+{
+  k_fill<<<sgrid(n), 128, 0, s>>>(n, v, a);
+  count_launch(1);
+}
+void s_divide(size_t n, double *a, const double *b, cudaStream_t s)
+{
+  k_divide<<<sgrid(n), 128, 0, s>>>(n, a, b);
+  count_launch(1);
+}
+void s_eta_to_qp(int mx, int my, int mz, const double *v, double *eta, cudaStream_t s)
+{
+  k_eta_to_qp<<<sgrid((size_t)mx * my * mz), 128, 0, s>>>(mx, my, mz, v, eta);
+  count_launch(1);
 }
 
 void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *eta, int geomean, double *Binv,

@@ -33,6 +33,10 @@ void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *
                     cudaStream_t s);
 void s_body_force(int mx, int my, int mz, const double *coords, const double *rho, double g[3], double *bu, cudaStream_t s);
 void s_restrict_eta(int mxc, int myc, int mzc, const double *eta_f, double *eta_c, cudaStream_t s);
+void s_eta_project(int mx, int my, int mz, const double *eta, double *A, double *B, cudaStream_t s);
+void s_divide(size_t n, double *a, const double *b, cudaStream_t s);
+void s_fill(size_t n, double v, double *a, cudaStream_t s);
+void s_eta_to_qp(int mx, int my, int mz, const double *v, double *eta, cudaStream_t s);
 void s_inject_coords(int cnx, int cny, int cnz, const double *cf, double *cc, cudaStream_t s);
 
 // galerkin.cu (27-point block-stencil coarse operators)

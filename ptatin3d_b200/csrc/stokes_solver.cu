@@ -36,6 +36,7 @@ struct Level {
   bool gal = false;              // Galerkin level: 27-point block stencil instead of a matrix-free operator
   double *G64 = nullptr;         // stencil coefficients (FP64, always kept)
   float *G32 = nullptr;          // FP32 copy (mixed mode smoothing)
+  double *vnode = nullptr, *vden = nullptr; // nodal viscosity and its weights (Q1 coefficient hierarchy)
   void *b = nullptr, *x = nullptr, *r = nullptr, *d = nullptr, *t = nullptr; // MG precision work vectors
 };
 
@@ -478,11 +479,13 @@ static void free_level(Level &L)
   p3d_op_destroy(L.op64);
   p3d_op_destroy(L.op32);
   L.op64 = L.op32 = nullptr;
-  for (void *p : {(void *)L.coords, (void *)L.eta, (void *)L.dinv, L.b, L.x, L.r, L.d, L.t, (void *)L.G64, (void *)L.G32})
+  for (void *p : {(void *)L.coords, (void *)L.eta, (void *)L.dinv, L.b, L.x, L.r, L.d, L.t, (void *)L.G64, (void *)L.G32,
+                  (void *)L.vnode, (void *)L.vden})
     if (p) cudaFree(p);
   L.coords = L.eta = L.dinv = nullptr;
   L.G64 = nullptr;
   L.G32 = nullptr;
+  L.vnode = L.vden = nullptr;
   L.b = L.x = L.r = L.d = L.t = nullptr;
 }
 
@@ -510,13 +513,29 @@ static int solver_setup(p3d_solver *s, const double *coords, const double *eta)
     } else {
       if (!L.coords) CK(dev_alloc((void **)&L.coords, 3 * nn * 8, "level coords"));
       if (!L.eta) CK(dev_alloc((void **)&L.eta, 27 * nel * 8, "level eta"));
+      const bool q1 = s->o.coarse_eta == P3D_COARSE_ETA_Q1 && nlev > 1;
+      if (q1 && !L.vnode) {
+        CK(dev_alloc((void **)&L.vnode, nn * 8, "nodal viscosity"));
+        CK(dev_alloc((void **)&L.vden, nn * 8, "nodal weights"));
+      }
       if (l == nlev - 1) {
         CU(cudaMemcpyAsync(L.coords, coords, 3 * nn * 8, cudaMemcpyDeviceToDevice, s->st), "coords");
         CU(cudaMemcpyAsync(L.eta, eta, 27 * nel * 8, cudaMemcpyDeviceToDevice, s->st), "eta");
+        if (q1) s_eta_project(L.m[0], L.m[1], L.m[2], eta, L.vnode, L.vden, s->st);
       } else {
         Level &F = s->lv[l + 1];
         s_inject_coords(L.n[0], L.n[1], L.n[2], F.coords, L.coords, s->st);
-        s_restrict_eta(L.m[0], L.m[1], L.m[2], F.eta, L.eta, s->st);
+        if (q1) {
+          // vc = (P^T vf) ./ (P^T 1), then clamped Q1 interpolation to the Gauss points
+          const size_t nnf = (size_t)F.n[0] * F.n[1] * F.n[2];
+          CK(mg_restrict<double>(L.n[0], L.n[1], L.n[2], 1, F.vnode, L.vnode, s->st));
+          s_fill(nnf, 1.0, F.vden, s->st);
+          CK(mg_restrict<double>(L.n[0], L.n[1], L.n[2], 1, F.vden, L.vden, s->st));
+          s_divide(nn, L.vnode, L.vden, s->st);
+          s_eta_to_qp(L.m[0], L.m[1], L.m[2], L.vnode, L.eta, s->st);
+        } else {
+          s_restrict_eta(L.m[0], L.m[1], L.m[2], F.eta, L.eta, s->st);
+        }
       }
       CU(cudaStreamSynchronize(s->st), "hierarchy");
       p3d_mesh_desc d;
@@ -678,6 +697,7 @@ int p3d_solver_default_opts(p3d_solver_opts *o)
   o->inner_its = 0;
   o->coarse_op = P3D_COARSE_GALERKIN;
   o->schur_eta = P3D_SCHUR_ETA_QP;
+  o->coarse_eta = P3D_COARSE_ETA_GEOMEAN;
   return P3D_OK;
 }
 
@@ -727,7 +747,8 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
   if (o.nlevels < 1 || o.nlevels > 12 || o.restart < 1 || o.restart > P3D_MAX_RESTART || o.max_it < 1 ||
       o.cheb_its < 1 || !(o.cheb_hi > o.cheb_lo) || o.cheb_lo <= 0 || (o.mg_precision != 64 && o.mg_precision != 32) ||
       o.inner_its < 0 || o.inner_its > 1000 || (o.coarse_op != P3D_COARSE_GALERKIN && o.coarse_op != P3D_COARSE_REDISC) ||
-      (o.schur_eta != P3D_SCHUR_ETA_QP && o.schur_eta != P3D_SCHUR_ETA_GEOMEAN))
+      (o.schur_eta != P3D_SCHUR_ETA_QP && o.schur_eta != P3D_SCHUR_ETA_GEOMEAN) ||
+      (o.coarse_eta != P3D_COARSE_ETA_GEOMEAN && o.coarse_eta != P3D_COARSE_ETA_Q1))
     return set_error(P3D_ERR_ARG, "solver_create: bad options");
   int f = 1 << (o.nlevels - 1);
   if (mesh->mx % f || mesh->my % f || mesh->mz % f)

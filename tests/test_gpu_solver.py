@@ -186,6 +186,31 @@ def test_schur_blocks_match_oracle(cuda, restatement, weighting):
     assert rel(zp.cpu().numpy(), ref) <= 1e-12
 
 
+def test_q1_coefficient_hierarchy_levels_match_oracle(cuda, restatement):
+    """Rediscretised coarse levels with the reference's Q1 viscosity hierarchy
+    (nodal projection, scaled restriction, clamped interpolation,
+    src/material_point_utils.c:894-1420): every level operator equals the
+    oracle's MatMult with the oracle's restricted viscosity and injected coordinates."""
+    from ptatin3d_b200 import COARSE_ETA_Q1
+    m, nlev = 8, 3
+    c, eta, _ = sinker(m, contrast=1e3, deform=0.1)
+    S = StokesSolver(m, m, m, BITS, nlevels=nlev, coarse_op=COARSE_REDISC, coarse_eta=COARSE_ETA_Q1)
+    S.setup(c, eta)
+    etas = restatement.eta_hierarchy((m, m, m), eta, nlev)
+    rng = np.random.default_rng(4)
+    cl = c
+    for depth in range(nlev):
+        mm = m >> depth
+        if depth:
+            nf = 2 * (2 * mm) + 1
+            cl = cl.reshape(nf, nf, nf, 3)[::2, ::2, ::2].reshape(-1).copy()  # injection
+        x = rng.uniform(-1, 1, size=3 * (2 * mm + 1) ** 3)
+        y = S.level_apply(nlev - 1 - depth, x).cpu().numpy()
+        mask = M.dirichlet_mask(mm, mm, mm, BITS)
+        ref = matmult_a11(lambda v: restatement.a11_raw((mm, mm, mm), cl, etas[depth], v), x, mask)
+        assert rel(y, ref) <= 1e-12, depth
+
+
 def test_graph_and_eager_preconditioner_agree(cuda):
     m = 8
     c, eta, rho = sinker(m)

@@ -114,3 +114,20 @@ def test_transfer_adjoint(restatement):
     f = restatement.prolong(cn, 1, lin)
     Fi, Fj, Fk = np.meshgrid(np.arange(5) / 2, np.arange(7) / 2, np.arange(3) / 2, indexing="ij")
     assert np.allclose(f, (1 + 2 * Fi + 3 * Fj - Fk).transpose(2, 1, 0).reshape(-1))
+
+
+def test_q1_coefficient_hierarchy_restatement(restatement):
+    """The oracle's Q1 viscosity hierarchy: constants are reproduced exactly,
+    values stay inside the fine range (clamping), and the nodal projection of
+    an element-wise field is its weighted average."""
+    import numpy as np
+    m = 4
+    eta = np.full((m ** 3, 27), 3.5)
+    for e in restatement.eta_hierarchy((m, m, m), eta, 3):
+        assert np.allclose(e, 3.5, rtol=0, atol=1e-14)
+    rng = np.random.default_rng(1)
+    eta = 10.0 ** rng.uniform(-2, 2, size=(m ** 3, 27))
+    levels = restatement.eta_hierarchy((m, m, m), eta, 3)
+    assert [lv.size for lv in levels] == [27 * 64, 27 * 8, 27]
+    for e in levels[1:]:
+        assert e.min() >= eta.min() - 1e-12 and e.max() <= eta.max() + 1e-12
