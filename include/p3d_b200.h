@@ -113,6 +113,19 @@ int p3d_a12_apply(p3d_op *op, const void *p, void *yu, void *stream);  /* yu += 
 int p3d_a21_apply(p3d_op *op, const void *u, void *yp, void *stream);  /* yp += A21 u; Dirichlet columns zeroed with MATMULT */
 int p3d_stokes_apply(p3d_op *op, const void *u, const void *p, void *yu, void *yp, void *stream); /* [A11 A12; A21 0] */
 
+/* Residual of the Stokes equations (FormFunction_Stokes with FormFunctionLocal_U
+ * and FormFunctionLocal_P, src/stokes_form_function.c:99-243, 357-564), FP64
+ * device arrays: the Dirichlet values phi (3*nn, read at Dirichlet dofs only;
+ * NULL = 0) are inserted into u, then
+ *   ru = A11 u + A12 p - f_u,   rp = A21 u - f_p,
+ * with f_u = sum_q w detJ N fu_q (fu: 3 per Gauss point, 81*nel, the Fu of the
+ * reference's QPntVolCoefStokes; NULL = 0) and f_p = sum_q w detJ Np fp_q (fp:
+ * 27*nel, the Fp; NULL = 0); finally the Dirichlet rows are ru_k = u_k - phi_k.
+ * Calls on one operator must not overlap (the operator's boundary mode is
+ * switched for the element pass). */
+int p3d_stokes_residual(p3d_op *op, const double *u, const double *p, const double *phi, const double *fu,
+                        const double *fp, double *ru, double *rp, void *stream);
+
 /* Host-buffer apply with the reference CUDA backend's synchronous contract
  * (src/stokes_operators_cuda.cu:457-532): copies x in, applies into a zeroed
  * device y, copies y out (y = A11 x, overwriting y as the reference backend's

@@ -211,6 +211,28 @@ def body_force(R: Restatement, dims, coords, rho, g=(0.0, 0.0, -1.0)):
     return bu
 
 
+def stokes_residual(R: Restatement, dims, coords, eta, mask, u, p, phi, fu, fp):
+    """FormFunction_Stokes (src/stokes_form_function.c:477-564): insert the
+    Dirichlet values phi into u, r_u = A11 u + A12 p - f_u, r_p = A21 u - f_p,
+    then the Dirichlet rows r_k = u_k - phi_k (BCListResidualDirichlet, scale 1)."""
+    for f in ("o_force_u", "o_force_p"):
+        getattr(R.L, f).argtypes = [C.c_int] * 3 + [_dp] * 3
+    m = mask.astype(bool)
+    ub = np.where(m, phi, u)
+    e = np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)
+    c = np.ascontiguousarray(coords, dtype=np.float64)
+    ru = R.a11_raw(dims, c, e, ub) + R.a12_raw(dims, c, p)
+    bu = np.zeros(c.size)
+    R.L.o_force_u(*dims, _p(c), _p(np.ascontiguousarray(fu, dtype=np.float64).reshape(-1)), _p(bu))
+    ru -= bu
+    rp = R.a21_raw(dims, c, ub)
+    bp = np.zeros(rp.size)
+    R.L.o_force_p(*dims, _p(c), _p(np.ascontiguousarray(fp, dtype=np.float64).reshape(-1)), _p(bp))
+    rp -= bp
+    ru[m] = u[m] - phi[m]
+    return ru, rp
+
+
 def stokes_dense(R: Restatement, dims, coords, eta, mask):
     """Assemble [A11 A12; A21 0] with the MatMult boundary convention by probing
     the oracle operators column by column (small meshes only)."""

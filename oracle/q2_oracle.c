@@ -579,3 +579,48 @@ void o_body_force(int mx, int my, int mz, const double *coords, const double *rh
     }
   }
 }
+
+/* Body-force terms of the Stokes residual from Gauss-point forces
+ * (the Be / Be arrays of FormFunctionLocal_U and FormFunctionLocal_P,
+ * src/stokes_form_function.c:99-243, 357-450):
+ *   bu[3n+l] += sum_q w detJ N_n(q) fu[e][q][l],   bp[4e+k] += sum_q w detJ Np_k(q) fp[e][q]  */
+void o_force_u(int mx, int my, int mz, const double *coords, const double *fu, double *bu)
+{
+  o_mesh m = {mx, my, mz};
+  o_tables();
+  long nel = (long)mx * my * mz;
+  for (long e = 0; e < nel; e++) {
+    long nid[27];
+    double elx[81], iJ[27][3][3], detJ[27];
+    o_element_nodes(&m, e, nid);
+    o_gather3(coords, nid, elx);
+    o_geometry(elx, iJ, detJ);
+    for (int q = 0; q < 27; q++) {
+      int qi = q % 3, qj = (q / 3) % 3, qk = q / 9;
+      double s = WQ[q] * detJ[q];
+      for (int n = 0; n < 27; n++) {
+        double N = BAS[qi][n % 3] * BAS[qj][(n / 3) % 3] * BAS[qk][n / 9];
+        for (int l = 0; l < 3; l++) bu[3 * nid[n] + l] += s * N * fu[81 * e + 3 * q + l];
+      }
+    }
+  }
+}
+
+void o_force_p(int mx, int my, int mz, const double *coords, const double *fp, double *bp)
+{
+  o_mesh m = {mx, my, mz};
+  o_tables();
+  long nel = (long)mx * my * mz;
+  for (long e = 0; e < nel; e++) {
+    long nid[27];
+    double elx[81], iJ[27][3][3], detJ[27];
+    o_element_nodes(&m, e, nid);
+    o_gather3(coords, nid, elx);
+    o_geometry(elx, iJ, detJ);
+    for (int q = 0; q < 27; q++) {
+      double Np[4];
+      o_pressure_basis(elx, q, Np);
+      for (int k = 0; k < 4; k++) bp[4 * e + k] += WQ[q] * detJ[q] * Np[k] * fp[27 * e + q];
+    }
+  }
+}

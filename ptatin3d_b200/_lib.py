@@ -106,6 +106,7 @@ _SIGS = {
     "p3d_op_sizes": ([C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     "p3d_a11_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_op_set_host_chunks": ([C.c_void_p, C.c_int], C.c_int),
+    "p3d_stokes_residual": ([C.c_void_p] * 9, C.c_int),
     "p3d_a11_mult": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_a11_diagonal": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_a12_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),

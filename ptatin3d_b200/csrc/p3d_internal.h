@@ -29,6 +29,7 @@ struct p3d_op {
   cudaStream_t s_h2d = nullptr, s_d2h = nullptr; // host-apply copy streams
   cudaEvent_t ev[32] = {};                      // host-apply chunk events (16 chunks x {x in, y done})
   int host_chunks = 0;                           // 0: automatic
+  void *res_u = nullptr;                         // residual: u with the Dirichlet values inserted
   cudaStream_t stream = nullptr;     // setup / host-apply stream
 };
 

@@ -12,6 +12,7 @@
 
 #include "p3d_b200.h"
 #include "p3d_internal.h"
+#include "solver_internal.h"
 #include "stokes_kernels.cuh"
 
 namespace p3d {
@@ -263,6 +264,27 @@ int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geo
   return cuda_check(cudaStreamSynchronize(st), "setup sync");
 }
 
+// Dirichlet values on the lattice of an operator.  mode 0: out = u with the
+// Dirichlet dofs replaced by phi (0 without phi) (BCListInsertLocal,
+// src/dmda_bcs.c:409-); mode 1: out_k = u_k - phi_k on the Dirichlet dofs only
+// (BCListResidualDirichlet with scale 1).
+__global__ void dirichlet_values_kernel(int gx, int gy, int gz, int ox, int oy, int oz, int ex, int ey, int ez, uint32_t dir,
+                                        const double *__restrict__ u, const double *__restrict__ phi, double *__restrict__ out,
+                                        int mode)
+{
+  const size_t nn = (size_t)gx * gy * gz;
+  for (size_t node = blockIdx.x * (size_t)blockDim.x + threadIdx.x; node < nn; node += (size_t)gridDim.x * blockDim.x) {
+    const int i = node % gx, j = (node / gx) % gy, k = node / ((size_t)gx * gy);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const size_t idx = 3 * node + c;
+      const bool d = is_dirichlet(dir, i, j, k, ox, oy, oz, ex, ey, ez, c);
+      if (mode == 0) out[idx] = d ? (phi ? phi[idx] : 0.0) : u[idx];
+      else if (d) out[idx] = u[idx] - (phi ? phi[idx] : 0.0);
+    }
+  }
+}
+
 } // namespace p3d
 
 using namespace p3d;
@@ -325,6 +347,7 @@ int p3d_op_destroy(p3d_op *op)
   free_dev(op->hx);
   free_dev(op->hy);
   if (op->flag) cudaFree(op->flag);
+  free_dev(op->res_u);
   for (auto &e : op->ev)
     if (e) cudaEventDestroy(e);
   if (op->s_h2d) cudaStreamDestroy(op->s_h2d);
@@ -395,6 +418,37 @@ int p3d_a11_apply(p3d_op *op, const void *x, void *y, void *stream)
   cudaStream_t st = (cudaStream_t)stream;
   if (op->prec == P3D_PREC_F64) return launch_a11<double>(op, (const double *)x, (double *)y, st);
   return launch_a11<float>(op, (const float *)x, (float *)y, st);
+}
+
+int p3d_stokes_residual(p3d_op *op, const double *u, const double *p, const double *phi, const double *fu,
+                        const double *fp, double *ru, double *rp, void *stream)
+{
+  P3D_REQUIRE_SETUP(op);
+  if (!u || !p || !ru || !rp) return set_error(P3D_ERR_ARG, "stokes_residual: null vector");
+  if (op->prec != P3D_PREC_F64) return set_error(P3D_ERR_ARG, "stokes_residual: FP64 operators only");
+  cudaStream_t st = (cudaStream_t)stream;
+  const p3d_mesh_desc &m = op->m;
+  const size_t nn = (size_t)m.gx * m.gy * m.gz, nel = (size_t)m.mx * m.my * m.mz;
+  int rc;
+  if (!op->res_u && (rc = dev_alloc(&op->res_u, 3 * nn * 8, "residual u"))) return rc;
+  const TileArgs<double> a = tile_args<double>(op, NW_GEN);
+  const int ex = m.ox + 2 * m.mx, ey = m.oy + 2 * m.my, ez = m.oz + 2 * m.mz;
+  double *ub = (double *)op->res_u;
+  dirichlet_values_kernel<<<grid_for(nn), 256, 0, st>>>(m.gx, m.gy, m.gz, m.ox, m.oy, m.oz, ex, ey, ez, a.dir, u, phi, ub, 0);
+  count_launch(1);
+  if ((rc = cuda_check(cudaMemsetAsync(ru, 0, 3 * nn * 8, st), "memset"))) return rc;
+  if ((rc = cuda_check(cudaMemsetAsync(rp, 0, 4 * nel * 8, st), "memset"))) return rc;
+  // element terms on u with the Dirichlet values in place: no column zeroing, no row handling
+  const int bc = op->bc;
+  op->bc = P3D_BC_NONE;
+  rc = launch_general<double, true, true, true>(op, ub, p, ru, rp, st, true);
+  op->bc = bc;
+  if (rc) return rc;
+  if (fu) s_force_u(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz, (const double *)op->coords, fu, ru, st);
+  if (fp) s_force_p(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz, (const double *)op->coords, fp, rp, st);
+  dirichlet_values_kernel<<<grid_for(nn), 256, 0, st>>>(m.gx, m.gy, m.gz, m.ox, m.oy, m.oz, ex, ey, ez, a.dir, u, phi, ru, 1);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "stokes residual");
 }
 
 int p3d_a11_mult(p3d_op *op, const void *x, void *y, void *stream)

@@ -298,6 +298,79 @@ void s_eta_to_qp(int mx, int my, int mz, const double *v, double *eta, cudaStrea
   count_launch(1);
 }
 
+// ---- residual body-force terms on a (possibly ghosted) local lattice
+__device__ void gather_element_g(int gx, int gy, int ox, int oy, int oz, int ex, int ey, int ez, const double *coords,
+                                 double X[27][3])
+{
+  for (int n = 0; n < 27; n++) {
+    size_t g = (size_t)(ox + 2 * ex + n % 3) + (size_t)gx * ((size_t)(oy + 2 * ey + (n / 3) % 3) + (size_t)gy * (oz + 2 * ez + n / 9));
+    for (int l = 0; l < 3; l++) X[n][l] = coords[3 * g + l];
+  }
+}
+// ru[3n+l] -= sum_q w detJ N_n(q) fu[e][q][l]
+__global__ void k_force_u(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, const double *__restrict__ coords,
+                          const double *__restrict__ fu, double *__restrict__ ru)
+{
+  size_t nel = (size_t)mx * my * mz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nel; e += (size_t)gridDim.x * blockDim.x) {
+    const int ex = e % mx, ey = (e / mx) % my, ez = e / ((size_t)mx * my);
+    double X[27][3];
+    gather_element_g(gx, gy, ox, oy, oz, ex, ey, ez, coords, X);
+    double acc[27][3] = {};
+    for (int q = 0; q < 27; q++) {
+      QPGeom g = qp_geom(X, q);
+      const int qi = q % 3, qj = (q / 3) % 3, qk = q / 9;
+      const double s = g.w * g.detJ;
+      const double f0 = fu[81 * e + 3 * q], f1 = fu[81 * e + 3 * q + 1], f2 = fu[81 * e + 3 * q + 2];
+      for (int n = 0; n < 27; n++) {
+        const double N = s * bq(qi, n % 3) * bq(qj, (n / 3) % 3) * bq(qk, n / 9);
+        acc[n][0] += N * f0; acc[n][1] += N * f1; acc[n][2] += N * f2;
+      }
+    }
+    for (int n = 0; n < 27; n++) {
+      size_t node = (size_t)(ox + 2 * ex + n % 3) + (size_t)gx * ((size_t)(oy + 2 * ey + (n / 3) % 3) + (size_t)gy * (oz + 2 * ez + n / 9));
+      for (int l = 0; l < 3; l++) atomicAdd(ru + 3 * node + l, -acc[n][l]);
+    }
+  }
+}
+// rp[4e+k] -= sum_q w detJ Np_k(q) fp[e][q]  (Np = [1, xh, yh, zh], the global-relative P1 basis)
+__global__ void k_force_p(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, const double *__restrict__ coords,
+                          const double *__restrict__ fp, double *__restrict__ rp)
+{
+  size_t nel = (size_t)mx * my * mz;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nel; e += (size_t)gridDim.x * blockDim.x) {
+    const int ex = e % mx, ey = (e / mx) % my, ez = e / ((size_t)mx * my);
+    double X[27][3];
+    gather_element_g(gx, gy, ox, oy, oz, ex, ey, ez, coords, X);
+    double avg[3] = {0, 0, 0};
+    for (int n = 0; n < 27; n++)
+      for (int l = 0; l < 3; l++) avg[l] += X[n][l];
+    for (int l = 0; l < 3; l++) avg[l] /= 27.0;
+    const double L[3] = {X[14][0] - X[12][0], X[16][1] - X[10][1], X[22][2] - X[4][2]};
+    double acc[4] = {0, 0, 0, 0};
+    for (int q = 0; q < 27; q++) {
+      QPGeom g = qp_geom(X, q);
+      const double s = g.w * g.detJ * fp[27 * e + q];
+      acc[0] += s;
+      for (int l = 0; l < 3; l++) acc[1 + l] += s * (g.xq[l] - avg[l]) / L[l];
+    }
+    for (int k = 0; k < 4; k++) rp[4 * e + k] -= acc[k];
+  }
+}
+
+void s_force_u(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, const double *coords, const double *fu,
+               double *ru, cudaStream_t s)
+{
+  k_force_u<<<sgrid((size_t)mx * my * mz), 128, 0, s>>>(mx, my, mz, gx, gy, ox, oy, oz, coords, fu, ru);
+  count_launch(1);
+}
+void s_force_p(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, const double *coords, const double *fp,
+               double *rp, cudaStream_t s)
+{
+  k_force_p<<<sgrid((size_t)mx * my * mz), 128, 0, s>>>(mx, my, mz, gx, gy, ox, oy, oz, coords, fp, rp);
+  count_launch(1);
+}
+
 void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *eta, int geomean, double *Binv,
                     cudaStream_t s)
 {

@@ -36,6 +36,10 @@ void s_restrict_eta(int mxc, int myc, int mzc, const double *eta_f, double *eta_
 void s_eta_project(int mx, int my, int mz, const double *eta, double *A, double *B, cudaStream_t s);
 void s_divide(size_t n, double *a, const double *b, cudaStream_t s);
 void s_fill(size_t n, double v, double *a, cudaStream_t s);
+void s_force_u(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, const double *coords, const double *fu,
+               double *ru, cudaStream_t s);
+void s_force_p(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, const double *coords, const double *fp,
+               double *rp, cudaStream_t s);
 void s_eta_to_qp(int mx, int my, int mz, const double *v, double *eta, cudaStream_t s);
 void s_inject_coords(int cnx, int cny, int cnz, const double *cf, double *cc, cudaStream_t s);
 

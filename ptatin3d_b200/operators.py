@@ -164,6 +164,25 @@ class MatStokesMF(MatA11MF):
                                      _stream()))
 
 
+    def residual(self, u, p, fu=None, fp=None, phi=None):
+        """FormFunction_Stokes: (ru, rp) = ([A11 u + A12 p - f_u; A21 u - f_p] with the
+        Dirichlet values phi inserted in u, Dirichlet rows u_k - phi_k).  fu: (nel, 27, 3)
+        Gauss-point force, fp: (nel, 27), phi: Dirichlet values -- CUDA tensors or arrays."""
+        def dev(a):
+            if a is None:
+                return None
+            if isinstance(a, torch.Tensor):
+                return a.to(device=self.device, dtype=torch.float64).contiguous().reshape(-1)
+            return torch.tensor(np.ascontiguousarray(a, dtype=np.float64).reshape(-1), device=self.device)
+        u_d, p_d, fu_d, fp_d, phi_d = dev(u), dev(p), dev(fu), dev(fp), dev(phi)
+        ru = torch.empty(self.n_velocity, dtype=torch.float64, device=self.device)
+        rp = torch.empty(self.n_pressure, dtype=torch.float64, device=self.device)
+        ptr = lambda t: None if t is None else _ptr(t)
+        check(lib().p3d_stokes_residual(self.h, self._vec(u_d, self.n_velocity, "u"), self._vec(p_d, self.n_pressure, "p"),
+                                        ptr(phi_d), ptr(fu_d), ptr(fp_d), _ptr(ru), _ptr(rp), _stream()))
+        return ru, rp
+
+
 def mg_prolong(xc: torch.Tensor, xf: torch.Tensor, cn, ndof=3):
     prec = PREC_F64 if xc.dtype == torch.float64 else PREC_F32
     check(lib().p3d_mg_prolong(prec, cn[0], cn[1], cn[2], ndof, _ptr(xc), _ptr(xf), _stream()))
