@@ -78,7 +78,12 @@ typedef struct p3d_op p3d_op; /* opaque: one mesh + coefficients resident in HBM
 
 #define P3D_GEOM_AUTO 0    /* affine fast path when every element is a parallelepiped */
 #define P3D_GEOM_GENERAL 1 /* per-quadrature-point Jacobian from the coordinates      */
-#define P3D_GEOM_AFFINE 2  /* force the per-element Jacobian (caller asserts affinity) */
+#define P3D_GEOM_AFFINE 2  /* the Jacobian of the element centre at every Gauss point:
+                              exact for parallelepipeds; on any other mesh it is the
+                              reference's low-order operator MatMult_MFStokes_A11LowOrder
+                              (ONEPOINTQ, src/stokes_operators.c:1207-1278,
+                              src/stokes_operators_mf.c:353-488)                     */
+#define P3D_GEOM_LOWORDER P3D_GEOM_AFFINE
 
 #define P3D_BC_NONE 0      /* raw element apply: y += sum_e A_e x  (SpMVOp contract)   */
 #define P3D_BC_MATMULT 1   /* MatMult contract: Dirichlet columns zeroed, rows y_k = x_k */

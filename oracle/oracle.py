@@ -124,7 +124,7 @@ class Restatement:
 class Reference:
     """The reference's own kernels; one mesh at a time (module-global state in the driver)."""
 
-    VARIANTS = {"tensor": 0, "avx": 1, "ref": 2}
+    VARIANTS = {"tensor": 0, "avx": 1, "ref": 2, "loworder": 3}
 
     def __init__(self):
         if not os.path.exists(REF_LIB):

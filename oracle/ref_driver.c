@@ -7,7 +7,7 @@
  * mesh, and exports plain-C entry points:
  *
  *   ref_setup(mx,my,mz, coords[3*nn], eta[27*nel])
- *   ref_a11(variant, x[3*nn], y[3*nn])   variant 0=tensor 1=avx 2=ref
+ *   ref_a11(variant, x[3*nn], y[3*nn])   variant 0=tensor 1=avx 2=ref 3=low-order (MFStokesWrapper_A11PC)
  *   ref_diag(y[3*nn]), ref_a12(p[4*nel], yu[3*nn]), ref_a21(u[3*nn], yp[4*nel])
  *
  * Each adds element contributions exactly as the reference's SpMVOp_MatMult
@@ -30,6 +30,7 @@
 PetscErrorCode MFStokesWrapper_A11_Tensor(MatA11MF, Quadrature, DM, PetscScalar[], PetscScalar[]);
 PetscErrorCode MFStokesWrapper_A11_AVX(MatA11MF, Quadrature, DM, PetscScalar[], PetscScalar[]);
 PetscErrorCode MFStokesWrapper_A11(MatA11MF, Quadrature, DM, PetscScalar[], PetscScalar[]);
+PetscErrorCode MFStokesWrapper_A11PC(Quadrature, DM, PetscScalar[], PetscScalar[]);
 PetscErrorCode MFStokesWrapper_diagA11(Quadrature, DM, PetscScalar[]);
 PetscErrorCode MFStokesWrapper_A12(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
 PetscErrorCode MFStokesWrapper_A21(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
@@ -231,6 +232,7 @@ int ref_a11(int variant, double *x, double *y)
   case 0: return MFStokesWrapper_A11_Tensor(NULL, &g_Q, &g_dau, x, y);
   case 1: return MFStokesWrapper_A11_AVX(NULL, &g_Q, &g_dau, x, y);
   case 2: return MFStokesWrapper_A11(NULL, &g_Q, &g_dau, x, y);
+  case 3: return MFStokesWrapper_A11PC(&g_Q, &g_dau, x, y);
   default: return PETSC_ERR_SUP;
   }
 }

@@ -142,6 +142,31 @@ def test_diagonal_a12_a21_fused(cuda, restatement, deform):
     assert rel(host(fp), host(yp)) <= TOL64
 
 
+def test_low_order_operator_matches_reference_golden(cuda):
+    """MatMult_MFStokes_A11LowOrder (ONEPOINTQ: the Jacobian of the element centre
+    at every Gauss point, src/stokes_operators_mf.c:353-488): the affine path
+    forced on a deformed mesh, against the reference's own kernel output."""
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "loworder_4x3x5.npz"))
+    dims = tuple(int(v) for v in g["dims"])
+    case = dict(dims=dims, coords=g["coords"], eta=g["eta"], bits=M.FREE_SLIP)
+    op = make_op(case, geom=GEOM_AFFINE)
+    y = torch.zeros(g["x"].size, dtype=torch.float64, device="cuda")
+    op.spmv(T(g["x"]), y)
+    assert rel(host(y), g["y"]) <= TOL64
+
+
+def test_low_order_operator_matches_reference_kernel(cuda, reference_kernels):
+    m = 6
+    c = M.perturb_interior(M.uniform_coords(m, m, m), m, m, m, frac=0.2, seed=1)
+    eta = 10 ** np.random.default_rng(2).uniform(-1, 1, size=(m ** 3, 27))
+    reference_kernels.setup((m, m, m), c, eta)
+    x = np.random.default_rng(3).uniform(-1, 1, size=c.size)
+    op = make_op(dict(dims=(m, m, m), coords=c, eta=eta, bits=M.FREE_SLIP), geom=GEOM_AFFINE)
+    y = torch.zeros(x.size, dtype=torch.float64, device="cuda")
+    op.spmv(T(x), y)
+    assert rel(host(y), reference_kernels.a11_raw(x, "loworder")) <= TOL64
+
+
 @pytest.mark.parametrize("deform,with_forces", [(0.15, True), (0.0, True), (0.15, False)])
 def test_stokes_residual_matches_oracle(cuda, restatement, deform, with_forces):
     """FormFunction_Stokes (src/stokes_form_function.c:99-564) on the GPU against

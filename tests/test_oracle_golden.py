@@ -131,3 +131,13 @@ def test_q1_coefficient_hierarchy_restatement(restatement):
     assert [lv.size for lv in levels] == [27 * 64, 27 * 8, 27]
     for e in levels[1:]:
         assert e.min() >= eta.min() - 1e-12 and e.max() <= eta.max() + 1e-12
+
+
+def test_loworder_golden_is_the_reference_kernel(reference_kernels):
+    """The committed low-order golden vectors are reproduced by the reference's compiled kernel."""
+    import os
+    import numpy as np
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "loworder_4x3x5.npz"))
+    reference_kernels.setup(tuple(int(v) for v in g["dims"]), g["coords"], g["eta"])
+    y = reference_kernels.a11_raw(g["x"], "loworder")
+    assert np.linalg.norm(y - g["y"]) <= 1e-14 * np.linalg.norm(g["y"])
