@@ -51,6 +51,10 @@ void g_dirichlet(int nx, int ny, int nz, uint32_t dir, double *G, cudaStream_t s
 void g_diag(int nx, int ny, int nz, const double *G, double *d, cudaStream_t s);
 void g_dense(int nx, int ny, int nz, const double *G, double *M, cudaStream_t s);
 
+// dense_inverse.cu (coarse-grid operator, in place, blocked Gauss-Jordan)
+size_t dense_inverse_scratch(int n);
+int dense_inverse_spd(int n, double *A, double *scratch, cudaStream_t s);
+
 // mg_transfer.cu
 template <typename T> int mg_prolong(int cnx, int cny, int cnz, int ndof, const T *xc, T *xf, cudaStream_t st);
 template <typename T> int mg_restrict(int cnx, int cny, int cnz, int ndof, const T *xf, T *xc, cudaStream_t st);

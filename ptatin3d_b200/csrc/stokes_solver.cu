@@ -52,7 +52,7 @@ struct p3d_solver {
   int nc = 0;
   double *cinv = nullptr;          // dense inverse of the Galerkin coarse operator
   double *cb64 = nullptr, *cx64 = nullptr;
-  double *gj = nullptr;            // Gauss-Jordan pivot row and column
+  double *gj = nullptr;            // scratch of the blocked Gauss-Jordan inverse
   // Stokes system
   size_t nu = 0, np = 0, N = 0;
   double *Binv = nullptr; // Schur block inverses
@@ -348,29 +348,6 @@ static int estimate_lmax(p3d_solver *s, Level &L)
   return P3D_OK;
 }
 
-// in-place Gauss-Jordan inversion of a dense SPD matrix (no pivoting), one step per pivot
-__global__ void k_gj_step(int n, int k, double *__restrict__ A, double *__restrict__ colk, double *__restrict__ rowk)
-{
-  // phase handled by the host loop: colk/rowk hold column and row k before the update
-  size_t total = (size_t)n * n;
-  double piv = rowk[k];
-  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
-    int i = idx / n, j = idx % n;
-    double v;
-    if (i == k) v = (j == k) ? 1.0 / piv : rowk[j] / piv;
-    else if (j == k) v = -colk[i] / piv;
-    else v = A[idx] - colk[i] * rowk[j] / piv;
-    A[idx] = v;
-  }
-}
-__global__ void k_gj_save(int n, int k, const double *__restrict__ A, double *__restrict__ colk, double *__restrict__ rowk)
-{
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    colk[i] = A[(size_t)i * n + k];
-    rowk[i] = A[(size_t)k * n + i];
-  }
-}
-
 // Galerkin coarse operator Ac = P~^T A1 P~ (+ identity on coarse Dirichlet rows), inverted in place
 static int build_coarse(p3d_solver *s)
 {
@@ -382,7 +359,7 @@ static int build_coarse(p3d_solver *s)
   if (!s->cinv) CK(dev_alloc((void **)&s->cinv, (size_t)nc * nc * 8, "coarse operator"));
   if (!s->cb64) CK(dev_alloc((void **)&s->cb64, (size_t)nc * 8, "coarse vec"));
   if (!s->cx64) CK(dev_alloc((void **)&s->cx64, (size_t)nc * 8, "coarse vec"));
-  if (!s->gj) CK(dev_alloc((void **)&s->gj, 2 * (size_t)nc * 8, "gauss-jordan"));
+  if (!s->gj) CK(dev_alloc((void **)&s->gj, dense_inverse_scratch(nc) * 8, "gauss-jordan"));
   // coarse Dirichlet mask on the host
   std::vector<char> isdir(nc, 0);
   {
@@ -436,13 +413,7 @@ static int build_coarse(p3d_solver *s)
     }
   }
   // Ac is symmetric: columns stored as rows is the same matrix.  Invert in place.
-  double *colk = s->gj, *rowk = s->gj + nc;
-  int g = (int)std::min<size_t>(((size_t)nc * nc + 255) / 256, 148 * 16);
-  for (int k = 0; k < nc; k++) {
-    k_gj_save<<<(nc + 255) / 256, 256, 0, s->st>>>(nc, k, s->cinv, colk, rowk);
-    k_gj_step<<<g, 256, 0, s->st>>>(nc, k, s->cinv, colk, rowk);
-  }
-  count_launch(2 * nc);
+  CK(dense_inverse_spd(nc, s->cinv, s->gj, s->st));
   return cuda_check(cudaStreamSynchronize(s->st), "coarse inverse");
 }
 
@@ -727,7 +698,7 @@ int p3d_solver_estimate_bytes(const p3d_mesh_desc *mesh, const p3d_solver_opts *
       const double op = 3 * nn + 1.2 * 27 * nel + 1.2 * 36 * nel; // operator: coords, packed eta, affine data
       total += 8.0 * op + (mixed && l > 0 ? 4.0 * op : 0.0);
     }
-    if (l == 0) total += 8.0 * (nv * nv + 4 * nv); // dense coarse inverse
+    if (l == 0) total += 8.0 * (nv * nv + 68 * nv + 1024); // dense coarse inverse and its scratch
     if (l == o.nlevels - 1) total += 8.0 * 16.0 * nel; // Schur blocks
   }
   *bytes = (int64_t)(1.1 * total) + (4 << 20);
