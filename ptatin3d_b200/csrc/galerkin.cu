@@ -11,8 +11,8 @@
 //   G[((o*3 + r)*3 + c) * nn + i]   o = (dk+1)*9 + (dj+1)*3 + (di+1)   neighbour
 //                                   r, c = row / column velocity component
 //
-// stored entry-major so that one thread per node reads its 243 coefficients
-// coalesced across the warp.  The reference forms the same operators with
+// stored entry-major so that the threads of a warp read consecutive nodes'
+// coefficients (coalesced).  The reference forms the same operators with
 // PETSc's MatPtAP on assembled matrices (OP_TYPE_GALERKIN,
 // src/ptatin_driver_linear_ts.c:712-762); here they are formed matrix-free
 // by probing: nodes coloured by (I mod 3, J mod 3, K mod 3) have at most one
@@ -35,30 +35,30 @@ static int ggrid(size_t n)
 
 #define G_LOOP(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
 
-// y = G x (overwrites y); accumulation in T
+// y = G x (overwrites y); accumulation in T.  One thread per (row component r,
+// node): threads of a warp share r and read 32 consecutive nodes' coefficients
+// (coalesced); the x values of a neighbourhood are shared through L1 by the
+// three row threads of a node.
 template <typename T>
 __global__ void __launch_bounds__(256) k_stencil_apply(int nx, int ny, int nz, const T *__restrict__ G, const T *__restrict__ x,
                                                        T *__restrict__ y)
 {
   const size_t nn = (size_t)nx * ny * nz;
-  G_LOOP(i, nn)
+  G_LOOP(t, 3 * nn)
   {
+    const int r = (int)(t / nn);
+    const size_t i = t - (size_t)r * nn;
     const int I = i % nx, J = (i / nx) % ny, K = i / ((size_t)nx * ny);
-    T a0 = 0, a1 = 0, a2 = 0;
+    T a = 0;
 #pragma unroll
     for (int o = 0; o < 27; o++) {
       const int di = o % 3 - 1, dj = (o / 3) % 3 - 1, dk = o / 9 - 1;
       if (I + di < 0 || I + di >= nx || J + dj < 0 || J + dj >= ny || K + dk < 0 || K + dk >= nz) continue;
       const long long j = (long long)i + di + (long long)nx * (dj + (long long)ny * dk);
-      const T x0 = x[3 * j], x1 = x[3 * j + 1], x2 = x[3 * j + 2];
-      const T *g = G + (size_t)o * 9 * nn + i;
-      a0 += g[0 * nn] * x0 + g[1 * nn] * x1 + g[2 * nn] * x2;
-      a1 += g[3 * nn] * x0 + g[4 * nn] * x1 + g[5 * nn] * x2;
-      a2 += g[6 * nn] * x0 + g[7 * nn] * x1 + g[8 * nn] * x2;
+      const T *g = G + ((size_t)o * 9 + 3 * r) * nn + i;
+      a += g[0] * x[3 * j] + g[nn] * x[3 * j + 1] + g[2 * nn] * x[3 * j + 2];
     }
-    y[3 * i] = a0;
-    y[3 * i + 1] = a1;
-    y[3 * i + 2] = a2;
+    y[3 * i + r] = a;
   }
 }
 
@@ -137,7 +137,7 @@ __global__ void k_stencil_dense(int nx, int ny, int nz, const double *__restrict
 
 template <typename T> void g_apply(int nx, int ny, int nz, const T *G, const T *x, T *y, cudaStream_t s)
 {
-  k_stencil_apply<T><<<ggrid((size_t)nx * ny * nz), 256, 0, s>>>(nx, ny, nz, G, x, y);
+  k_stencil_apply<T><<<ggrid(3 * (size_t)nx * ny * nz), 256, 0, s>>>(nx, ny, nz, G, x, y);
   count_launch(1);
 }
 void g_probe_vec(int nx, int ny, int nz, int ci, int cj, int ck, int d, uint32_t dir, double *x, cudaStream_t s)
