@@ -23,6 +23,7 @@ struct p3d_op {
   bool have_coef = false;
   void *coords = nullptr; // [3*gx*gy*gz] in operator precision
   void *kgen = nullptr;   // general path: eta, brick order (NW_GEN)
+  void *kgq = nullptr;    // general FP64 path: Gauss-point coordinate table, brick order (NW_GEN)
   void *kaff = nullptr;   // affine path: J^{-1} + eta*w*detJ, brick order (NW_AFF)
   void *hx = nullptr, *hy = nullptr; // host-apply staging
   unsigned long long *flag = nullptr; // affinity test result (kept: re-setup allocates nothing)

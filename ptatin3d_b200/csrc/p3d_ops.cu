@@ -127,6 +127,7 @@ int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_
 {
   TileArgs<T> a = tile_args<T>(op, NW_GEN);
   a.x = u; a.y = yu; a.p = p; a.yp = yp; a.kdat = reinterpret_cast<const T *>(op->kgen);
+  a.kgq = reinterpret_cast<const T *>(op->kgq);
   a.overwrite = overwrite ? 1 : 0;
   // FP64: Jacobian columns exchanged by warp shuffles; FP32: per-element geometry table
   auto kern = sizeof(T) == 8 ? stokes_general_kernel<T, NW_GEN, DA11, DA12, DA21>
@@ -232,6 +233,14 @@ int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geo
     pack_eta_kernel<float, NW_GEN><<<grid_for(ng), 256, 0, st>>>(m.mx, m.my, m.mz, ntx, nty, ntz, eta, (float *)op->kgen);
   count_launch(1);
   if ((rc = cuda_check(cudaGetLastError(), "pack eta"))) return rc;
+  if (op->prec == P3D_PREC_F64) {
+    const size_t ngq = (size_t)ntx * nty * ntz * Brick<NW_GEN>::NE;
+    if (!op->kgq && (rc = dev_alloc(&op->kgq, ngq * GQC * 8, "gauss-point coordinates"))) return rc;
+    pack_gauss_coords_kernel<double, NW_GEN><<<grid_for(ngq), 128, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz, ntx,
+                                                                           nty, ntz, coords, (double *)op->kgq);
+    count_launch(1);
+    if ((rc = cuda_check(cudaGetLastError(), "pack gauss coords"))) return rc;
+  }
   // affinity
   int mode = geom_mode;
   if (mode == P3D_GEOM_AUTO) {
@@ -343,6 +352,7 @@ int p3d_op_destroy(p3d_op *op)
   cudaSetDevice(op->device);
   free_dev(op->coords);
   free_dev(op->kgen);
+  free_dev(op->kgq);
   free_dev(op->kaff);
   free_dev(op->hx);
   free_dev(op->hy);

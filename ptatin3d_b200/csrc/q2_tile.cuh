@@ -124,6 +124,7 @@ template <typename T> struct TileArgs {
   T *__restrict__ y;       // velocity out (+=)
   const T *__restrict__ coords;
   const T *__restrict__ kdat; // brick-ordered coefficients
+  const T *__restrict__ kgq;  // brick-ordered Gauss-point coordinates (general FP64 path)
   const T *__restrict__ p;    // pressure in  (A12)
   T *__restrict__ yp;         // pressure out (A21)
   int diag;                   // diagonal kernel: 1 -> Dirichlet slots = 1

@@ -216,6 +216,13 @@ __global__ void __launch_bounds__(32 * NW, 4) a11_affine_kernel(TileArgs<T> A)
   write_tile<T, NW>(A, b, s_acc, s_y, 0);
 }
 
+// Gauss-point coordinate table of one element (general FP64 path), packed at
+// setup in brick order: the 27 Gauss-point values of each coordinate f
+// ([f][27], the tensor interpolation of the element's nodes), the centroid of
+// the 27 nodes (3 values) and the reciprocal mid-face extents 1/L (3 values)
+// of the pressure basis, one pad value (16-byte multiple).
+constexpr int GQC = 88;
+
 // ------------------------------------------------------- general geometry
 // The Jacobian is recomputed at every Gauss point.  Lane f owns column f of
 // M = [dx_l/dxi_d] (d = row); at each point it fetches the element's other two
@@ -224,9 +231,10 @@ __global__ void __launch_bounds__(32 * NW, 4) a11_affine_kernel(TileArgs<T> A)
 // rotated so that row 0 belongs to direction f (the rotation makes the strain
 // exchange a uniform pair of shuffles).  The 1/det factors of the gradient
 // and of the pulled-back stress combine into one scale eta*w/det per point,
-// so the action runs on the unscaled adjugate.  Gauss-point coordinates are
-// interpolated once per element into shared memory and read one point plane
-// (9 points) at a time.  The register cap (6 CTAs of 64 threads per SM, 168
+// so the action runs on the unscaled adjugate.  The element's Gauss-point
+// coordinates come from the setup-time table (one contiguous 16-byte copy per
+// brick instead of node rows and an interpolation per apply) and are read one
+// point plane (9 points) at a time.  The register cap (6 CTAs of 64 threads per SM, 168
 // registers) trades a few hundred bytes of spills for 50 % more resident warps,
 // which this latency-bound kernel converts into speed (measured at 96^3:
 // 1.65 ms uncapped, 1.45 ms capped; 128 registers: 1.52 ms).
@@ -234,8 +242,7 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSme
   using BK = Brick<NW>;
   static constexpr bool NEEDX = DA11 || DA21;
   static constexpr bool NEEDY = DA11 || DA12;
-  static constexpr int CT = align16(3 * BK::NN, sizeof(T));  // coordinate tile / accumulator
-  static constexpr int CQ = align16(BK::NE * 81, sizeof(T)); // Gauss-point coordinates
+  static constexpr int CQ = align16(BK::NE * GQC, sizeof(T)); // Gauss-point coordinate table
   static constexpr int OX = 0;
   static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
   static constexpr int OC = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
@@ -256,44 +263,19 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
   T *sm = reinterpret_cast<T *>(p3d_smem);
   T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_c = sm + SM::OC, *s_k = sm + SM::OK;
   const BrickPos b = brick_pos<T, NW>(A);
+  const size_t brick = (size_t)blockIdx.x + A.brick0;
   if (SM::NEEDX) stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
-  stage_nodes<T, NW>(A, b, A.coords, s_c, false);
-  stage_block(A.kdat + (size_t)(blockIdx.x + A.brick0) * BK::NE * 27, s_k, BK::NE * 27);
+  stage_block(A.kgq + brick * BK::NE * GQC, s_c, BK::NE * GQC); // Gauss-point coordinates, centroid, 1/L
+  stage_block(A.kdat + brick * BK::NE * 27, s_k, BK::NE * 27);
   if (NEEDY && !A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
   cp_async_wait_all();
   __syncthreads();
 
   const LaneMap L = lane_map();
   const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
-  // coordinates at the Gauss points (lane f: coordinate f) and the pressure-basis scaling
-  T avg = (T)0, rL = (T)1;
-  {
-    T xq[27];
-#pragma unroll
-    for (int n = 0; n < 27; n++) xq[n] = s_c[3 * brick_node<NW>(L.a, L.b, L.c, n) + L.f];
-    if (!valid) { // a unit cube stands in for a slot outside the mesh (its result is never written)
-#pragma unroll
-      for (int n = 0; n < 27; n++) {
-        const int a3 = (L.f == 0) ? n % 3 : ((L.f == 1) ? (n / 3) % 3 : n / 9);
-        xq[n] = (T)(0.5 * a3);
-      }
-    }
-    if (PB) {
-#pragma unroll
-      for (int n = 0; n < 27; n++) avg += xq[n];
-      avg *= cst<T>(1.0 / 27.0);
-      T Lf = (L.f == 0) ? xq[14] - xq[12] : ((L.f == 1) ? xq[16] - xq[10] : xq[22] - xq[4]);
-      rL = (T)1 / Lf;
-    }
-    interp27(xq);
-    __syncthreads(); // every warp has read the coordinate tile: reuse it for the Gauss-point coordinates
-    if (L.active) {
-#pragma unroll
-      for (int n = 0; n < 27; n++) s_c[L.slot * 81 + L.f * 27 + n] = xq[n];
-    }
-  }
-  __syncwarp();
-  const T *X = s_c + L.slot * 81 + L.f * 27;
+  const T *E = s_c + L.slot * GQC;
+  const T *X = E + L.f * 27;           // coordinate f at the element's 27 Gauss points
+  const T avg = PB ? E[81 + L.f] : (T)0, rL = PB ? E[84 + L.f] : (T)1;
   const T *eta_e = s_k + L.slot * 27;
 
   const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
@@ -671,6 +653,46 @@ __global__ void pack_eta_kernel(int mx, int my, int mz, int ntx, int nty, int nt
     T v = (T)0;
     if (ex < mx && ey < my && ez < mz) v = (T)eta[27 * ((size_t)ex + (size_t)mx * ((size_t)ey + (size_t)my * ez)) + q];
     out[idx] = v;
+  }
+}
+
+// Gauss-point coordinate table (GQC values per element, brick order).  Slots
+// outside the mesh get a unit cube (their results are never written).
+template <typename T, int NW>
+__global__ void pack_gauss_coords_kernel(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, int ntx, int nty,
+                                         int ntz, const double *__restrict__ coords, T *__restrict__ out)
+{
+  using BK = Brick<NW>;
+  const size_t total = (size_t)ntx * nty * ntz * BK::NE;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int slot = idx % BK::NE;
+    const size_t t = idx / BK::NE;
+    const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / ((size_t)ntx * nty);
+    const int a = slot % TX, bb = (slot / TX) % TY, c = slot / (TX * TY);
+    const int ex = tx * TX + a, ey = ty * TY + bb, ez = tz * NW + c;
+    const bool valid = ex < mx && ey < my && ez < mz;
+    T *o = out + idx * GQC;
+    for (int f = 0; f < 3; f++) {
+      double xq[27];
+      for (int n = 0; n < 27; n++) {
+        const int na = n % 3, nb = (n / 3) % 3, nc = n / 9;
+        if (valid) {
+          const size_t gi = (size_t)(ox + 2 * ex + na) + (size_t)gx * ((size_t)(oy + 2 * ey + nb) + (size_t)gy * (oz + 2 * ez + nc));
+          xq[n] = coords[3 * gi + f];
+        } else {
+          xq[n] = 0.5 * (f == 0 ? na : (f == 1 ? nb : nc));
+        }
+      }
+      double avg = 0.0;
+      for (int n = 0; n < 27; n++) avg += xq[n];
+      avg *= 1.0 / 27.0;
+      const double Lf = (f == 0) ? xq[14] - xq[12] : ((f == 1) ? xq[16] - xq[10] : xq[22] - xq[4]);
+      interp27(xq);
+      for (int n = 0; n < 27; n++) o[27 * f + n] = (T)xq[n];
+      o[81 + f] = (T)avg;
+      o[84 + f] = (T)(1.0 / Lf);
+    }
+    o[87] = (T)0;
   }
 }
 
