@@ -4,9 +4,9 @@
 //   A CTA owns a brick of TX x TY x NW elements (TX=5, TY=2): warp w holds the
 //   element layer z=w, lanes 3*s+f (s = 0..9 element slot, f = 0..2 velocity
 //   component), lanes 30,31 idle.  The node brick (2TX+1)(2TY+1)(2NW+1) of x
-//   (and of the coordinates in the general-geometry path) is staged in shared
-//   memory with coalesced loads; each lane then works on ONE velocity
-//   component of ONE element entirely in registers:
+//   is staged in shared memory with coalesced loads, per-element data (eta,
+//   packed geometry) with contiguous 16-byte copies; each lane then works on
+//   ONE velocity component of ONE element in registers:
 //     1. interpolate its 27 nodal values to the 27 Gauss points (three 1-D
 //        stages of the Q2 basis at the Gauss points, B(0) row = [0,1,0]),
 //     2. per Gauss point take reference derivatives with the collocated
@@ -20,17 +20,17 @@
 //   (src/stokes_operators_tensor.c:40-288, src/stokes_operators_cuda.cu:79-159)
 //   re-associated through the Gauss-point values; it needs ~1/3 fewer flops
 //   and no cross-lane traffic except 2 shuffles per Gauss point.
-//   The nodal contributions go to shared memory, a deterministic gather sums
-//   the <=8 element contributions of every node of the brick, and the brick is
-//   added to y: plain read-modify-write for nodes no other CTA touches,
-//   atomicAdd for nodes on brick faces shared with neighbouring bricks.
+//   The nodal contributions are added into a shared node tile (parity classes
+//   of elements take turns, accumulate_phases), and the tile is written to y:
+//   plain stores for nodes no other CTA touches, atomicAdd for nodes on brick
+//   faces shared with neighbouring bricks.
 //
 // Geometry paths
-//   AFFINE : every element is a parallelepiped; setup stores per element
-//            J^{-1} (9) and eta*w*detJ per Gauss point (27) in brick order.
-//   general: coordinates are streamed; pass 1 builds J at the Gauss points
-//            (lane f owns column f), then each lane inverts 9 of the 27
-//            points into a per-element shared-memory table read by pass 2.
+//   AFFINE : setup stores per element J^{-1} of the element centre (9) and
+//            eta*w*detJ per Gauss point (27) in brick order; exact for
+//            parallelepipeds, the reference's low-order operator otherwise.
+//   general: the Jacobian of every Gauss point is recomputed per apply from
+//            the element's Gauss-point coordinates (stokes_kernels.cuh).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
