@@ -233,11 +233,15 @@ int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geo
     pack_eta_kernel<float, NW_GEN><<<grid_for(ng), 256, 0, st>>>(m.mx, m.my, m.mz, ntx, nty, ntz, eta, (float *)op->kgen);
   count_launch(1);
   if ((rc = cuda_check(cudaGetLastError(), "pack eta"))) return rc;
-  if (op->prec == P3D_PREC_F64) {
+  {
     const size_t ngq = (size_t)ntx * nty * ntz * Brick<NW_GEN>::NE;
-    if (!op->kgq && (rc = dev_alloc(&op->kgq, ngq * GQC * 8, "gauss-point coordinates"))) return rc;
-    pack_gauss_coords_kernel<double, NW_GEN><<<grid_for(ngq), 128, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz, ntx,
-                                                                           nty, ntz, coords, (double *)op->kgq);
+    if (!op->kgq && (rc = dev_alloc(&op->kgq, ngq * GQC * es, "gauss-point coordinates"))) return rc;
+    if (op->prec == P3D_PREC_F64)
+      pack_gauss_coords_kernel<double, NW_GEN><<<grid_for(ngq), 128, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz,
+                                                                             ntx, nty, ntz, coords, (double *)op->kgq);
+    else
+      pack_gauss_coords_kernel<float, NW_GEN><<<grid_for(ngq), 128, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz,
+                                                                            ntx, nty, ntz, coords, (float *)op->kgq);
     count_launch(1);
     if ((rc = cuda_check(cudaGetLastError(), "pack gauss coords"))) return rc;
   }

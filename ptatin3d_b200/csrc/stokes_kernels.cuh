@@ -395,17 +395,16 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
 
 // ---------------------------------------- general geometry, table variant
 // Used for FP32, where the table costs less than the shuffle exchange.
-// Geometry is built one Gauss-point plane (9 points, fixed k) at a time: the
-// interpolated coordinates of each element stay in shared memory and every
-// lane inverts 3 of the plane's 9 Jacobians, so the per-element geometry table
-// holds 9 points instead of 27 (3x less shared memory, more CTAs per SM).
+// Geometry is built one Gauss-point plane (9 points, fixed k) at a time from
+// the staged Gauss-point coordinate table: every lane inverts 3 of the plane's
+// 9 Jacobians into a per-element table read by all three lanes, which holds 9
+// points instead of 27 (3x less shared memory, more CTAs per SM).
 template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralTabSmem {
   using BK = Brick<NW>;
   static constexpr bool NEEDX = DA11 || DA21;
   static constexpr bool NEEDY = DA11 || DA12;
   static constexpr int GQ = (DA12 || DA21) ? 14 : 10;
-  static constexpr int CT = align16(3 * BK::NN, sizeof(T));  // coordinate tile / accumulator
-  static constexpr int CQ = align16(BK::NE * 81, sizeof(T)); // Gauss-point coordinates
+  static constexpr int CQ = align16(BK::NE * GQC, sizeof(T)); // Gauss-point coordinate table
   static constexpr int OX = 0;
   static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
   static constexpr int OC = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
@@ -428,37 +427,19 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
   T *sm = reinterpret_cast<T *>(p3d_smem);
   T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_c = sm + SM::OC, *s_k = sm + SM::OK, *s_g = sm + SM::OG;
   const BrickPos b = brick_pos<T, NW>(A);
+  const size_t brick = (size_t)blockIdx.x + A.brick0;
   if (SM::NEEDX) stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
-  stage_nodes<T, NW>(A, b, A.coords, s_c, false);
-  stage_block(A.kdat + (size_t)(blockIdx.x + A.brick0) * BK::NE * 27, s_k, BK::NE * 27);
+  stage_block(A.kgq + brick * BK::NE * GQC, s_c, BK::NE * GQC); // Gauss-point coordinates, centroid, 1/L
+  stage_block(A.kdat + brick * BK::NE * 27, s_k, BK::NE * 27);
   if (NEEDY && !A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
   cp_async_wait_all();
   __syncthreads();
 
   const LaneMap L = lane_map();
   const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
-  // coordinates at the Gauss points (lane f: coordinate f) and the pressure-basis scaling
-  T avg = (T)0, rL = (T)1;
-  {
-    T xq[27];
-#pragma unroll
-    for (int n = 0; n < 27; n++) xq[n] = s_c[3 * brick_node<NW>(L.a, L.b, L.c, n) + L.f];
-    if (PB) {
-#pragma unroll
-      for (int n = 0; n < 27; n++) avg += xq[n];
-      avg *= cst<T>(1.0 / 27.0);
-      T Lf = (L.f == 0) ? xq[14] - xq[12] : ((L.f == 1) ? xq[16] - xq[10] : xq[22] - xq[4]);
-      rL = valid ? (T)1 / Lf : (T)0;
-    }
-    interp27(xq);
-    __syncthreads(); // every warp has read the coordinate tile: reuse it for the Gauss-point coordinates
-    if (L.active) {
-#pragma unroll
-      for (int n = 0; n < 27; n++) s_c[L.slot * 81 + L.f * 27 + n] = xq[n];
-    }
-  }
-  __syncwarp();
-  const T *X = s_c + L.slot * 81 + L.f * 27;
+  const T *E = s_c + L.slot * GQC;
+  const T *X = E + L.f * 27; // coordinate f at the element's 27 Gauss points
+  const T avg = PB ? E[81 + L.f] : (T)0, rL = PB ? E[84 + L.f] : (T)1;
   const T *eta_e = s_k + L.slot * 27;
   T *g = s_g + L.slot * 9 * GQ;
 
