@@ -53,10 +53,18 @@ struct Pending {
   double t_submit;
 };
 
+static bool same_opts(const p3d_solver_opts &a, const p3d_solver_opts &b)
+{
+  return a.nlevels == b.nlevels && a.cheb_its == b.cheb_its && a.cheb_lo == b.cheb_lo && a.cheb_hi == b.cheb_hi &&
+         a.esteig_its == b.esteig_its && a.mg_precision == b.mg_precision && a.restart == b.restart &&
+         a.max_it == b.max_it && a.rtol == b.rtol && a.atol == b.atol && a.use_graph == b.use_graph &&
+         a.verbose == b.verbose && a.inner_its == b.inner_its && a.coarse_op == b.coarse_op &&
+         a.schur_eta == b.schur_eta && a.coarse_eta == b.coarse_eta;
+}
+
 static bool same_shape(const Slot &s, const p3d_request &r)
 {
-  return s.mx == r.mx && s.my == r.my && s.mz == r.mz && s.dirichlet == r.dirichlet &&
-         memcmp(&s.opts, &r.opts, sizeof(p3d_solver_opts)) == 0;
+  return s.mx == r.mx && s.my == r.my && s.mz == r.mz && s.dirichlet == r.dirichlet && same_opts(s.opts, r.opts);
 }
 
 static int64_t request_bytes(const p3d_request &r)

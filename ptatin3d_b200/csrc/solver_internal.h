@@ -26,6 +26,7 @@ template <typename T>
 void v_cg_xr(size_t n, const double *num, const double *den, T *x, T *r, const T *p, const T *q, bool update_r, cudaStream_t s);
 template <typename T> void v_cg_p(size_t n, const double *num, const double *den, const T *z, T *p, cudaStream_t s);
 void v_block4(size_t nel, const double *B, const double *x, double *y, double alpha, cudaStream_t s);
+void v_invert_diag(size_t n, const double *d, double *dinv, unsigned int *bad, cudaStream_t s);
 void v_dense_mv(int n, const double *M, const double *x, double *y, cudaStream_t s);
 
 // setup_kernels.cu (whole-mesh lattices, FP64)

@@ -522,15 +522,16 @@ static int solver_setup(p3d_solver *s, const double *coords, const double *eta)
       CU(cudaMemsetAsync(L.t, 0, L.nv * 8, s->st), "memset");
       CK(launch_diag<double>(L.op64, (double *)L.t, s->st));
     }
-    // dinv = 1 / diag
-    std::vector<double> hd(L.nv);
-    CU(cudaMemcpyAsync(hd.data(), L.t, L.nv * 8, cudaMemcpyDeviceToHost, s->st), "d2h diag");
-    CU(cudaStreamSynchronize(s->st), "diag");
-    for (auto &v : hd) {
-      if (!(v > 0) || !std::isfinite(v)) return set_error(P3D_ERR_BREAKDOWN, "non-positive A11 diagonal %g", v);
-      v = 1.0 / v;
+    // dinv = 1 / diag on the device; only the count of bad entries comes back
+    {
+      unsigned int *bad = reinterpret_cast<unsigned int *>(s->hdev + 2 * s->hs + 1);
+      CU(cudaMemsetAsync(bad, 0, sizeof(unsigned int), s->st), "memset");
+      v_invert_diag(L.nv, (const double *)L.t, L.dinv, bad, s->st);
+      unsigned int hbad = 0;
+      CU(cudaMemcpyAsync(&hbad, bad, sizeof hbad, cudaMemcpyDeviceToHost, s->st), "d2h");
+      CU(cudaStreamSynchronize(s->st), "diag");
+      if (hbad) return set_error(P3D_ERR_BREAKDOWN, "A11 diagonal: %u entries not positive on level %d", hbad, l);
     }
-    CU(cudaMemcpyAsync(L.dinv, hd.data(), L.nv * 8, cudaMemcpyHostToDevice, s->st), "h2d dinv");
     if (l > 0) CK(estimate_lmax(s, L));
   }
   CK(build_coarse(s));

@@ -167,6 +167,20 @@ __global__ void k_cg_p(size_t n, const double *__restrict__ num, const double *_
   GS_LOOP(i, n) p[i] = (T)((double)z[i] + b * (double)p[i]);
 }
 
+// dinv = 1/d; counts entries that are not positive and finite
+__global__ void k_invert_diag(size_t n, const double *__restrict__ d, double *__restrict__ dinv, unsigned int *__restrict__ bad)
+{
+  unsigned nb = 0;
+  GS_LOOP(i, n)
+  {
+    const double v = d[i];
+    const bool ok = v > 0.0 && isfinite(v);
+    dinv[i] = ok ? 1.0 / v : 1.0;
+    nb += ok ? 0u : 1u;
+  }
+  if (nb) atomicAdd(bad, nb);
+}
+
 // y = blockdiag(B_e) x  with B_e 4x4 per element (Schur approximation inverse)
 __global__ void k_block4(size_t nel, const double *__restrict__ B, const double *__restrict__ x, double *__restrict__ y, double alpha)
 {
@@ -287,6 +301,11 @@ void v_cg_xr(size_t n, const double *num, const double *den, T *x, T *r, const T
 template <typename T> void v_cg_p(size_t n, const double *num, const double *den, const T *z, T *p, cudaStream_t s)
 {
   k_cg_p<<<vgrid(n), 256, 0, s>>>(n, num, den, z, p);
+  count_launch(1);
+}
+void v_invert_diag(size_t n, const double *d, double *dinv, unsigned int *bad, cudaStream_t s)
+{
+  k_invert_diag<<<vgrid(n), 256, 0, s>>>(n, d, dinv, bad);
   count_launch(1);
 }
 void v_block4(size_t nel, const double *B, const double *x, double *y, double alpha, cudaStream_t s)
