@@ -20,8 +20,8 @@
 //   (src/stokes_operators_tensor.c:40-288, src/stokes_operators_cuda.cu:79-159)
 //   re-associated through the Gauss-point values; it needs ~1/3 fewer flops
 //   and no cross-lane traffic except 2 shuffles per Gauss point.
-//   The nodal contributions are added into a shared node tile (parity classes
-//   of elements take turns, accumulate_phases), and the tile is written to y:
+//   The nodal contributions are added into a shared node tile (shared-memory
+//   atomic adds, accumulate_phases), and the tile is written to y:
 //   plain stores for nodes no other CTA touches, atomicAdd for nodes on brick
 //   faces shared with neighbouring bricks.
 //
@@ -152,7 +152,6 @@ template <int NW> struct Brick {
   static constexpr int NN = NX * NY * NZ;
   static constexpr int NE = TX * TY * NW;
   static constexpr int PL = 3 * NX * NY;          // values of one node plane
-  static constexpr int BOT = (NW - 1) * PL;       // bottom planes of warps 1..NW-1 (accumulation)
 };
 
 // Brick geometry for blockIdx.x
@@ -239,36 +238,18 @@ template <typename T> __device__ __forceinline__ void stage_block(const T *__res
 }
 
 // Add the lane's 27 nodal contributions r[] into the brick's node tile s_acc
-// (zeroed by the caller, with the Brick::BOT values after it).  Warp c owns
-// element layer c, i.e. node planes 2c..2c+2; plane 2c+2 is also the bottom
-// plane of warp c+1, so warps c >= 1 put their bottom plane into a private
-// buffer (s_acc + 3*NN) that is folded in after one CTA barrier.  Inside a
-// warp, elements whose (a,b) parities agree share no node: 4 parity classes
-// take turns, separated by __syncwarp, and every update is a plain
-// shared-memory read-modify-write.  Must be reached by every thread.
+// (zeroed by the caller) with shared-memory atomic adds: every lane adds at
+// once, and the few nodes that neighbouring elements share are serialised by
+// the hardware (measured faster than parity classes taking turns).  Must be
+// reached by every thread of the CTA.
 template <typename T, int NW>
 __device__ __forceinline__ void accumulate_phases(T *s_acc, const T r[27], int a, int bb, int c, int f, bool doit)
 {
   using BK = Brick<NW>;
-  T *s_bot = s_acc + 3 * BK::NN;
-  const int par = (a & 1) | ((bb & 1) << 1);
   T *base = s_acc + 3 * (2 * a + BK::NX * (2 * bb + BK::NY * 2 * c)) + f;
-  T *bot = c > 0 ? s_bot + (c - 1) * BK::PL + 3 * (2 * a + BK::NX * 2 * bb) + f : base;
-  for (int ph = 0; ph < 4; ph++) {
-    if (doit && ph == par) {
+  if (doit) {
 #pragma unroll
-      for (int n = 0; n < 27; n++) {
-        const int off = 3 * ((n % 3) + BK::NX * ((n / 3) % 3));
-        if (n / 9 == 0) bot[off] += r[n];
-        else base[off + (n / 9) * BK::PL] += r[n];
-      }
-    }
-    __syncwarp();
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < BK::BOT; i += blockDim.x) {
-    const int cz = i / BK::PL + 1;
-    s_acc[2 * cz * BK::PL + (i - (cz - 1) * BK::PL)] += s_bot[i];
+    for (int n = 0; n < 27; n++) atomicAdd(base + 3 * ((n % 3) + BK::NX * ((n / 3) % 3)) + (n / 9) * BK::PL, r[n]);
   }
   __syncthreads();
 }

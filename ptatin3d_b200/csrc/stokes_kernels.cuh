@@ -166,7 +166,7 @@ template <typename T, int NW> struct AffineSmem {
   static constexpr int OY = OX + align16(3 * BK::NN, sizeof(T));
   static constexpr int OK = OY + align16(3 * BK::NN, sizeof(T));
   static constexpr int OA = OK + align16(BK::NE * KS, sizeof(T)); // node-tile accumulator
-  static constexpr int TOTAL = OA + 3 * BK::NN + BK::BOT;
+  static constexpr int TOTAL = OA + 3 * BK::NN;
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
 };
 
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(32 * NW, 4) a11_affine_kernel(TileArgs<T> A)
   stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
   stage_block(A.kdat + (size_t)(blockIdx.x + A.brick0) * BK::NE * SM::KS, s_k, BK::NE * SM::KS);
   if (!A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
-  for (int i = threadIdx.x; i < 3 * BK::NN + BK::BOT; i += blockDim.x) s_acc[i] = (T)0;
+  for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
   cp_async_wait_all();
   __syncthreads();
 
@@ -246,7 +246,7 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSme
   static constexpr int OX = 0;
   static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
   static constexpr int OC = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
-  static constexpr int CA = align16(3 * BK::NN + BK::BOT, sizeof(T)); // accumulator (reuses the tile region)
+  static constexpr int CA = align16(3 * BK::NN, sizeof(T)); // accumulator (reuses the tile region)
   static constexpr int OK = OC + (CA > CQ ? CA : CQ);
   static constexpr int TOTAL = OK + align16(BK::NE * 27, sizeof(T));
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
     interp27T(r);
     __syncthreads(); // every warp is done with the Gauss-point coordinates: reuse as the accumulator
     T *s_acc = s_c;
-    for (int i = threadIdx.x; i < 3 * BK::NN + BK::BOT; i += blockDim.x) s_acc[i] = (T)0;
+    for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
     __syncthreads();
     accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
@@ -408,7 +408,7 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralTab
   static constexpr int OX = 0;
   static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
   static constexpr int OC = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
-  static constexpr int CA = align16(3 * BK::NN + BK::BOT, sizeof(T)); // accumulator (reuses the tile region)
+  static constexpr int CA = align16(3 * BK::NN, sizeof(T)); // accumulator (reuses the tile region)
   static constexpr int OK = OC + (CA > CQ ? CA : CQ);
   static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
   static constexpr int TOTAL = OG + BK::NE * 9 * GQ;
@@ -543,7 +543,7 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
     interp27T(r);
     __syncthreads(); // every warp is done with the Gauss-point coordinates: reuse as the accumulator
     T *s_acc = s_c;
-    for (int i = threadIdx.x; i < 3 * BK::NN + BK::BOT; i += blockDim.x) s_acc[i] = (T)0;
+    for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
     __syncthreads();
     accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
@@ -559,7 +559,7 @@ template <typename T, int NW> struct DiagSmem {
   static constexpr int GQ = 10;
   static constexpr int OY = 0;
   static constexpr int OC = OY + align16(3 * BK::NN, sizeof(T));
-  static constexpr int OK = OC + align16(3 * BK::NN + BK::BOT, sizeof(T));
+  static constexpr int OK = OC + align16(3 * BK::NN, sizeof(T));
   static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
   static constexpr int TOTAL = OG + BK::NE * 27 * GQ;
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
   }
   __syncthreads();
   T *s_acc = s_c;
-  for (int i = threadIdx.x; i < 3 * BK::NN + BK::BOT; i += blockDim.x) s_acc[i] = (T)0;
+  for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
   __syncthreads();
   accumulate_phases<T, NW>(s_acc, dg, L.a, L.b, L.c, L.f, L.active && valid);
   write_tile<T, NW>(A, b, s_acc, s_y, 2);
