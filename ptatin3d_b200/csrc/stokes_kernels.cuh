@@ -216,12 +216,20 @@ __global__ void __launch_bounds__(32 * NW, 4) a11_affine_kernel(TileArgs<T> A)
   write_tile<T, NW>(A, b, s_acc, s_y, 0);
 }
 
-// Gauss-point coordinate table of one element (general FP64 path), packed at
-// setup in brick order: the 27 Gauss-point values of each coordinate f
-// ([f][27], the tensor interpolation of the element's nodes), the centroid of
-// the 27 nodes (3 values) and the reciprocal mid-face extents 1/L (3 values)
-// of the pressure basis, one pad value (16-byte multiple).
+// Gauss-point coordinate table (general path), packed at setup, GQC values per
+// element in blocks of one brick.  A brick's block holds
+//   [n][slot][f]  the coordinate f of element slot at Gauss point n (27 x NE x 3,
+//                 the tensor interpolation of the element's nodes), so that the
+//                 30 lanes of a warp read 30 consecutive values (no bank conflicts);
+//   [slot][6]     the centroid of the 27 nodes (3 values) and the reciprocal
+//                 mid-face extents 1/L (3 values) of the pressure basis;
+//   zeros up to NE * GQC values.
 constexpr int GQC = 88;
+template <int NW> struct GQLayout {
+  static constexpr int PT = 3 * Brick<NW>::NE; // values per Gauss point
+  static constexpr int EX = 27 * PT;           // start of the per-element extras
+  static_assert(EX + 6 * Brick<NW>::NE <= GQC * Brick<NW>::NE, "Gauss-point table block");
+};
 
 // ------------------------------------------------------- general geometry
 // The Jacobian is recomputed at every Gauss point.  Lane f owns column f of
@@ -233,11 +241,11 @@ constexpr int GQC = 88;
 // and of the pulled-back stress combine into one scale eta*w/det per point,
 // so the action runs on the unscaled adjugate.  The element's Gauss-point
 // coordinates come from the setup-time table (one contiguous 16-byte copy per
-// brick instead of node rows and an interpolation per apply) and are read one
-// point plane (9 points) at a time.  The register cap (6 CTAs of 64 threads per SM, 168
-// registers) trades a few hundred bytes of spills for 50 % more resident warps,
-// which this latency-bound kernel converts into speed (measured at 96^3:
-// 1.65 ms uncapped, 1.45 ms capped; 128 registers: 1.52 ms).
+// brick instead of node rows and an interpolation per apply); each point reads
+// the up to 7 coordinate values its column needs from shared memory, which keeps
+// the spills of the 168-register cap to 64 bytes.  The cap (6 CTAs of 64
+// threads per SM) gives 50 % more resident warps than the uncapped 254
+// registers, which this latency-bound kernel converts into speed.
 template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSmem {
   using BK = Brick<NW>;
   static constexpr bool NEEDX = DA11 || DA21;
@@ -273,9 +281,9 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
 
   const LaneMap L = lane_map();
   const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
-  const T *E = s_c + L.slot * GQC;
-  const T *X = E + L.f * 27;           // coordinate f at the element's 27 Gauss points
-  const T avg = PB ? E[81 + L.f] : (T)0, rL = PB ? E[84 + L.f] : (T)1;
+  using GL = GQLayout<NW>;
+  const T *X = s_c + 3 * L.slot + L.f; // coordinate f at Gauss point n: X[n * GL::PT]
+  const T avg = PB ? s_c[GL::EX + 6 * L.slot + L.f] : (T)0, rL = PB ? s_c[GL::EX + 6 * L.slot + 3 + L.f] : (T)1;
   const T *eta_e = s_k + L.slot * 27;
 
   const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
@@ -296,34 +304,25 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
   T ap0 = 0, ap1 = 0, ap2 = 0, ap3 = 0; // A21: [1, hat_f, hat_{f+1}, hat_{f+2}] moments
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    // ---- plane k: column f of M at the plane's 9 points
-    T c0[9], c1[9], c2[9], hat[9];
-    {
-      T xp[27];
-#pragma unroll
-      for (int n = 0; n < 27; n++) xp[n] = X[n];
-#pragma unroll
-      for (int j = 0; j < 3; j++)
-#pragma unroll
-        for (int i = 0; i < 3; i++) {
-          const int q9 = i + 3 * j;
-          c0[q9] = dcol(i, xp[3 * j + 9 * k], xp[1 + 3 * j + 9 * k], xp[2 + 3 * j + 9 * k]);
-          c1[q9] = dcol(j, xp[i + 9 * k], xp[i + 3 + 9 * k], xp[i + 6 + 9 * k]);
-          c2[q9] = dcol(k, xp[i + 3 * j], xp[i + 3 * j + 9], xp[i + 3 * j + 18]);
-          if (PB) hat[q9] = (xp[q9 + 9 * k] - avg) * rL;
-        }
-    }
 #pragma unroll
     for (int j = 0; j < 3; j++)
 #pragma unroll
       for (int i = 0; i < 3; i++) {
         const int q9 = i + 3 * j;
+        // column f of M at this point, straight from the staged Gauss-point
+        // coordinates (conflict-free reads; keeping a plane's columns in
+        // registers instead costs spills)
+#define P3D_XG(n) X[(n) * GL::PT]
+        const T cc0 = dcol(i, P3D_XG(3 * j + 9 * k), P3D_XG(1 + 3 * j + 9 * k), P3D_XG(2 + 3 * j + 9 * k));
+        const T cc1 = dcol(j, P3D_XG(i + 9 * k), P3D_XG(i + 3 + 9 * k), P3D_XG(i + 6 + 9 * k));
+        const T cc2 = dcol(k, P3D_XG(i + 3 * j), P3D_XG(i + 3 * j + 9), P3D_XG(i + 3 * j + 18));
+        const T hq = PB ? (P3D_XG(q9 + 9 * k) - avg) * rL : (T)0;
+#undef P3D_XG
         // the element's other two columns: a = col_{f+1}, bb = col_{f+2}
-        const T a0 = __shfl_sync(0xffffffffu, c0[q9], src1), a1 = __shfl_sync(0xffffffffu, c1[q9], src1),
-                a2 = __shfl_sync(0xffffffffu, c2[q9], src1);
-        const T b0 = __shfl_sync(0xffffffffu, c0[q9], src2), b1 = __shfl_sync(0xffffffffu, c1[q9], src2),
-                b2 = __shfl_sync(0xffffffffu, c2[q9], src2);
-        const T cc0 = c0[q9], cc1 = c1[q9], cc2 = c2[q9];
+        const T a0 = __shfl_sync(0xffffffffu, cc0, src1), a1 = __shfl_sync(0xffffffffu, cc1, src1),
+                a2 = __shfl_sync(0xffffffffu, cc2, src1);
+        const T b0 = __shfl_sync(0xffffffffu, cc0, src2), b1 = __shfl_sync(0xffffffffu, cc1, src2),
+                b2 = __shfl_sync(0xffffffffu, cc2, src2);
         // unscaled rows of M^{-1}: R0 (direction f) = a x b, R1 = b x c, R2 = c x a
         T Jr[9];
         Jr[0] = a1 * b2 - a2 * b1; Jr[1] = a2 * b0 - a0 * b2; Jr[2] = a0 * b1 - a1 * b0;
@@ -345,7 +344,7 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
         }
         if (PB) {
           // hats of the element's three lanes, rotated: h0 = hat_f, h1 = hat_{f+1}, h2 = hat_{f+2}
-          const T h0 = hat[q9], h1 = __shfl_sync(0xffffffffu, h0, src1), h2 = __shfl_sync(0xffffffffu, h0, src2);
+          const T h0 = hq, h1 = __shfl_sync(0xffffffffu, h0, src1), h2 = __shfl_sync(0xffffffffu, h0, src2);
           if (DA12) {
             // -w detJ p_q grad(N) = -w p_q * (adjugate row f) (det cancels)
             const T t = valid ? -wq * (pr0 + pr1 * h0 + pr2 * h1 + pr3 * h2) : (T)0;
@@ -437,9 +436,9 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
 
   const LaneMap L = lane_map();
   const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
-  const T *E = s_c + L.slot * GQC;
-  const T *X = E + L.f * 27; // coordinate f at the element's 27 Gauss points
-  const T avg = PB ? E[81 + L.f] : (T)0, rL = PB ? E[84 + L.f] : (T)1;
+  using GL = GQLayout<NW>;
+  const T *X = s_c + 3 * L.slot + L.f; // coordinate f at Gauss point n: X[n * GL::PT]
+  const T avg = PB ? s_c[GL::EX + 6 * L.slot + L.f] : (T)0, rL = PB ? s_c[GL::EX + 6 * L.slot + 3 + L.f] : (T)1;
   const T *eta_e = s_k + L.slot * 27;
   T *g = s_g + L.slot * 9 * GQ;
 
@@ -459,7 +458,7 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
     {
       T xp[27];
 #pragma unroll
-      for (int n = 0; n < 27; n++) xp[n] = X[n];
+      for (int n = 0; n < 27; n++) xp[n] = X[n * GL::PT];
 #pragma unroll
       for (int j = 0; j < 3; j++)
 #pragma unroll
@@ -637,8 +636,8 @@ __global__ void pack_eta_kernel(int mx, int my, int mz, int ntx, int nty, int nt
   }
 }
 
-// Gauss-point coordinate table (GQC values per element, brick order).  Slots
-// outside the mesh get a unit cube (their results are never written).
+// Gauss-point coordinate table (GQLayout, one block per brick).  Slots outside
+// the mesh get a unit cube (their results are never written).
 template <typename T, int NW>
 __global__ void pack_gauss_coords_kernel(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, int ntx, int nty,
                                          int ntz, const double *__restrict__ coords, T *__restrict__ out)
@@ -652,7 +651,8 @@ __global__ void pack_gauss_coords_kernel(int mx, int my, int mz, int gx, int gy,
     const int a = slot % TX, bb = (slot / TX) % TY, c = slot / (TX * TY);
     const int ex = tx * TX + a, ey = ty * TY + bb, ez = tz * NW + c;
     const bool valid = ex < mx && ey < my && ez < mz;
-    T *o = out + idx * GQC;
+    using GL = GQLayout<NW>;
+    T *o = out + t * (BK::NE * GQC);
     for (int f = 0; f < 3; f++) {
       double xq[27];
       for (int n = 0; n < 27; n++) {
@@ -669,11 +669,12 @@ __global__ void pack_gauss_coords_kernel(int mx, int my, int mz, int gx, int gy,
       avg *= 1.0 / 27.0;
       const double Lf = (f == 0) ? xq[14] - xq[12] : ((f == 1) ? xq[16] - xq[10] : xq[22] - xq[4]);
       interp27(xq);
-      for (int n = 0; n < 27; n++) o[27 * f + n] = (T)xq[n];
-      o[81 + f] = (T)avg;
-      o[84 + f] = (T)(1.0 / Lf);
+      for (int n = 0; n < 27; n++) o[n * GL::PT + 3 * slot + f] = (T)xq[n];
+      o[GL::EX + 6 * slot + f] = (T)avg;
+      o[GL::EX + 6 * slot + 3 + f] = (T)(1.0 / Lf);
     }
-    o[87] = (T)0;
+    if (slot == 0)
+      for (int i = GL::EX + 6 * BK::NE; i < BK::NE * GQC; i++) o[i] = (T)0;
   }
 }
 
