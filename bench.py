@@ -217,8 +217,11 @@ def solve_leg(device, m=32, seed=1):
         u, p = sols[name]
         out[name]["u_err"] = float(np.linalg.norm(u - ur) / np.linalg.norm(ur))
         out[name]["p_err"] = float(np.linalg.norm(p - pr) / np.linalg.norm(pr))
+    (u64, p64), (u32, p32) = sols["fp64"], sols["mixed"]
     return {"workload": SOLVE_WORKLOAD, "unit": "s", "fp64_s": out["fp64"]["s"], "mixed_s": out["mixed"]["s"],
             "speedup_mixed_vs_fp64": out["fp64"]["s"] / out["mixed"]["s"], "fp64": out["fp64"], "mixed": out["mixed"],
+            "u_diff_mixed_vs_fp64": float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64)),
+            "p_diff_mixed_vs_fp64": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64)),
             "oracle_solve": out["ref"]}
 
 
