@@ -35,31 +35,39 @@ static int ggrid(size_t n)
 
 #define G_LOOP(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
 
-// y = G x (overwrites y); accumulation in T.  One thread per (row component r,
-// node): threads of a warp share r and read 32 consecutive nodes' coefficients
-// (coalesced); the x values of a neighbourhood are shared through L1 by the
-// three row threads of a node.
+// y = G x (overwrites y); accumulation in T.  A block covers 32 consecutive
+// nodes with 9 warps, one per (row component r, neighbour plane dk): each
+// thread sums the 9 neighbours of its plane (27 coalesced coefficient loads,
+// the x values shared through L1), and the three plane partials of a row meet
+// in shared memory.  Nine independent load streams per node keep enough bytes
+// in flight to stream the coefficients even on the small coarse levels.
+constexpr int STENCIL_NODES = 32;
 template <typename T>
-__global__ void __launch_bounds__(256) k_stencil_apply(int nx, int ny, int nz, const T *__restrict__ G, const T *__restrict__ x,
-                                                       T *__restrict__ y)
+__global__ void __launch_bounds__(9 * STENCIL_NODES) k_stencil_apply(int nx, int ny, int nz, const T *__restrict__ G,
+                                                                    const T *__restrict__ x, T *__restrict__ y)
 {
+  __shared__ T part[9][STENCIL_NODES];
   const size_t nn = (size_t)nx * ny * nz;
-  G_LOOP(t, 3 * nn)
-  {
-    const int r = (int)(t / nn);
-    const size_t i = t - (size_t)r * nn;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5; // w = 3 r + (dk + 1)
+  const int r = w / 3, dk = w % 3 - 1;
+  const size_t i = (size_t)blockIdx.x * STENCIL_NODES + lane;
+  T a = 0;
+  if (i < nn) {
     const int I = i % nx, J = (i / nx) % ny, K = i / ((size_t)nx * ny);
-    T a = 0;
+    if (K + dk >= 0 && K + dk < nz) {
 #pragma unroll
-    for (int o = 0; o < 27; o++) {
-      const int di = o % 3 - 1, dj = (o / 3) % 3 - 1, dk = o / 9 - 1;
-      if (I + di < 0 || I + di >= nx || J + dj < 0 || J + dj >= ny || K + dk < 0 || K + dk >= nz) continue;
-      const long long j = (long long)i + di + (long long)nx * (dj + (long long)ny * dk);
-      const T *g = G + ((size_t)o * 9 + 3 * r) * nn + i;
-      a += g[0] * x[3 * j] + g[nn] * x[3 * j + 1] + g[2 * nn] * x[3 * j + 2];
+      for (int o9 = 0; o9 < 9; o9++) {
+        const int di = o9 % 3 - 1, dj = o9 / 3 - 1;
+        if (I + di < 0 || I + di >= nx || J + dj < 0 || J + dj >= ny) continue;
+        const long long j = (long long)i + di + (long long)nx * (dj + (long long)ny * dk);
+        const T *g = G + ((size_t)((dk + 1) * 9 + o9) * 9 + 3 * r) * nn + i;
+        a += g[0] * x[3 * j] + g[nn] * x[3 * j + 1] + g[2 * nn] * x[3 * j + 2];
+      }
     }
-    y[3 * i + r] = a;
   }
+  part[w][lane] = a;
+  __syncthreads();
+  if (dk == -1 && i < nn) y[3 * i + r] = part[w][lane] + part[w + 1][lane] + part[w + 2][lane];
 }
 
 // probe vector: component d of every node of colour (ci,cj,ck), zero on Dirichlet dofs
@@ -137,7 +145,8 @@ __global__ void k_stencil_dense(int nx, int ny, int nz, const double *__restrict
 
 template <typename T> void g_apply(int nx, int ny, int nz, const T *G, const T *x, T *y, cudaStream_t s)
 {
-  k_stencil_apply<T><<<ggrid(3 * (size_t)nx * ny * nz), 256, 0, s>>>(nx, ny, nz, G, x, y);
+  const size_t nn = (size_t)nx * ny * nz;
+  k_stencil_apply<T><<<(unsigned)((nn + STENCIL_NODES - 1) / STENCIL_NODES), 9 * STENCIL_NODES, 0, s>>>(nx, ny, nz, G, x, y);
   count_launch(1);
 }
 void g_probe_vec(int nx, int ny, int nz, int ci, int cj, int ck, int d, uint32_t dir, double *x, cudaStream_t s)

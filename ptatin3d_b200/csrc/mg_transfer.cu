@@ -11,6 +11,8 @@
 
 #include "p3d_b200.h"
 #include "p3d_internal.h"
+#include "q2_tile.cuh"
+#include "solver_internal.h"
 
 namespace p3d {
 
@@ -64,6 +66,65 @@ __global__ void restrict_kernel(int cnx, int cny, int cnz, int ndof, const T *__
   }
 }
 
+// Velocity V-cycle forms (3 dofs per node, Dirichlet bits dir on the faces of
+// both lattices): the residual b - Ax is formed on the fly and its Dirichlet
+// dofs count as zero, the coarse Dirichlet dofs are zeroed; one pass instead
+// of residual, mask, restriction and mask.
+template <typename T>
+__global__ void restrict_residual_kernel(int cnx, int cny, int cnz, uint32_t dir, const T *__restrict__ b,
+                                         const T *__restrict__ Ax, T *__restrict__ xc)
+{
+  const int fnx = 2 * cnx - 1, fny = 2 * cny - 1, fnz = 2 * cnz - 1;
+  const size_t total = (size_t)cnx * cny * cnz * 3;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int d = idx % 3;
+    const size_t node = idx / 3;
+    const int I = node % cnx, J = (node / cnx) % cny, K = node / ((size_t)cnx * cny);
+    if (is_dirichlet(dir, I, J, K, 0, 0, 0, cnx - 1, cny - 1, cnz - 1, d)) {
+      xc[idx] = (T)0;
+      continue;
+    }
+    T acc = (T)0;
+    for (int c = -1; c <= 1; c++) {
+      const int k = 2 * K + c;
+      if (k < 0 || k >= fnz) continue;
+      const T wk = c == 0 ? (T)1 : (T)0.5;
+      for (int bb = -1; bb <= 1; bb++) {
+        const int j = 2 * J + bb;
+        if (j < 0 || j >= fny) continue;
+        const T wj = bb == 0 ? (T)1 : (T)0.5;
+        for (int a = -1; a <= 1; a++) {
+          const int i = 2 * I + a;
+          if (i < 0 || i >= fnx) continue;
+          if (is_dirichlet(dir, i, j, k, 0, 0, 0, fnx - 1, fny - 1, fnz - 1, d)) continue;
+          const T wi = a == 0 ? (T)1 : (T)0.5;
+          const size_t f = ((size_t)i + (size_t)fnx * ((size_t)j + (size_t)fny * k)) * 3 + d;
+          acc += wi * wj * wk * (b[f] - Ax[f]);
+        }
+      }
+    }
+    xc[idx] = acc;
+  }
+}
+
+template <typename T>
+__global__ void prolong_add_kernel(int cnx, int cny, int cnz, uint32_t dir, const T *__restrict__ xc, T *__restrict__ xf)
+{
+  const int fnx = 2 * cnx - 1, fny = 2 * cny - 1, fnz = 2 * cnz - 1;
+  const size_t total = (size_t)fnx * fny * fnz * 3;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+    const int d = idx % 3;
+    const size_t node = idx / 3;
+    const int i = node % fnx, j = (node / fnx) % fny, k = node / ((size_t)fnx * fny);
+    if (is_dirichlet(dir, i, j, k, 0, 0, 0, fnx - 1, fny - 1, fnz - 1, d)) continue;
+    const int i0 = i >> 1, i1 = (i + 1) >> 1, j0 = j >> 1, j1 = (j + 1) >> 1, k0 = k >> 1, k1 = (k + 1) >> 1;
+    auto C = [&](int a, int bb, int c) { return xc[((size_t)a + (size_t)cnx * ((size_t)bb + (size_t)cny * c)) * 3 + d]; };
+    const T s00 = C(i0, j0, k0) + C(i1, j0, k0), s10 = C(i0, j1, k0) + C(i1, j1, k0);
+    const T s01 = C(i0, j0, k1) + C(i1, j0, k1), s11 = C(i0, j1, k1) + C(i1, j1, k1);
+    xf[idx] += (T)0.125 * ((s00 + s10) + (s01 + s11));
+  }
+}
+
 static int tgrid(size_t n)
 {
   size_t g = (n + 255) / 256;
@@ -85,6 +146,25 @@ template <typename T> int mg_restrict(int cnx, int cny, int cnz, int ndof, const
   count_launch(1);
   return cuda_check(cudaGetLastError(), "restrict launch");
 }
+template <typename T>
+int mg_restrict_residual(int cnx, int cny, int cnz, uint32_t dir, const T *b, const T *Ax, T *xc, cudaStream_t st)
+{
+  size_t n = (size_t)cnx * cny * cnz * 3;
+  restrict_residual_kernel<T><<<tgrid(n), 256, 0, st>>>(cnx, cny, cnz, dir, b, Ax, xc);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "restrict launch");
+}
+template <typename T> int mg_prolong_add(int cnx, int cny, int cnz, uint32_t dir, const T *xc, T *xf, cudaStream_t st)
+{
+  size_t n = (size_t)(2 * cnx - 1) * (2 * cny - 1) * (2 * cnz - 1) * 3;
+  prolong_add_kernel<T><<<tgrid(n), 256, 0, st>>>(cnx, cny, cnz, dir, xc, xf);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "prolong launch");
+}
+template int mg_restrict_residual<double>(int, int, int, uint32_t, const double *, const double *, double *, cudaStream_t);
+template int mg_restrict_residual<float>(int, int, int, uint32_t, const float *, const float *, float *, cudaStream_t);
+template int mg_prolong_add<double>(int, int, int, uint32_t, const double *, double *, cudaStream_t);
+template int mg_prolong_add<float>(int, int, int, uint32_t, const float *, float *, cudaStream_t);
 template int mg_prolong<double>(int, int, int, int, const double *, double *, cudaStream_t);
 template int mg_prolong<float>(int, int, int, int, const float *, float *, cudaStream_t);
 template int mg_restrict<double>(int, int, int, int, const double *, double *, cudaStream_t);

@@ -25,6 +25,8 @@ struct p3d_op {
   void *kgen = nullptr;   // general path: eta, brick order (NW_GEN)
   void *kgq = nullptr;    // general FP64 path: Gauss-point coordinate table, brick order (NW_GEN)
   void *kaff = nullptr;   // affine path: J^{-1} + eta*w*detJ, brick order (NW_AFF)
+  void *kpre = nullptr;   // affine path: pressure-basis map + detJ, brick order (NW_AFF)
+  bool aff_exact = false; // every element tested affine: A12/A21 take the affine kernels too
   void *hx = nullptr, *hy = nullptr; // host-apply staging
   unsigned long long *flag = nullptr; // affinity test result (kept: re-setup allocates nothing)
   cudaStream_t s_h2d = nullptr, s_d2h = nullptr; // host-apply copy streams

@@ -102,29 +102,39 @@ template <typename T> static int brick_range(TileArgs<T> &a, int tzb, int tze)
 
 int a11_brick_height(const p3d_op *op) { return op->geom == P3D_GEOM_AFFINE ? NW_AFF : NW_GEN; }
 
+// per-element constant Jacobian: A11 on affine meshes (or the low-order
+// operator), and A12 / A21 / the fused operator where every element was tested affine
+template <typename T, bool DA11, bool DA12, bool DA21>
+static int launch_affine(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st, bool overwrite, int tzb,
+                         int tze)
+{
+  TileArgs<T> a = tile_args<T>(op, NW_AFF);
+  a.x = u; a.y = yu; a.p = p; a.yp = yp;
+  a.kdat = reinterpret_cast<const T *>(op->kaff);
+  a.kgq = reinterpret_cast<const T *>(op->kpre);
+  a.overwrite = overwrite ? 1 : 0;
+  auto kern = stokes_affine_kernel<T, NW_AFF, DA11, DA12, DA21>;
+  size_t smem = AffineSmem<T, NW_AFF, DA11, DA12, DA21>::BYTES;
+  int rc = prep_kernel(kern, smem);
+  if (rc) return rc;
+  const int nb = brick_range(a, tzb, tze);
+  if (nb == 0) return P3D_OK;
+  kern<<<nb, 32 * NW_AFF, smem, st>>>(a);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "affine launch");
+}
+
 template <typename T> int launch_a11(p3d_op *op, const T *x, T *y, cudaStream_t st, bool overwrite, int tzb, int tze)
 {
-  if (op->geom == P3D_GEOM_AFFINE) {
-    TileArgs<T> a = tile_args<T>(op, NW_AFF);
-    a.x = x; a.y = y; a.kdat = reinterpret_cast<const T *>(op->kaff);
-    a.overwrite = overwrite ? 1 : 0;
-    auto kern = a11_affine_kernel<T, NW_AFF>;
-    size_t smem = AffineSmem<T, NW_AFF>::BYTES;
-    int rc = prep_kernel(kern, smem);
-    if (rc) return rc;
-    const int nb = brick_range(a, tzb, tze);
-    if (nb == 0) return P3D_OK;
-    kern<<<nb, 32 * NW_AFF, smem, st>>>(a);
-  } else {
-    return launch_general<T, true, false, false>(op, x, nullptr, y, nullptr, st, overwrite, tzb, tze);
-  }
-  count_launch(1);
-  return cuda_check(cudaGetLastError(), "a11 launch");
+  if (op->geom == P3D_GEOM_AFFINE) return launch_affine<T, true, false, false>(op, x, nullptr, y, nullptr, st, overwrite, tzb, tze);
+  return launch_general<T, true, false, false>(op, x, nullptr, y, nullptr, st, overwrite, tzb, tze);
 }
 
 template <typename T, bool DA11, bool DA12, bool DA21>
 int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_t st, bool overwrite, int tzb, int tze)
 {
+  if (op->geom == P3D_GEOM_AFFINE && (op->aff_exact || !(DA12 || DA21)))
+    return launch_affine<T, DA11, DA12, DA21>(op, u, p, yu, yp, st, overwrite, tzb, tze);
   TileArgs<T> a = tile_args<T>(op, NW_GEN);
   a.x = u; a.y = yu; a.p = p; a.yp = yp; a.kdat = reinterpret_cast<const T *>(op->kgen);
   a.kgq = reinterpret_cast<const T *>(op->kgq);
@@ -259,16 +269,23 @@ int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geo
     if (rc) return rc;
     mode = (hbad == 0 && nel > 0) ? P3D_GEOM_AFFINE : P3D_GEOM_GENERAL;
   }
+  // the affine A12 / A21 kernels need every element affine (a forced low-order
+  // A11 on a deformed mesh keeps the exact general ones)
+  op->aff_exact = geom_mode == P3D_GEOM_AUTO && mode == P3D_GEOM_AFFINE;
   if (mode == P3D_GEOM_AFFINE) {
     bricks(m, NW_AFF, ntx, nty, ntz);
     size_t na = (size_t)ntx * nty * ntz * Brick<NW_AFF>::NE;
-    if (!op->kaff && (rc = dev_alloc(&op->kaff, na * 36 * es, "affine geometry"))) return rc;
+    if (!op->kaff && (rc = dev_alloc(&op->kaff, na * KAFF * es, "affine geometry"))) return rc;
+    if (op->aff_exact && !op->kpre && (rc = dev_alloc(&op->kpre, na * KPRE * es, "affine pressure basis"))) return rc;
+    void *pre = op->aff_exact ? op->kpre : nullptr;
     if (op->prec == P3D_PREC_F64)
       pack_affine_kernel<double, NW_AFF><<<grid_for(na), 256, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz,
-                                                                      ntx, nty, ntz, coords, eta, (double *)op->kaff);
+                                                                      ntx, nty, ntz, coords, eta, (double *)op->kaff,
+                                                                      (double *)pre);
     else
       pack_affine_kernel<float, NW_AFF><<<grid_for(na), 256, 0, st>>>(m.mx, m.my, m.mz, m.gx, m.gy, m.ox, m.oy, m.oz,
-                                                                     ntx, nty, ntz, coords, eta, (float *)op->kaff);
+                                                                     ntx, nty, ntz, coords, eta, (float *)op->kaff,
+                                                                     (float *)pre);
     count_launch(1);
     if ((rc = cuda_check(cudaGetLastError(), "pack affine"))) return rc;
   }
@@ -358,6 +375,7 @@ int p3d_op_destroy(p3d_op *op)
   free_dev(op->kgen);
   free_dev(op->kgq);
   free_dev(op->kaff);
+  free_dev(op->kpre);
   free_dev(op->hx);
   free_dev(op->hy);
   if (op->flag) cudaFree(op->flag);

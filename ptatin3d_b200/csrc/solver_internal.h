@@ -16,7 +16,11 @@ template <typename T> void v_scale(size_t n, T a, T *y, cudaStream_t s);
 template <typename T> void v_jacobi(size_t n, const double *dinv, const T *r, T *z, cudaStream_t s);
 template <typename T> void v_cheb_init(size_t n, const double *dinv, const T *r, T inv_theta, T *d, cudaStream_t s);
 template <typename T>
-void v_cheb_step(size_t n, const double *dinv, T *x, T *r, const T *Ad, T *d, T c1, T c2, cudaStream_t s);
+void v_cheb_step(size_t n, const double *dinv, T *x, T *r, const T *Ad, T *d, T c1, T c2, bool last, cudaStream_t s);
+template <typename T>
+void v_cheb_init0(size_t n, const double *dinv, const T *b, T inv_theta, T *x, T *r, T *d, cudaStream_t s);
+template <typename T>
+void v_cheb_init_res(size_t n, const double *dinv, const T *b, const T *Ax, T inv_theta, T *r, T *d, cudaStream_t s);
 template <typename T> void v_residual(size_t n, const T *b, const T *Ax, T *r, cudaStream_t s);
 template <typename T> void v_mask(int nx, int ny, int nz, uint32_t dir, T *v, cudaStream_t s);
 template <typename T>
@@ -59,5 +63,10 @@ int dense_inverse_spd(int n, double *A, double *scratch, cudaStream_t s);
 // mg_transfer.cu
 template <typename T> int mg_prolong(int cnx, int cny, int cnz, int ndof, const T *xc, T *xf, cudaStream_t st);
 template <typename T> int mg_restrict(int cnx, int cny, int cnz, int ndof, const T *xf, T *xc, cudaStream_t st);
+// velocity V-cycle transfers with the Dirichlet mask dir fused in:
+// xc = mask(P^T mask(b - Ax)) and xf += mask(P xc)
+template <typename T>
+int mg_restrict_residual(int cnx, int cny, int cnz, uint32_t dir, const T *b, const T *Ax, T *xc, cudaStream_t st);
+template <typename T> int mg_prolong_add(int cnx, int cny, int cnz, uint32_t dir, const T *xc, T *xf, cudaStream_t st);
 
 } // namespace p3d

@@ -1,6 +1,6 @@
 // Element kernels built on the brick decomposition of q2_tile.cuh.
 //
-//   a11_affine_kernel      y += A11 x, per-element constant Jacobian
+//   stokes_affine_kernel   any of {A11, A12, A21}, per-element constant Jacobian
 //   stokes_general_kernel  any of {A11, A12, A21} with per-Gauss-point geometry
 //   diag_general_kernel    d += diag(A11)
 //   setup kernels          brick packing of eta, affinity test, affine packing
@@ -158,62 +158,153 @@ template <typename T, int i, int j, int k> struct QP {
   dcolT(j, ro1, r[(i) + 9 * (k)], r[(i) + 3 + 9 * (k)], r[(i) + 6 + 9 * (k)]);                                   \
   dcolT(k, ro2, r[(i) + 3 * (j)], r[(i) + 3 * (j) + 9], r[(i) + 3 * (j) + 18]);
 
-// ---------------------------------------------------------------- A11 affine
-template <typename T, int NW> struct AffineSmem {
+// A21 epilogue shared by the element kernels: lane f holds the moments
+// [t, t*hat_f, t*hat_{f+1}, t*hat_{f+2}] of its own terms t; the element's three
+// lanes sum them and lane 0 adds them to the element's 4 pressure rows in the
+// basis order [1, xh, yh, zh].
+template <typename T>
+__device__ __forceinline__ void a21_moments(const LaneMap &L, bool valid, int src1, int src2, T ap0, T ap1, T ap2, T ap3,
+                                            T *__restrict__ yp)
+{
+  const T s0 = ap0 + __shfl_sync(0xffffffffu, ap0, src1) + __shfl_sync(0xffffffffu, ap0, src2);
+  // component m of the basis: lane f stores it in slot 1 + (m - f) mod 3
+  T mom[3];
+#pragma unroll
+  for (int m = 0; m < 3; m++) {
+    const int sl0 = (m - L.f + 3) % 3;           // this lane's slot for basis m
+    const int sl1 = (m - (L.f + 1) % 3 + 3) % 3; // lane src1's slot
+    const int sl2 = (m - (L.f + 2) % 3 + 3) % 3; // lane src2's slot
+    const T v0 = sl0 == 0 ? ap1 : (sl0 == 1 ? ap2 : ap3);
+    const T w1 = __shfl_sync(0xffffffffu, ap1, src1), w2 = __shfl_sync(0xffffffffu, ap2, src1),
+            w3 = __shfl_sync(0xffffffffu, ap3, src1);
+    const T u1 = __shfl_sync(0xffffffffu, ap1, src2), u2 = __shfl_sync(0xffffffffu, ap2, src2),
+            u3 = __shfl_sync(0xffffffffu, ap3, src2);
+    mom[m] = v0 + (sl1 == 0 ? w1 : (sl1 == 1 ? w2 : w3)) + (sl2 == 0 ? u1 : (sl2 == 1 ? u2 : u3));
+  }
+  if (L.active && valid && L.f == 0) {
+    yp[0] += s0; yp[1] += mom[0]; yp[2] += mom[1]; yp[3] += mom[2];
+  }
+}
+
+// ------------------------------------------------------------ affine kernels
+// Per-element constant Jacobian.  kdat: [brick][slot][36] = J^{-1} (9) and
+// eta*w*detJ at the 27 Gauss points; kpre (A12/A21 only): [brick][slot][12] =
+// the pressure-basis map C[d][m] = M[d][m] / (2 M[m][m]) (9, M = dx/dxi) and
+// detJ, 2 pad.  On an affine element the basis coordinate
+//   hat_m(x(xi)) = (x_m(xi) - mean of the 27 nodes) / L_m = sum_d C[d][m] xi_d,
+// because the node mean is x(0) and the mid-face extent L_m is 2 M[m][m]
+// (src/element_utils_q2.c:183-224).
+constexpr int KAFF = 36, KPRE = 12;
+template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct AffineSmem {
   using BK = Brick<NW>;
-  static constexpr int KS = 36; // J^{-1} (9) + eta*w*detJ (27)
+  static constexpr bool NEEDX = DA11 || DA21;
+  static constexpr bool NEEDY = DA11 || DA12;
+  static constexpr bool PB = DA12 || DA21;
   static constexpr int OX = 0;
-  static constexpr int OY = OX + align16(3 * BK::NN, sizeof(T));
-  static constexpr int OK = OY + align16(3 * BK::NN, sizeof(T));
-  static constexpr int OA = OK + align16(BK::NE * KS, sizeof(T)); // node-tile accumulator
-  static constexpr int TOTAL = OA + 3 * BK::NN;
+  static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OK = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OP = OK + align16(BK::NE * KAFF, sizeof(T));
+  static constexpr int OA = OP + (PB ? align16(BK::NE * KPRE, sizeof(T)) : 0); // node-tile accumulator
+  static constexpr int TOTAL = OA + (NEEDY ? 3 * BK::NN : 0);
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
 };
 
-template <typename T, int NW>
-__global__ void __launch_bounds__(32 * NW, 4) a11_affine_kernel(TileArgs<T> A)
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW, (DA12 || DA21) ? (DA11 ? 2 : 3) : 4) stokes_affine_kernel(TileArgs<T> A)
 {
   using BK = Brick<NW>;
-  using SM = AffineSmem<T, NW>;
+  using SM = AffineSmem<T, NW, DA11, DA12, DA21>;
+  constexpr bool NEEDX = SM::NEEDX, NEEDY = SM::NEEDY, PB = SM::PB;
   extern __shared__ __align__(16) unsigned char p3d_smem[];
   T *sm = reinterpret_cast<T *>(p3d_smem);
-  T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_k = sm + SM::OK, *s_acc = sm + SM::OA;
+  T *s_x = sm + SM::OX, *s_y = sm + SM::OY, *s_k = sm + SM::OK, *s_p = sm + SM::OP, *s_acc = sm + SM::OA;
   const BrickPos b = brick_pos<T, NW>(A);
-  stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
-  stage_block(A.kdat + (size_t)(blockIdx.x + A.brick0) * BK::NE * SM::KS, s_k, BK::NE * SM::KS);
-  if (!A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
-  for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
+  const size_t brick = (size_t)blockIdx.x + A.brick0;
+  if (NEEDX) stage_nodes<T, NW>(A, b, A.x, s_x, A.bc != 0);
+  stage_block(A.kdat + brick * BK::NE * KAFF, s_k, BK::NE * KAFF);
+  if (PB) stage_block(A.kgq + brick * BK::NE * KPRE, s_p, BK::NE * KPRE);
+  if (NEEDY && !A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
+  if (NEEDY)
+    for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
   cp_async_wait_all();
   __syncthreads();
 
   const LaneMap L = lane_map();
   const bool valid = L.a < b.ax && L.b < b.ay && L.c < b.az;
   const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
-  const T *K = s_k + L.slot * SM::KS;
+  const T *K = s_k + L.slot * KAFF;
   T Jr[9];
   {
     const int r0 = 3 * L.f, r1 = 3 * ((L.f + 1) % 3), r2 = 3 * ((L.f + 2) % 3);
 #pragma unroll
     for (int d = 0; d < 3; d++) { Jr[d] = K[r0 + d]; Jr[3 + d] = K[r1 + d]; Jr[6 + d] = K[r2 + d]; }
   }
+  // pressure basis, rotated to the lane's direction: Cr[3d + t] = C[d][f + t]
+  T Cr[9], detJ = 0, pr0 = 0, pr1 = 0, pr2 = 0, pr3 = 0;
+  size_t eg = 0;
+  if (PB) {
+    const T *P = s_p + L.slot * KPRE;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+      for (int t = 0; t < 3; t++) Cr[3 * d + t] = P[3 * d + (L.f + t) % 3];
+    detJ = P[9];
+    eg = (size_t)(b.e0x + L.a) + (size_t)A.mx * ((size_t)(b.e0y + L.b) + (size_t)A.my * (b.e0z + L.c));
+    if (DA12 && valid) {
+      const T p0 = A.p[4 * eg], p1 = A.p[4 * eg + 1], p2 = A.p[4 * eg + 2], p3 = A.p[4 * eg + 3];
+      pr0 = p0;
+      pr1 = L.f == 0 ? p1 : (L.f == 1 ? p2 : p3);
+      pr2 = L.f == 0 ? p2 : (L.f == 1 ? p3 : p1);
+      pr3 = L.f == 0 ? p3 : (L.f == 1 ? p1 : p2);
+    }
+  }
   T uq[27], r[27];
-  load_interp<T, NW>(s_x, L, uq);
+  if (NEEDX) load_interp<T, NW>(s_x, L, uq);
 #pragma unroll
   for (int n = 0; n < 27; n++) r[n] = (T)0;
+  T ap0 = 0, ap1 = 0, ap2 = 0, ap3 = 0;
 #pragma unroll
   for (int k = 0; k < 3; k++)
 #pragma unroll
     for (int j = 0; j < 3; j++)
 #pragma unroll
       for (int i = 0; i < 3; i++) {
-        P3D_GRAD(uq, i, j, k, g0, g1, g2)
-        T D0, ro0, ro1, ro2;
-        qp_action(Jr, K[9 + i + 3 * j + 9 * k], g0, g1, g2, src1, src2, D0, ro0, ro1, ro2);
-        P3D_SCATTER(r, i, j, k, ro0, ro1, ro2)
+        T D0 = 0, ro0 = 0, ro1 = 0, ro2 = 0;
+        if (NEEDX) {
+          P3D_GRAD(uq, i, j, k, g0, g1, g2)
+          if (DA11) {
+            qp_action(Jr, K[9 + i + 3 * j + 9 * k], g0, g1, g2, src1, src2, D0, ro0, ro1, ro2);
+          } else {
+            D0 = Jr[0] * g0 + Jr[1] * g1 + Jr[2] * g2;
+          }
+        }
+        if (PB) {
+          // Gauss coordinates -s, 0, s; hats h0 = hat_f, h1 = hat_{f+1}, h2 = hat_{f+2}
+          const T xi = cst<T>(i == 0 ? -0.77459666924148337704 : (i == 1 ? 0.0 : 0.77459666924148337704));
+          const T xj = cst<T>(j == 0 ? -0.77459666924148337704 : (j == 1 ? 0.0 : 0.77459666924148337704));
+          const T xk = cst<T>(k == 0 ? -0.77459666924148337704 : (k == 1 ? 0.0 : 0.77459666924148337704));
+          const T h0 = Cr[0] * xi + Cr[3] * xj + Cr[6] * xk;
+          const T h1 = Cr[1] * xi + Cr[4] * xj + Cr[7] * xk;
+          const T h2 = Cr[2] * xi + Cr[5] * xj + Cr[8] * xk;
+          const T wdet = cst<T>(w1d(i) * w1d(j) * w1d(k)) * detJ;
+          if (DA12) {
+            // -w detJ p_q grad(N) . e_f = -w detJ p_q (row f of J^{-1}) . grad_xi(N)
+            const T t = valid ? -wdet * (pr0 + pr1 * h0 + pr2 * h1 + pr3 * h2) : (T)0;
+            ro0 += t * Jr[0]; ro1 += t * Jr[1]; ro2 += t * Jr[2];
+          }
+          if (DA21) {
+            const T t = valid ? -wdet * D0 : (T)0; // -w detJ Np du_f/dx_f
+            ap0 += t; ap1 += t * h0; ap2 += t * h1; ap3 += t * h2;
+          }
+        }
+        if (NEEDY) { P3D_SCATTER(r, i, j, k, ro0, ro1, ro2) }
       }
-  interp27T(r);
-  accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
-  write_tile<T, NW>(A, b, s_acc, s_y, 0);
+  if (DA21) a21_moments(L, valid, src1, src2, ap0, ap1, ap2, ap3, A.yp + 4 * eg);
+  if (NEEDY) {
+    interp27T(r);
+    accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
+    write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
+  }
 }
 
 // Gauss-point coordinate table (general path), packed at setup, GQC values per
@@ -359,28 +450,7 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
         if (NEEDY) { P3D_SCATTER(r, i, j, k, ro0, ro1, ro2) }
       }
   }
-  if (DA21) {
-    // moments of the three lanes, back to the basis order [1, xh, yh, zh]:
-    // lane f holds [t, t*hat_f, t*hat_{f+1}, t*hat_{f+2}] summed over its own t
-    const T s0 = ap0 + __shfl_sync(0xffffffffu, ap0, src1) + __shfl_sync(0xffffffffu, ap0, src2);
-    // component m of the basis: lane f stores it in slot 1 + (m - f) mod 3
-    T mom[3];
-#pragma unroll
-    for (int m = 0; m < 3; m++) {
-      const int sl0 = (m - L.f + 3) % 3;                 // this lane's slot for basis m
-      const int sl1 = (m - (L.f + 1) % 3 + 3) % 3;       // lane src1's slot
-      const int sl2 = (m - (L.f + 2) % 3 + 3) % 3;       // lane src2's slot
-      const T v0 = sl0 == 0 ? ap1 : (sl0 == 1 ? ap2 : ap3);
-      const T w1 = __shfl_sync(0xffffffffu, ap1, src1), w2 = __shfl_sync(0xffffffffu, ap2, src1),
-              w3 = __shfl_sync(0xffffffffu, ap3, src1);
-      const T u1 = __shfl_sync(0xffffffffu, ap1, src2), u2 = __shfl_sync(0xffffffffu, ap2, src2),
-              u3 = __shfl_sync(0xffffffffu, ap3, src2);
-      mom[m] = v0 + (sl1 == 0 ? w1 : (sl1 == 1 ? w2 : w3)) + (sl2 == 0 ? u1 : (sl2 == 1 ? u2 : u3));
-    }
-    if (L.active && valid && L.f == 0) {
-      A.yp[4 * eg] += s0; A.yp[4 * eg + 1] += mom[0]; A.yp[4 * eg + 2] += mom[1]; A.yp[4 * eg + 3] += mom[2];
-    }
-  }
+  if (DA21) a21_moments(L, valid, src1, src2, ap0, ap1, ap2, ap3, A.yp + 4 * eg);
   if (NEEDY) {
     interp27T(r);
     __syncthreads(); // every warp is done with the Gauss-point coordinates: reuse as the accumulator
@@ -705,11 +775,12 @@ __global__ void affine_check_kernel(int mx, int my, int mz, int gx, int gy, int 
   }
 }
 
-// per element J^{-1} and eta*w*detJ (affine elements), brick-ordered [brick][slot][36]
+// per element J^{-1} and eta*w*detJ (affine elements), brick-ordered [brick][slot][KAFF];
+// pre (optional): the pressure-basis map and detJ, [brick][slot][KPRE]
 template <typename T, int NW>
 __global__ void pack_affine_kernel(int mx, int my, int mz, int gx, int gy, int ox, int oy, int oz, int ntx, int nty,
                                    int ntz, const double *__restrict__ coords, const double *__restrict__ eta,
-                                   T *__restrict__ out)
+                                   T *__restrict__ out, T *__restrict__ pre)
 {
   using BK = Brick<NW>;
   size_t total = (size_t)ntx * nty * ntz * BK::NE;
@@ -719,9 +790,11 @@ __global__ void pack_affine_kernel(int mx, int my, int mz, int gx, int gy, int o
     int tx = t % ntx, ty = (t / ntx) % nty, tz = t / ((size_t)ntx * nty);
     int a = slot % TX, bb = (slot / TX) % TY, c = slot / (TX * TY);
     int ex = tx * TX + a, ey = ty * TY + bb, ez = tz * NW + c;
-    T *o = out + idx * 36;
+    T *o = out + idx * KAFF;
     if (!(ex < mx && ey < my && ez < mz)) {
-      for (int r = 0; r < 36; r++) o[r] = (T)0;
+      for (int r = 0; r < KAFF; r++) o[r] = (T)0;
+      if (pre)
+        for (int r = 0; r < KPRE; r++) pre[idx * KPRE + r] = (T)0;
       continue;
     }
     auto X = [&](int a2, int b2, int c2, int d) {
@@ -736,6 +809,12 @@ __global__ void pack_affine_kernel(int mx, int my, int mz, int gx, int gy, int o
     }
     double det = inv3<double>(M, Mi);
     for (int r = 0; r < 9; r++) o[r] = (T)Mi[r];
+    if (pre) {
+      T *pp = pre + idx * KPRE;
+      for (int d = 0; d < 3; d++)
+        for (int mm = 0; mm < 3; mm++) pp[3 * d + mm] = (T)(M[3 * d + mm] / (2.0 * M[3 * mm + mm]));
+      pp[9] = (T)det; pp[10] = (T)0; pp[11] = (T)0;
+    }
     size_t e = (size_t)ex + (size_t)mx * ((size_t)ey + (size_t)my * ez);
     for (int q = 0; q < 27; q++) {
       int qi = q % 3, qj = (q / 3) % 3, qk = q / 9;

@@ -112,33 +112,33 @@ template <typename T> static int smooth(p3d_solver *s, Level &L, const T *b, T *
   const double lo = s->o.cheb_lo * L.lmax, hi = s->o.cheb_hi * L.lmax;
   const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
   if (zero_guess) {
-    CU(cudaMemsetAsync(x, 0, n * sizeof(T), s->st), "memset");
-    CU(cudaMemcpyAsync(r, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s->st), "copy");
+    v_cheb_init0<T>(n, L.dinv, b, (T)(1.0 / theta), x, r, d, s->st); // x = 0, r = b
   } else {
     CK(a11<T>(s, L, x, t));
-    v_residual<T>(n, b, t, r, s->st);
+    v_cheb_init_res<T>(n, L.dinv, b, t, (T)(1.0 / theta), r, d, s->st); // r = b - A x
   }
-  v_cheb_init<T>(n, L.dinv, r, (T)(1.0 / theta), d, s->st);
   double rho = 1.0 / sigma;
   const int K = std::max(1, s->o.cheb_its);
-  for (int k = 0; k < K; k++) {
-    if (k == K - 1) {
-      v_axpby<T>(n, (T)1, d, (T)1, x, s->st); // x += d
-      break;
-    }
+  if (K == 1) {
+    v_axpby<T>(n, (T)1, d, (T)1, x, s->st); // x += d
+    return P3D_OK;
+  }
+  for (int k = 0; k < K - 1; k++) {
     CK(a11<T>(s, L, d, t));
     double rho_new = 1.0 / (2.0 * sigma - rho);
-    v_cheb_step<T>(n, L.dinv, x, r, t, d, (T)(rho_new * rho), (T)(2.0 * rho_new / delta), s->st);
+    // the last step also adds the final direction to x
+    v_cheb_step<T>(n, L.dinv, x, r, t, d, (T)(rho_new * rho), (T)(2.0 * rho_new / delta), k == K - 2, s->st);
     rho = rho_new;
   }
   return P3D_OK;
 }
 
-// coarse solve: x = Ac^{-1} b (FP64 dense inverse)
-template <typename T> static int coarse_solve(p3d_solver *s, const T *b, T *x)
+// coarse solve: x = Ac^{-1} b (FP64 dense inverse); mask: b may hold values on
+// Dirichlet dofs (a one-level hierarchy), zero them first
+template <typename T> static int coarse_solve(p3d_solver *s, const T *b, T *x, bool mask)
 {
   Level &L = s->lv[0];
-  v_mask<T>(L.n[0], L.n[1], L.n[2], level_dir(s), const_cast<T *>(b), s->st);
+  if (mask) v_mask<T>(L.n[0], L.n[1], L.n[2], level_dir(s), const_cast<T *>(b), s->st);
   if (sizeof(T) == 8) {
     v_dense_mv(s->nc, s->cinv, (const double *)b, (double *)x, s->st);
   } else {
@@ -152,20 +152,16 @@ template <typename T> static int coarse_solve(p3d_solver *s, const T *b, T *x)
 // V-cycle on level l: x = MG(b), x overwritten
 template <typename T> static int vcycle(p3d_solver *s, int l, const T *b, T *x)
 {
-  if (l == 0) return coarse_solve<T>(s, b, x);
+  // the coarse right-hand side comes masked from the restriction
+  if (l == 0) return coarse_solve<T>(s, b, x, (int)s->lv.size() == 1);
   Level &L = s->lv[l], &C = s->lv[l - 1];
   const uint32_t dir = level_dir(s);
   CK(smooth<T>(s, L, b, x, true));
-  T *t = (T *)L.t, *r = (T *)L.r;
+  T *t = (T *)L.t;
   CK(a11<T>(s, L, x, t));
-  v_residual<T>(L.nv, b, t, r, s->st);
-  v_mask<T>(L.n[0], L.n[1], L.n[2], dir, r, s->st);
-  CK(mg_restrict<T>(C.n[0], C.n[1], C.n[2], 3, r, (T *)C.b, s->st));
-  v_mask<T>(C.n[0], C.n[1], C.n[2], dir, (T *)C.b, s->st);
+  CK(mg_restrict_residual<T>(C.n[0], C.n[1], C.n[2], dir, b, t, (T *)C.b, s->st)); // C.b = mask(P^T mask(b - A x))
   CK(vcycle<T>(s, l - 1, (const T *)C.b, (T *)C.x));
-  CK(mg_prolong<T>(C.n[0], C.n[1], C.n[2], 3, (const T *)C.x, t, s->st));
-  v_mask<T>(L.n[0], L.n[1], L.n[2], dir, t, s->st);
-  v_axpby<T>(L.nv, (T)1, t, (T)1, x, s->st);
+  CK(mg_prolong_add<T>(C.n[0], C.n[1], C.n[2], dir, (const T *)C.x, x, s->st)); // x += mask(P C.x)
   CK(smooth<T>(s, L, b, x, false));
   return P3D_OK;
 }

@@ -45,18 +45,49 @@ __global__ void k_cheb_init(size_t n, const double *__restrict__ dinv, const T *
 {
   GS_LOOP(i, n) d[i] = (T)(dinv[i] * (double)r[i]) * inv_theta;
 }
-// x += d ; r -= Ad ; d = c1 d + c2 dinv .* r   (one pass for the Chebyshev recurrence)
+// Chebyshev start from x = 0: x = 0, r = b, d = dinv .* b / theta (one pass)
+template <typename T>
+__global__ void k_cheb_init0(size_t n, const double *__restrict__ dinv, const T *__restrict__ b, T inv_theta,
+                             T *__restrict__ x, T *__restrict__ r, T *__restrict__ d)
+{
+  GS_LOOP(i, n)
+  {
+    const T bi = b[i];
+    x[i] = (T)0;
+    r[i] = bi;
+    d[i] = (T)(dinv[i] * (double)bi) * inv_theta;
+  }
+}
+// Chebyshev start from x: r = b - Ax, d = dinv .* r / theta (one pass)
+template <typename T>
+__global__ void k_cheb_init_res(size_t n, const double *__restrict__ dinv, const T *__restrict__ b, const T *__restrict__ Ax,
+                                T inv_theta, T *__restrict__ r, T *__restrict__ d)
+{
+  GS_LOOP(i, n)
+  {
+    const T ri = b[i] - Ax[i];
+    r[i] = ri;
+    d[i] = (T)(dinv[i] * (double)ri) * inv_theta;
+  }
+}
+// x += d ; r -= Ad ; d = c1 d + c2 dinv .* r   (one pass for the Chebyshev recurrence);
+// last: the recurrence ends here, so the new d is added to x as well
 template <typename T>
 __global__ void k_cheb_step(size_t n, const double *__restrict__ dinv, T *__restrict__ x, T *__restrict__ r,
-                            const T *__restrict__ Ad, T *__restrict__ d, T c1, T c2)
+                            const T *__restrict__ Ad, T *__restrict__ d, T c1, T c2, int last)
 {
   GS_LOOP(i, n)
   {
     T di = d[i];
-    x[i] += di;
     T ri = r[i] - Ad[i];
-    r[i] = ri;
-    d[i] = c1 * di + c2 * (T)(dinv[i] * (double)ri);
+    T dn = c1 * di + c2 * (T)(dinv[i] * (double)ri);
+    if (last) {
+      x[i] += di + dn;
+    } else {
+      x[i] += di;
+      r[i] = ri;
+      d[i] = dn;
+    }
   }
 }
 // r = b - Ax
@@ -231,9 +262,21 @@ template <typename T> void v_cheb_init(size_t n, const double *dinv, const T *r,
   count_launch(1);
 }
 template <typename T>
-void v_cheb_step(size_t n, const double *dinv, T *x, T *r, const T *Ad, T *d, T c1, T c2, cudaStream_t s)
+void v_cheb_init0(size_t n, const double *dinv, const T *b, T inv_theta, T *x, T *r, T *d, cudaStream_t s)
 {
-  k_cheb_step<<<vgrid(n), 256, 0, s>>>(n, dinv, x, r, Ad, d, c1, c2);
+  k_cheb_init0<<<vgrid(n), 256, 0, s>>>(n, dinv, b, inv_theta, x, r, d);
+  count_launch(1);
+}
+template <typename T>
+void v_cheb_init_res(size_t n, const double *dinv, const T *b, const T *Ax, T inv_theta, T *r, T *d, cudaStream_t s)
+{
+  k_cheb_init_res<<<vgrid(n), 256, 0, s>>>(n, dinv, b, Ax, inv_theta, r, d);
+  count_launch(1);
+}
+template <typename T>
+void v_cheb_step(size_t n, const double *dinv, T *x, T *r, const T *Ad, T *d, T c1, T c2, bool last, cudaStream_t s)
+{
+  k_cheb_step<<<vgrid(n), 256, 0, s>>>(n, dinv, x, r, Ad, d, c1, c2, last ? 1 : 0);
   count_launch(1);
 }
 template <typename T> void v_residual(size_t n, const T *b, const T *Ax, T *r, cudaStream_t s)
@@ -326,7 +369,9 @@ template void v_convert<float, double>(size_t, const float *, double *, cudaStre
   template void v_scale<T>(size_t, T, T *, cudaStream_t);                                                              \
   template void v_jacobi<T>(size_t, const double *, const T *, T *, cudaStream_t);                                     \
   template void v_cheb_init<T>(size_t, const double *, const T *, T, T *, cudaStream_t);                               \
-  template void v_cheb_step<T>(size_t, const double *, T *, T *, const T *, T *, T, T, cudaStream_t);                  \
+  template void v_cheb_step<T>(size_t, const double *, T *, T *, const T *, T *, T, T, bool, cudaStream_t);            \
+  template void v_cheb_init0<T>(size_t, const double *, const T *, T, T *, T *, T *, cudaStream_t);                   \
+  template void v_cheb_init_res<T>(size_t, const double *, const T *, const T *, T, T *, T *, cudaStream_t);          \
   template void v_residual<T>(size_t, const T *, const T *, T *, cudaStream_t);                                        \
   template void v_mask<T>(int, int, int, uint32_t, T *, cudaStream_t);                                                 \
   template void v_mdot<T>(size_t, int, const T *const *, const T *, double *, double *, cudaStream_t);                 \

@@ -116,11 +116,20 @@ def test_reference_expected_on_gpu(cuda, name):
             assert abs(val - gold) <= 5e-9 * abs(gold), (k, val, gold)
 
 
-@pytest.mark.parametrize("deform", [0.0, 0.15])
-def test_diagonal_a12_a21_fused(cuda, restatement, deform):
+SHEAR = np.array([[1.0, 0.3, 0.1], [0.2, 1.2, -0.15], [0.05, 0.25, 0.9]])
+
+
+@pytest.mark.parametrize("deform,shear", [(0.0, False), (0.0, True), (0.15, False)])
+def test_diagonal_a12_a21_fused(cuda, restatement, deform, shear):
+    """diag(A11), A12, A21 and the fused operator against the oracle: on the
+    uniform and the sheared (affine, off-diagonal Jacobian) mesh through the
+    per-element-Jacobian kernels, on the perturbed mesh through the general ones."""
     case = sinker_case(6, deform=deform, seed=4)
+    if shear:
+        case["coords"] = (case["coords"].reshape(-1, 3) @ SHEAR.T + 0.5).reshape(-1)
     d, c, e, mask = case["dims"], case["coords"], case["eta"].reshape(-1), case["mask"]
     op = make_op(case)
+    assert op.geometry_mode == (GEOM_GENERAL if deform else GEOM_AFFINE)
     nv, npr = op.n_velocity, op.n_pressure
     x, p = T(case["x"]), T(case["p"])
     dg = torch.empty(nv, dtype=torch.float64, device="cuda")
@@ -199,6 +208,27 @@ def test_fp32_operator(cuda, deform):
     y32 = torch.empty(case["x"].size, dtype=torch.float32, device="cuda")
     op32.mult(T(case["x"], torch.float32), y32)
     assert rel(host(y32), host(y64)) <= TOL32
+
+
+@pytest.mark.parametrize("deform", [0.0, 0.2])
+def test_fp32_pressure_coupling(cuda, deform):
+    """FP32 A12, A21 and the fused operator against FP64 (affine and general kernels)."""
+    case = sinker_case(12, deform=deform, eta1=1e2)
+    op64, op32 = make_op(case), make_op(case, prec=PREC_F32)
+    x64, p64 = T(case["x"]), T(case["p"])
+    x32, p32 = T(case["x"], torch.float32), T(case["p"], torch.float32)
+    nv, npr = op64.n_velocity, op64.n_pressure
+    out = {}
+    for name, op, x, p, dt in (("64", op64, x64, p64, torch.float64), ("32", op32, x32, p32, torch.float32)):
+        yu = torch.empty(nv, dtype=dt, device="cuda")
+        yp = torch.empty(npr, dtype=dt, device="cuda")
+        op.mult_a12(p, yu)
+        op.mult_a21(x, yp)
+        fu, fp = torch.empty_like(yu), torch.empty_like(yp)
+        op.mult_stokes(x, p, fu, fp)
+        out[name] = [host(v) for v in (yu, yp, fu, fp)]
+    for a, b in zip(out["32"], out["64"]):
+        assert rel(a, b) <= TOL32
 
 
 def test_host_apply_matches_device(cuda):
