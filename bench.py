@@ -177,14 +177,54 @@ def cpu_reference_apply(wl, steps, warmup, threads=None):
     return dt, n
 
 
+def cpu_slab_apply(wl, steps, warmup):
+    """Time the reference's A11 kernel on z-slabs, one process (one thread) per
+    host core, the way the reference runs one MPI rank per core."""
+    from oracle.cpu_slabs import slab_apply_time
+    from oracle.oracle import Reference, build
+    if not Reference.available():
+        build()
+    n = os.cpu_count()
+    return slab_apply_time(wl["coords"], wl["eta"], wl["x"], wl["m"], n, steps=steps, warmup=warmup), n
+
+
+def cpu_best_apply(wl, steps, warmup):
+    """The faster of the two ways the reference runs on a host (a short probe
+    of each decides), timed over `steps` applies; returns (s, cores, config)."""
+    t_omp, n = cpu_reference_apply(wl, 2, 1)
+    try:
+        t_slab, _ = cpu_slab_apply(wl, 2, 1)
+    except Exception:
+        t_slab = float("inf")
+    if t_slab < t_omp:
+        dt, n = cpu_slab_apply(wl, steps, warmup)
+        return dt, n, f"{n} processes x 1 thread on z-slabs (MPI-rank layout)"
+    dt, n = cpu_reference_apply(wl, steps, warmup)
+    return dt, n, f"OpenMP {n} threads"
+
+
 SOLVE_WORKLOAD = ("Stokes solve, Q2-P1disc 32^3 unit cube, 8 sinkers r=0.1 (eta contrast 1e4, density +1%), "
                   "g=-z, free slip walls/base, free surface top; FGMRES(30) + Schur upper (geometric-mean "
                   "viscosity-scaled mass matrix) + 4-level Galerkin GMG, Chebyshev(3)/Jacobi, rtol 1e-6")
 
 
-def solve_leg(device, m=32, seed=1):
+def cpu_solve_sample(m, c, eta, rho, bits, iterations=10):
+    """The solver restated on the host cores (oracle/cpu_solver.py: the same
+    FGMRES + Schur-upper + Galerkin GMG, with the reference's own AVX operator
+    kernels on the fine level), timed over a bounded number of iterations."""
+    from oracle.cpu_solver import CpuStokesSolver
+    from oracle.oracle import Reference, build
+    if not Reference.available():
+        build()
+    S = CpuStokesSolver(m, c, eta, rho, bits, nlevels=4, threads=os.cpu_count())
+    _, _, its, _, dt = S.solve(rtol=1e-6, max_it=iterations)
+    return S.setup_s, dt / max(1, its), its
+
+
+def solve_leg(device, m=32, seed=1, cpu=True):
     """FP64 vs mixed-precision device-resident Stokes solve, each checked
-    against an FP64 solve converged to rtol 1e-10."""
+    against an FP64 solve converged to rtol 1e-10; the CPU restatement of the
+    same solve timed on a bounded sample of iterations."""
     import torch
 
     from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
@@ -218,11 +258,24 @@ def solve_leg(device, m=32, seed=1):
         out[name]["u_err"] = float(np.linalg.norm(u - ur) / np.linalg.norm(ur))
         out[name]["p_err"] = float(np.linalg.norm(p - pr) / np.linalg.norm(pr))
     (u64, p64), (u32, p32) = sols["fp64"], sols["mixed"]
+    cpu_solve = None
+    if cpu:
+        try:
+            setup_s, s_it, its = cpu_solve_sample(m, c, eta, rho, bits)
+            est = setup_s + s_it * out["fp64"]["iterations"]
+            cpu_solve = {"kind": "port", "cores": os.cpu_count(), "setup_s": setup_s, "s_per_iteration": s_it,
+                         "iterations_sampled": its, "est_solve_s": est,
+                         "est_speedup_gpu_fp64": est / (out["fp64"]["s"] + out["fp64"]["setup_s"]),
+                         "sample": f"setup plus {its} FGMRES iterations of the solver restated on the host "
+                                   "(oracle/cpu_solver.py; fine-level operators are the reference's AVX kernels, "
+                                   "OpenMP), extrapolated to the FP64 GPU solve's iteration count"}
+        except Exception as exc:  # reported, not required
+            cpu_solve = {"kind": "port", "sample": f"failed: {exc}"}
     return {"workload": SOLVE_WORKLOAD, "unit": "s", "fp64_s": out["fp64"]["s"], "mixed_s": out["mixed"]["s"],
             "speedup_mixed_vs_fp64": out["fp64"]["s"] / out["mixed"]["s"], "fp64": out["fp64"], "mixed": out["mixed"],
             "u_diff_mixed_vs_fp64": float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64)),
             "p_diff_mixed_vs_fp64": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64)),
-            "oracle_solve": out["ref"]}
+            "oracle_solve": out["ref"], "cpu_solve": cpu_solve}
 
 
 SERVE_SIZES = (8, 12, 16, 24, 32, 48)
@@ -316,7 +369,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     wl = workload()
-    dt, n = cpu_reference_apply(wl, args.steps, args.warmup)
+    dt, n, how = cpu_best_apply(wl, args.steps, args.warmup)
     ndof = wl["x"].size
     v = ndof / dt / 1e9
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
@@ -325,7 +378,7 @@ def run_reference(args):
             "config": {"workload": "A11 MatMult, Q2 96^3 deformed mesh, log-normal eta", "elements": wl["m"] ** 3,
                        "dofs": ndof},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": n, "kind": "reference",
-                             "sample": f"{args.steps} full applies of MFStokesWrapper_A11_AVX (OpenMP {n} threads)"},
+                             "sample": f"{args.steps} full applies of MFStokesWrapper_A11_AVX ({how})"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -444,16 +497,26 @@ def run_b200(args):
             sub = dict(wl)
             dt, n = cpu_reference_apply(sub, steps=20, warmup=2)
             dt1, _ = cpu_reference_apply(sub, steps=1, warmup=0, threads=1)
-            cpu = {"value": ndof / dt / 1e9, "unit": UNIT, "cores": n, "kind": "reference",
-                   "sample": f"20 full {m}^3 applies of the reference MFStokesWrapper_A11_AVX (oracle/_ref), OpenMP "
-                             f"{n} threads, after 2 warm-up applies",
+            try:
+                dts, _ = cpu_slab_apply(sub, steps=20, warmup=2)
+            except Exception:
+                dts = float("inf")
+            best = min(dt, dts)
+            cpu = {"value": ndof / best / 1e9, "unit": UNIT, "cores": n, "kind": "reference",
+                   "sample": f"best of two layouts of the reference MFStokesWrapper_A11_AVX (oracle/_ref), 20 full "
+                             f"{m}^3 applies each after 2 warm-up applies: "
+                             + ("z-slabs, one process per core" if dts < dt else f"OpenMP {n} threads"),
+                   "openmp": {"value": ndof / dt / 1e9, "unit": UNIT, "threads": n},
+                   "slabs": {"value": ndof / dts / 1e9 if dts < float("inf") else None, "unit": UNIT, "processes": n,
+                             "sample": "one z-slab per process, 1 thread each, started at a barrier; time of the "
+                                       "slowest slab; the shared-plane sums are not timed"},
                    "single_thread": {"value": ndof / dt1 / 1e9, "unit": UNIT, "sample": f"1 full {m}^3 apply, 1 thread"}}
         except Exception as exc:  # the baseline is reported, not required
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {exc}"}
 
     solve = None
     if rank == 0 and not args.no_solve:
-        solve = solve_leg(local)
+        solve = solve_leg(local, cpu=not args.no_cpu)
     serving = None
     if rank == 0 and args.serve_requests > 0:
         serving = serve_leg(local, args.serve_requests)

@@ -137,6 +137,8 @@ class Reference:
         L.ref_diag.argtypes = [_dp]
         L.ref_a12.argtypes = [_dp, _dp]
         L.ref_a21.argtypes = [_dp, _dp]
+        L.ref_a12_avx.argtypes = [_dp, _dp]
+        L.ref_a_avx.argtypes = [_dp] * 4
         L.ref_set_threads.argtypes = [C.c_int]
         self.L = L
         self.dims = None
@@ -175,6 +177,19 @@ class Reference:
         y = np.zeros(4 * self.dims[0] * self.dims[1] * self.dims[2])
         assert self.L.ref_a21(_p(np.ascontiguousarray(u, dtype=np.float64)), _p(y)) == 0
         return y
+
+    def a12_avx_raw(self, p):
+        y = np.zeros(self._coords.size)
+        assert self.L.ref_a12_avx(_p(np.ascontiguousarray(p, dtype=np.float64)), _p(y)) == 0
+        return y
+
+    def stokes_avx_raw(self, u, p):
+        """MFStokesWrapper_A_AVX: [A11 u + A12 p; A21 u] without boundary conditions."""
+        yu = np.zeros(self._coords.size)
+        yp = np.zeros(4 * self.dims[0] * self.dims[1] * self.dims[2])
+        assert self.L.ref_a_avx(_p(np.ascontiguousarray(u, dtype=np.float64)), _p(np.ascontiguousarray(p, dtype=np.float64)),
+                                _p(yu), _p(yp)) == 0
+        return yu, yp
 
 
 # --------------------------------------------------- MatMult conventions ---

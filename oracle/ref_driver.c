@@ -8,7 +8,8 @@
  *
  *   ref_setup(mx,my,mz, coords[3*nn], eta[27*nel])
  *   ref_a11(variant, x[3*nn], y[3*nn])   variant 0=tensor 1=avx 2=ref 3=low-order (MFStokesWrapper_A11PC)
- *   ref_diag(y[3*nn]), ref_a12(p[4*nel], yu[3*nn]), ref_a21(u[3*nn], yp[4*nel])
+ *   ref_diag(y[3*nn]), ref_a12(p[4*nel], yu[3*nn]), ref_a21(u[3*nn], yp[4*nel]),
+ *   ref_a12_avx(p, yu), ref_a_avx(u, p, yu, yp)
  *
  * Each adds element contributions exactly as the reference's SpMVOp_MatMult
  * callback does (the caller zeroes y and applies Dirichlet rows/columns).
@@ -34,6 +35,8 @@ PetscErrorCode MFStokesWrapper_A11PC(Quadrature, DM, PetscScalar[], PetscScalar[
 PetscErrorCode MFStokesWrapper_diagA11(Quadrature, DM, PetscScalar[]);
 PetscErrorCode MFStokesWrapper_A12(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
 PetscErrorCode MFStokesWrapper_A21(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
+PetscErrorCode MFStokesWrapper_A12_AVX(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
+PetscErrorCode MFStokesWrapper_A_AVX(Quadrature, DM, PetscScalar[], DM, PetscScalar[], PetscScalar[], PetscScalar[]);
 
 struct _p_shim_Vec {
   PetscScalar *a;
@@ -239,5 +242,9 @@ int ref_a11(int variant, double *x, double *y)
 int ref_diag(double *y) { return MFStokesWrapper_diagA11(&g_Q, &g_dau, y); }
 int ref_a12(double *p, double *yu) { return MFStokesWrapper_A12(&g_Q, &g_dau, &g_dap, p, yu); }
 int ref_a21(double *u, double *yp) { return MFStokesWrapper_A21(&g_Q, &g_dau, &g_dap, u, yp); }
+/* the AVX back end's A12 and fused [A11 A12; A21 0] (what MatMult_MFStokes_A12 and
+ * MatMult_MFStokes_A call when __AVX__ is defined, src/stokes_operators.c:927,1323) */
+int ref_a12_avx(double *p, double *yu) { return MFStokesWrapper_A12_AVX(&g_Q, &g_dau, &g_dap, p, yu); }
+int ref_a_avx(double *u, double *p, double *yu, double *yp) { return MFStokesWrapper_A_AVX(&g_Q, &g_dau, u, &g_dap, p, yu, yp); }
 int ref_set_threads(int n) { omp_set_num_threads(n); return 0; }
 int ref_max_threads(void) { return omp_get_max_threads(); }
