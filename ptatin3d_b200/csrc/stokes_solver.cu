@@ -758,7 +758,9 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
   if (!rc) rc = dev_alloc((void **)&s->xsol, N * 8, "solution");
   s->hs = m + 1;
   if (!rc) rc = dev_alloc((void **)&s->Vptr, (size_t)(m + 2) * sizeof(double *), "V ptrs");
-  if (!rc) rc = dev_alloc((void **)&s->part, (size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK * 8, "partials");
+  // partials of the multi-dot kernels, then their ticket counter (zero between launches)
+  if (!rc) rc = dev_alloc((void **)&s->part, ((size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK + 2) * 8, "partials");
+  if (!rc) rc = cuda_check(cudaMemset(s->part, 0, ((size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK + 2) * 8), "partials");
   if (!rc) rc = dev_alloc((void **)&s->hdev, (size_t)(2 * s->hs + 2) * 8, "h");
   if (!rc) rc = cuda_check(cudaMallocHost((void **)&s->hhost, (size_t)(2 * s->hs + 2) * 8), "pinned h");
   if (!rc) {

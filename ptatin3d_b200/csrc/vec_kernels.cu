@@ -114,9 +114,11 @@ __global__ void k_mask(int nx, int ny, int nz, uint32_t dir, T *__restrict__ v)
 // partial dot products  part[blk*KC + j] = sum_i V_j[i] w[i]   (FP64 accumulation),
 // KC vectors per launch so that the accumulators stay in registers
 template <typename T, int KC>
-__global__ void k_mdot_partial(size_t n, const T *const *__restrict__ V, const T *__restrict__ w, double *__restrict__ part)
+__global__ void k_mdot_partial(size_t n, const T *const *__restrict__ V, const T *__restrict__ w, double *__restrict__ part,
+                               unsigned int *__restrict__ ticket, double *__restrict__ out)
 {
   __shared__ double red[32][KC];
+  __shared__ bool last;
   const T *v[KC];
   double acc[KC];
 #pragma unroll
@@ -143,15 +145,21 @@ __global__ void k_mdot_partial(size_t n, const T *const *__restrict__ V, const T
     for (int q = 0; q < nw; q++) x += red[q][threadIdx.x];
     part[(size_t)blockIdx.x * KC + threadIdx.x] = x;
   }
-}
-__global__ void k_sum_partials(int nblk, int k, const double *__restrict__ part, double *__restrict__ out)
-{
-  // one warp per output
-  int j = blockIdx.x;
-  double s = 0.0;
-  for (int b = threadIdx.x; b < nblk; b += 32) s += part[(size_t)b * k + j];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if (threadIdx.x == 0) out[j] = s;
+  // the last block to finish sums the partials in block order (deterministic)
+  // and re-arms the ticket for the next launch on the stream
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (warp < KC) {
+    double x = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(part + (size_t)b * KC + warp);
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) out[warp] = x;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
 }
 // w += sign * sum_j h_j V_j   (h on device), KC vectors per launch
 template <typename T, int KC>
@@ -292,9 +300,10 @@ template <typename T> void v_mask(int nx, int ny, int nz, uint32_t dir, T *v, cu
 }
 template <typename T, int KC> static void mdot_chunk(size_t n, const T *const *V_dev, const T *w, double *part, double *out, cudaStream_t s)
 {
-  k_mdot_partial<T, KC><<<P3D_MDOT_BLOCKS, 256, 0, s>>>(n, V_dev, w, part);
-  k_sum_partials<<<KC, 32, 0, s>>>(P3D_MDOT_BLOCKS, KC, part, out);
-  count_launch(2);
+  // part holds P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK partials, then the ticket counter
+  unsigned int *ticket = reinterpret_cast<unsigned int *>(part + (size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK);
+  k_mdot_partial<T, KC><<<P3D_MDOT_BLOCKS, 256, 0, s>>>(n, V_dev, w, part, ticket, out);
+  count_launch(1);
 }
 template <typename T>
 void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s)
