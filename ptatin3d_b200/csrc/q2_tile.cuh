@@ -151,8 +151,20 @@ template <int NW> struct Brick {
   static constexpr int NX = 2 * TX + 1, NY = 2 * TY + 1, NZ = 2 * NW + 1;
   static constexpr int NN = NX * NY * NZ;
   static constexpr int NE = TX * TY * NW;
-  static constexpr int PL = 3 * NX * NY;          // values of one node plane
+  // node tiles in shared memory: rows of NX nodes x 3 components (33 values)
+  // stored with a stride of 34, so that the 30 lanes of a warp, which read
+  // nodes 2 apart in x and rows 2 apart in y, meet in at most 2 of the 16
+  // 8-byte banks per half-warp (3 with stride 33)
+  static constexpr int RS = 3 * NX + 1;           // row stride
+  static constexpr int PL = NY * RS;              // node-plane stride
+  static constexpr int TILE = NZ * PL;            // values of one node tile
 };
+// offset of node n (0..26) of the element at brick slot (a, b, c) in a node tile
+template <int NW> __device__ __forceinline__ int tile_node(int a, int b, int c, int n)
+{
+  using BK = Brick<NW>;
+  return 3 * (2 * a + n % 3) + BK::RS * ((2 * b + (n / 3) % 3) + BK::NY * (2 * c + n / 9));
+}
 
 // Brick geometry for blockIdx.x
 struct BrickPos {
@@ -204,7 +216,7 @@ __device__ __forceinline__ void stage_nodes(const TileArgs<T> &A, const BrickPos
                                             bool mask)
 {
   using BK = Brick<NW>;
-  constexpr int ROWLEN = 3 * BK::NX, NROWS = BK::NY * BK::NZ;
+  constexpr int NROWS = BK::NY * BK::NZ;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nax = 2 * b.ax + 1, nay = 2 * b.ay + 1, naz = 2 * b.az + 1;
   const int li0 = lane / 3, c0 = lane - 3 * li0; // column `lane`
@@ -216,7 +228,7 @@ __device__ __forceinline__ void stage_nodes(const TileArgs<T> &A, const BrickPos
     if (lj >= nay || lk >= naz) continue;
     const int iy = b.n0y + lj, iz = b.n0z + lk;
     const T *gr = src + 3 * ((size_t)b.n0x + (size_t)A.gx * ((size_t)iy + (size_t)A.gy * (size_t)iz));
-    T *sr = s + row * ROWLEN;
+    T *sr = s + row * BK::RS;
     bool m0 = ok0, m1 = ok1;
     if (domask) {
       m0 = m0 && !is_dirichlet(A.dir, b.n0x + li0, iy, iz, A.ox, A.oy, A.oz, exn, eyn, ezn, c0);
@@ -246,10 +258,10 @@ template <typename T, int NW>
 __device__ __forceinline__ void accumulate_phases(T *s_acc, const T r[27], int a, int bb, int c, int f, bool doit)
 {
   using BK = Brick<NW>;
-  T *base = s_acc + 3 * (2 * a + BK::NX * (2 * bb + BK::NY * 2 * c)) + f;
+  T *base = s_acc + tile_node<NW>(a, bb, c, 0) + f;
   if (doit) {
 #pragma unroll
-    for (int n = 0; n < 27; n++) atomicAdd(base + 3 * ((n % 3) + BK::NX * ((n / 3) % 3)) + (n / 9) * BK::PL, r[n]);
+    for (int n = 0; n < 27; n++) atomicAdd(base + 3 * (n % 3) + BK::RS * ((n / 3) % 3) + (n / 9) * BK::PL, r[n]);
   }
   __syncthreads();
 }
@@ -263,7 +275,7 @@ __device__ __forceinline__ void write_tile(const TileArgs<T> &A, const BrickPos 
                                            int rowmode)
 {
   using BK = Brick<NW>;
-  constexpr int ROWLEN = 3 * BK::NX, NROWS = BK::NY * BK::NZ;
+  constexpr int NROWS = BK::NY * BK::NZ;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nax = 2 * b.ax + 1, nay = 2 * b.ay + 1, naz = 2 * b.az + 1;
   const int exn = A.ox + 2 * A.mx, eyn = A.oy + 2 * A.my, ezn = A.oz + 2 * A.mz;
@@ -292,9 +304,9 @@ __device__ __forceinline__ void write_tile(const TileArgs<T> &A, const BrickPos 
         if (rown && (k ? own1 : own0)) A.y[g] = rowmode == 0 ? A.x[g] : (rowmode == 1 ? (T)0 : (T)1);
         continue;
       }
-      const T v = s_acc[row * ROWLEN + col];
+      const T v = s_acc[row * BK::RS + col];
       if (rs || (k ? xs1 : xs0)) atomicAdd(A.y + g, v);
-      else A.y[g] = A.overwrite ? v : s_y[row * ROWLEN + col] + v;
+      else A.y[g] = A.overwrite ? v : s_y[row * BK::RS + col] + v;
     }
   }
 }

@@ -35,11 +35,6 @@ __device__ __forceinline__ LaneMap lane_map()
   return m;
 }
 
-template <int NW> __device__ __forceinline__ int brick_node(int a, int b, int c, int n)
-{
-  using BK = Brick<NW>;
-  return (2 * a + n % 3) + BK::NX * ((2 * b + (n / 3) % 3) + BK::NY * (2 * c + n / 9));
-}
 
 // correctly rounded reciprocal (CUDA's intrinsics)
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
@@ -74,7 +69,7 @@ __device__ __forceinline__ void geometry_pass(const T *s_c, const T *s_eta, T *g
 {
   T xq[27];
 #pragma unroll
-  for (int n = 0; n < 27; n++) xq[n] = s_c[3 * brick_node<NW>(L.a, L.b, L.c, n) + L.f];
+  for (int n = 0; n < 27; n++) xq[n] = s_c[tile_node<NW>(L.a, L.b, L.c, n) + L.f];
   T avg = (T)0, rL = (T)1;
   if (PB) {
 #pragma unroll
@@ -127,7 +122,7 @@ __device__ __forceinline__ void geometry_pass(const T *s_c, const T *s_eta, T *g
 template <typename T, int NW> __device__ __forceinline__ void load_interp(const T *s_x, const LaneMap &L, T uq[27])
 {
 #pragma unroll
-  for (int n = 0; n < 27; n++) uq[n] = s_x[3 * brick_node<NW>(L.a, L.b, L.c, n) + L.f];
+  for (int n = 0; n < 27; n++) uq[n] = s_x[tile_node<NW>(L.a, L.b, L.c, n) + L.f];
   interp27(uq);
 }
 
@@ -191,25 +186,27 @@ __device__ __forceinline__ void a21_moments(const LaneMap &L, bool valid, int sr
 }
 
 // ------------------------------------------------------------ affine kernels
-// Per-element constant Jacobian.  kdat: [brick][slot][36] = J^{-1} (9) and
-// eta*w*detJ at the 27 Gauss points; kpre (A12/A21 only): [brick][slot][12] =
-// the pressure-basis map C[d][m] = M[d][m] / (2 M[m][m]) (9, M = dx/dxi) and
-// detJ, 2 pad.  On an affine element the basis coordinate
+// Per-element constant Jacobian.  kdat: [brick][slot][37] = J^{-1} (9),
+// eta*w*detJ at the 27 Gauss points, 1 pad; kpre (A12/A21 only):
+// [brick][slot][13] = the pressure-basis map C[d][m] = M[d][m] / (2 M[m][m])
+// (9, M = dx/dxi), detJ, 3 pad.  The odd strides put the 10 elements of a warp
+// on 10 different shared-memory banks (36 and 12 put them on 4).  On an affine
+// element the basis coordinate
 //   hat_m(x(xi)) = (x_m(xi) - mean of the 27 nodes) / L_m = sum_d C[d][m] xi_d,
 // because the node mean is x(0) and the mid-face extent L_m is 2 M[m][m]
 // (src/element_utils_q2.c:183-224).
-constexpr int KAFF = 36, KPRE = 12;
+constexpr int KAFF = 37, KPRE = 13;
 template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct AffineSmem {
   using BK = Brick<NW>;
   static constexpr bool NEEDX = DA11 || DA21;
   static constexpr bool NEEDY = DA11 || DA12;
   static constexpr bool PB = DA12 || DA21;
   static constexpr int OX = 0;
-  static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
-  static constexpr int OK = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
+  static constexpr int OY = OX + (NEEDX ? align16(BK::TILE, sizeof(T)) : 0);
+  static constexpr int OK = OY + (NEEDY ? align16(BK::TILE, sizeof(T)) : 0);
   static constexpr int OP = OK + align16(BK::NE * KAFF, sizeof(T));
   static constexpr int OA = OP + (PB ? align16(BK::NE * KPRE, sizeof(T)) : 0); // node-tile accumulator
-  static constexpr int TOTAL = OA + (NEEDY ? 3 * BK::NN : 0);
+  static constexpr int TOTAL = OA + (NEEDY ? BK::TILE : 0);
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
 };
 
@@ -229,7 +226,7 @@ __global__ void __launch_bounds__(32 * NW, (DA12 || DA21) ? (DA11 ? 2 : 3) : 4) 
   if (PB) stage_block(A.kgq + brick * BK::NE * KPRE, s_p, BK::NE * KPRE);
   if (NEEDY && !A.overwrite) stage_nodes<T, NW>(A, b, A.y, s_y, false);
   if (NEEDY)
-    for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
+    for (int i = threadIdx.x; i < BK::TILE; i += blockDim.x) s_acc[i] = (T)0;
   cp_async_wait_all();
   __syncthreads();
 
@@ -347,9 +344,9 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSme
   static constexpr bool NEEDY = DA11 || DA12;
   static constexpr int CQ = align16(BK::NE * GQC, sizeof(T)); // Gauss-point coordinate table
   static constexpr int OX = 0;
-  static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
-  static constexpr int OC = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
-  static constexpr int CA = align16(3 * BK::NN, sizeof(T)); // accumulator (reuses the tile region)
+  static constexpr int OY = OX + (NEEDX ? align16(BK::TILE, sizeof(T)) : 0);
+  static constexpr int OC = OY + (NEEDY ? align16(BK::TILE, sizeof(T)) : 0);
+  static constexpr int CA = align16(BK::TILE, sizeof(T)); // accumulator (reuses the tile region)
   static constexpr int OK = OC + (CA > CQ ? CA : CQ);
   static constexpr int TOTAL = OK + align16(BK::NE * 27, sizeof(T));
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
@@ -460,7 +457,7 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
     interp27T(r);
     __syncthreads(); // every warp is done with the Gauss-point coordinates: reuse as the accumulator
     T *s_acc = s_c;
-    for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
+    for (int i = threadIdx.x; i < BK::TILE; i += blockDim.x) s_acc[i] = (T)0;
     __syncthreads();
     accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
@@ -480,9 +477,9 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralTab
   static constexpr int GQ = (DA12 || DA21) ? 14 : 10;
   static constexpr int CQ = align16(BK::NE * GQC, sizeof(T)); // Gauss-point coordinate table
   static constexpr int OX = 0;
-  static constexpr int OY = OX + (NEEDX ? align16(3 * BK::NN, sizeof(T)) : 0);
-  static constexpr int OC = OY + (NEEDY ? align16(3 * BK::NN, sizeof(T)) : 0);
-  static constexpr int CA = align16(3 * BK::NN, sizeof(T)); // accumulator (reuses the tile region)
+  static constexpr int OY = OX + (NEEDX ? align16(BK::TILE, sizeof(T)) : 0);
+  static constexpr int OC = OY + (NEEDY ? align16(BK::TILE, sizeof(T)) : 0);
+  static constexpr int CA = align16(BK::TILE, sizeof(T)); // accumulator (reuses the tile region)
   static constexpr int OK = OC + (CA > CQ ? CA : CQ);
   static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
   static constexpr int TOTAL = OG + BK::NE * 9 * GQ;
@@ -617,7 +614,7 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
     interp27T(r);
     __syncthreads(); // every warp is done with the Gauss-point coordinates: reuse as the accumulator
     T *s_acc = s_c;
-    for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
+    for (int i = threadIdx.x; i < BK::TILE; i += blockDim.x) s_acc[i] = (T)0;
     __syncthreads();
     accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
@@ -632,8 +629,8 @@ template <typename T, int NW> struct DiagSmem {
   using BK = Brick<NW>;
   static constexpr int GQ = 10;
   static constexpr int OY = 0;
-  static constexpr int OC = OY + align16(3 * BK::NN, sizeof(T));
-  static constexpr int OK = OC + align16(3 * BK::NN, sizeof(T));
+  static constexpr int OC = OY + align16(BK::TILE, sizeof(T));
+  static constexpr int OK = OC + align16(BK::TILE, sizeof(T));
   static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
   static constexpr int TOTAL = OG + BK::NE * 27 * GQ;
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
@@ -683,7 +680,7 @@ __global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
   }
   __syncthreads();
   T *s_acc = s_c;
-  for (int i = threadIdx.x; i < 3 * BK::NN; i += blockDim.x) s_acc[i] = (T)0;
+  for (int i = threadIdx.x; i < BK::TILE; i += blockDim.x) s_acc[i] = (T)0;
   __syncthreads();
   accumulate_phases<T, NW>(s_acc, dg, L.a, L.b, L.c, L.f, L.active && valid);
   write_tile<T, NW>(A, b, s_acc, s_y, 2);
@@ -818,8 +815,10 @@ __global__ void pack_affine_kernel(int mx, int my, int mz, int gx, int gy, int o
       T *pp = pre + idx * KPRE;
       for (int d = 0; d < 3; d++)
         for (int mm = 0; mm < 3; mm++) pp[3 * d + mm] = (T)(M[3 * d + mm] / (2.0 * M[3 * mm + mm]));
-      pp[9] = (T)det; pp[10] = (T)0; pp[11] = (T)0;
+      pp[9] = (T)det;
+      for (int r = 10; r < KPRE; r++) pp[r] = (T)0;
     }
+    for (int r = 36; r < KAFF; r++) o[r] = (T)0;
     size_t e = (size_t)ex + (size_t)mx * ((size_t)ey + (size_t)my * ez);
     for (int q = 0; q < 27; q++) {
       int qi = q % 3, qj = (q / 3) % 3, qk = q / 9;

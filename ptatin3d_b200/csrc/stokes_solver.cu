@@ -692,7 +692,7 @@ int p3d_solver_estimate_bytes(const p3d_mesh_desc *mesh, const p3d_solver_opts *
       total += 243.0 * nn * (8.0 + (mixed && l > 0 ? 4.0 : 0.0));
     } else {
       total += 8.0 * (3 * nn + 27 * nel);                         // level coordinates + viscosity
-      const double op = 3 * nn + 1.2 * (27 + 36 + 88) * nel; // operator: coords, packed eta, affine data, Gauss-point coords
+      const double op = 3 * nn + 1.2 * (27 + 37 + 13 + 88) * nel; // operator: coords, packed eta, affine data and pressure map, Gauss-point coords
       total += 8.0 * op + (mixed && l > 0 ? 4.0 * op : 0.0);
     }
     if (l == 0) total += 8.0 * (nv * nv + 68 * nv + 1024); // dense coarse inverse and its scratch

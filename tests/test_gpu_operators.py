@@ -300,3 +300,51 @@ def test_mg_transfer(cuda, restatement):
         gc = torch.empty(xc.size, dtype=dt, device="cuda")
         mg_restrict(T(xf, dt), gc, cn)
         assert rel(host(gc), restatement.restrict(cn, 3, xf)) <= tol
+
+
+@pytest.mark.parametrize("deform", [0.0, 0.15])
+def test_ghosted_local_arrays(cuda, restatement, deform):
+    """The drop-in layout: a rank's elements inside a ghosted node lattice
+    (PETSc local vectors, ghost layers of 2 nodes on some sides, faces of the
+    local block not on the global boundary).  The raw element apply, A12 and
+    A21 must equal the oracle on the owned sub-lattice and leave every
+    ghost-only entry untouched."""
+    mx, my, mz = 4, 3, 5
+    lo, hi = (2, 0, 2), (2, 2, 0)  # ghost nodes before / after the owned block
+    gx, gy, gz = (2 * m + 1 + a + b for m, a, b in zip((mx, my, mz), lo, hi))
+    full = M.uniform_coords(gx // 2, gy // 2, gz // 2)  # any lattice of the right extent works for ghosts
+    c = full.reshape(gz, gy, gx, 3).copy()
+    owned = (slice(lo[2], lo[2] + 2 * mz + 1), slice(lo[1], lo[1] + 2 * my + 1), slice(lo[0], lo[0] + 2 * mx + 1))
+    c_loc = M.uniform_coords(mx, my, mz)
+    if deform:
+        c_loc = M.perturb_interior(c_loc, mx, my, mz, frac=deform, seed=3)
+    c[owned] = c_loc.reshape(2 * mz + 1, 2 * my + 1, 2 * mx + 1, 3)
+    rng = np.random.default_rng(5)
+    eta = 10 ** rng.uniform(-1, 1, size=(mx * my * mz, 27))
+    x = rng.uniform(-1, 1, size=(gz, gy, gx, 3))
+    p = rng.uniform(-1, 1, size=4 * mx * my * mz)
+    d = mesh_desc_whole(mx, my, mz, M.FREE_SLIP)
+    d.gx, d.gy, d.gz = gx, gy, gz
+    d.ox, d.oy, d.oz = lo
+    d.global_faces = 0  # an interior rank: no Dirichlet face
+    op = MatStokesMF(d, PREC_F64)
+    op.set_coefficients(c.reshape(-1), eta)
+    assert op.geometry_mode == (GEOM_GENERAL if deform else GEOM_AFFINE)
+    y = torch.zeros(x.size, dtype=torch.float64, device="cuda")
+    op.spmv(T(x.reshape(-1)), y)
+    dims = (mx, my, mz)
+    xl = x[owned].reshape(-1)
+    ref = restatement.a11_raw(dims, c_loc, eta.reshape(-1), xl)
+    yh = host(y).reshape(gz, gy, gx, 3)
+    assert rel(yh[owned].reshape(-1), ref) <= TOL64
+    ghost = np.ones((gz, gy, gx), dtype=bool)
+    ghost[owned] = False
+    assert np.all(yh[ghost] == 0.0)
+    yu = torch.zeros(x.size, dtype=torch.float64, device="cuda")
+    op.mult_a12(T(p), yu, boundary=False)
+    yuh = host(yu).reshape(gz, gy, gx, 3)
+    assert rel(yuh[owned].reshape(-1), restatement.a12_raw(dims, c_loc, p)) <= TOL64
+    assert np.all(yuh[ghost] == 0.0)
+    yp = torch.zeros(p.size, dtype=torch.float64, device="cuda")
+    op.mult_a21(T(x.reshape(-1)), yp, boundary=False)
+    assert rel(host(yp), restatement.a21_raw(dims, c_loc, xl)) <= TOL64
