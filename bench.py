@@ -278,6 +278,51 @@ def solve_leg(device, m=32, seed=1, cpu=True):
             "oracle_solve": out["ref"], "cpu_solve": cpu_solve}
 
 
+SOLVE_C4_WORKLOAD = ("Stokes solve, Q2-P1disc 96^3 deformed mesh (interior nodes +-0.2h, Jacobians per Gauss point), "
+                     "per-element log-normal eta with sigma 1 decade (corr 0.1), 8 sinkers of density +1%, g=-z, "
+                     "free slip walls/base, free surface top; FGMRES(30) + Schur upper (geometric mean) + 5-level "
+                     "Galerkin GMG, Chebyshev(3)/Jacobi, rtol 1e-6")
+
+
+def solve_c4_leg(device, coords, m=96, seed=4):
+    """FP64 vs mixed-precision solve on the deformed 96^3 mesh of the apply
+    benchmark.  The apply's sigma = 2 decades field spans 12 decades of eta,
+    where this preconditioner family stagnates (the CPU restatement too), so
+    the solve takes the same construction with sigma = 1 decade."""
+    import torch
+
+    from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
+    from ptatin3d_b200 import mesh as M
+    from ptatin3d_b200.solver import StokesSolver
+    bits = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
+    eta = M.lognormal_grf_eta(m, m, m, seed=seed, sigma_decades=1.0, corr_len=0.1)
+    qp = M.qp_coords(coords, m, m, m)
+    cen, r = M.random_sinkers(8, 1, 0.1)
+    rho = M.sinker_density(qp, cen, r, 1.0, 1.01)
+    out, sols = {}, {}
+    for name, prec in (("fp64", PREC_F64), ("mixed", PREC_F32)):
+        S = StokesSolver(m, m, m, bits, device=device, nlevels=5, rtol=1e-6, max_it=2000, mg_precision=prec,
+                         schur_eta=SCHUR_ETA_GEOMEAN)
+        S.setup(coords, eta)
+        S.set_rhs_body_force(rho)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, p, st = S.solve(raise_on_noconv=False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        sols[name] = (u.cpu().numpy(), p.cpu().numpy())
+        out[name] = {"s": dt, "iterations": st["iterations"], "converged": bool(st["converged"]),
+                     "rel_residual": st["rfinal"] / st["r0"], "setup_s": st["setup_ms"] * 1e-3}
+        S.destroy()
+        del S, u, p
+        torch.cuda.empty_cache()
+    (u64, p64), (u32, p32) = sols["fp64"], sols["mixed"]
+    return {"workload": SOLVE_C4_WORKLOAD, "unit": "s", "fp64_s": out["fp64"]["s"], "mixed_s": out["mixed"]["s"],
+            "speedup_mixed_vs_fp64": out["fp64"]["s"] / out["mixed"]["s"], "fp64": out["fp64"], "mixed": out["mixed"],
+            "u_diff_mixed_vs_fp64": float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64)),
+            "p_diff_mixed_vs_fp64": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))}
+
+
 SERVE_SIZES = (8, 12, 16, 24, 32, 48)
 
 
@@ -517,6 +562,11 @@ def run_b200(args):
     solve = None
     if rank == 0 and not args.no_solve:
         solve = solve_leg(local, cpu=not args.no_cpu)
+        if m == 96 and args.workload == "deformed":
+            try:
+                solve["deformed_96"] = solve_c4_leg(local, wl["coords"])
+            except Exception as exc:  # reported, not required
+                solve["deformed_96"] = {"failed": str(exc)}
     serving = None
     if rank == 0 and args.serve_requests > 0:
         serving = serve_leg(local, args.serve_requests)
