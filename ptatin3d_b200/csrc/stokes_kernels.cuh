@@ -482,7 +482,11 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralTab
   static constexpr int CA = align16(BK::TILE, sizeof(T)); // accumulator (reuses the tile region)
   static constexpr int OK = OC + (CA > CQ ? CA : CQ);
   static constexpr int OG = OK + align16(BK::NE * 27, sizeof(T));
-  static constexpr int TOTAL = OG + BK::NE * 9 * GQ;
+  // per-element stride of the plane's Jacobian table: 9 points x GQ values,
+  // padded so that the 30 lanes of a warp spread over the 4-byte banks
+  // (90 -> 105 and 126 -> 133 cut the table's shared wavefronts by a third)
+  static constexpr int ES = GQ == 10 ? 105 : (GQ == 14 ? 133 : 9 * GQ);
+  static constexpr int TOTAL = OG + BK::NE * ES;
   static constexpr size_t BYTES = (size_t)TOTAL * sizeof(T);
 };
 
@@ -512,7 +516,7 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
   const T *X = s_c + 3 * L.slot + L.f; // coordinate f at Gauss point n: X[n * GL::PT]
   const T avg = PB ? s_c[GL::EX + 6 * L.slot + L.f] : (T)0, rL = PB ? s_c[GL::EX + 6 * L.slot + 3 + L.f] : (T)1;
   const T *eta_e = s_k + L.slot * 27;
-  T *g = s_g + L.slot * 9 * GQ;
+  T *g = s_g + L.slot * SM::ES;
 
   const int src1 = L.base + (L.f + 1) % 3, src2 = L.base + (L.f + 2) % 3;
   const int r0 = 3 * L.f, r1 = 3 * ((L.f + 1) % 3), r2 = 3 * ((L.f + 2) % 3);
