@@ -14,7 +14,6 @@ template <typename A, typename B> void v_convert(size_t n, const A *x, B *y, cud
 template <typename T> void v_axpby(size_t n, T a, const T *x, T b, T *y, cudaStream_t s);
 template <typename T> void v_scale(size_t n, T a, T *y, cudaStream_t s);
 template <typename T> void v_jacobi(size_t n, const double *dinv, const T *r, T *z, cudaStream_t s);
-template <typename T> void v_cheb_init(size_t n, const double *dinv, const T *r, T inv_theta, T *d, cudaStream_t s);
 template <typename T>
 void v_cheb_step(size_t n, const double *dinv, T *x, T *r, const T *Ad, T *d, T c1, T c2, bool last, cudaStream_t s);
 template <typename T>

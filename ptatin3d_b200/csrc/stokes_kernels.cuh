@@ -143,10 +143,6 @@ __device__ __forceinline__ void qp_action(const T Jr[9], T ce, T g0, T g1, T g2,
   ro2 = Jr[2] * T0 + Jr[5] * T1 + Jr[8] * T2;
 }
 
-template <typename T, int i, int j, int k> struct QP {
-  static constexpr int q = i + 3 * j + 9 * k;
-};
-
 // gradient of the Gauss-point field uq at (i,j,k) in reference directions
 #define P3D_GRAD(uq, i, j, k, g0, g1, g2)                                                                       \
   T g0 = dcol(i, uq[3 * (j) + 9 * (k)], uq[1 + 3 * (j) + 9 * (k)], uq[2 + 3 * (j) + 9 * (k)]);                  \

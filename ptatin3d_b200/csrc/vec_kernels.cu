@@ -38,13 +38,6 @@ template <typename T> __global__ void k_jacobi(size_t n, const double *__restric
 {
   GS_LOOP(i, n) z[i] = (T)(dinv[i] * (double)r[i]);
 }
-// Chebyshev start: r = b - A x was formed in r (or r = b when x = 0);
-// d = dinv .* r / theta
-template <typename T>
-__global__ void k_cheb_init(size_t n, const double *__restrict__ dinv, const T *__restrict__ r, T inv_theta, T *__restrict__ d)
-{
-  GS_LOOP(i, n) d[i] = (T)(dinv[i] * (double)r[i]) * inv_theta;
-}
 // Chebyshev start from x = 0: x = 0, r = b, d = dinv .* b / theta (one pass)
 template <typename T>
 __global__ void k_cheb_init0(size_t n, const double *__restrict__ dinv, const T *__restrict__ b, T inv_theta,
@@ -264,11 +257,6 @@ template <typename T> void v_jacobi(size_t n, const double *dinv, const T *r, T 
   k_jacobi<<<vgrid(n), 256, 0, s>>>(n, dinv, r, z);
   count_launch(1);
 }
-template <typename T> void v_cheb_init(size_t n, const double *dinv, const T *r, T inv_theta, T *d, cudaStream_t s)
-{
-  k_cheb_init<<<vgrid(n), 256, 0, s>>>(n, dinv, r, inv_theta, d);
-  count_launch(1);
-}
 template <typename T>
 void v_cheb_init0(size_t n, const double *dinv, const T *b, T inv_theta, T *x, T *r, T *d, cudaStream_t s)
 {
@@ -377,7 +365,6 @@ template void v_convert<float, double>(size_t, const float *, double *, cudaStre
   template void v_axpby<T>(size_t, T, const T *, T, T *, cudaStream_t);                                                \
   template void v_scale<T>(size_t, T, T *, cudaStream_t);                                                              \
   template void v_jacobi<T>(size_t, const double *, const T *, T *, cudaStream_t);                                     \
-  template void v_cheb_init<T>(size_t, const double *, const T *, T, T *, cudaStream_t);                               \
   template void v_cheb_step<T>(size_t, const double *, T *, T *, const T *, T *, T, T, bool, cudaStream_t);            \
   template void v_cheb_init0<T>(size_t, const double *, const T *, T, T *, T *, T *, cudaStream_t);                   \
   template void v_cheb_init_res<T>(size_t, const double *, const T *, const T *, T, T *, T *, cudaStream_t);          \
