@@ -42,6 +42,22 @@ def test_errors_are_codes_not_exits():
     assert L.p3d_mg_prolong(16, 2, 2, 2, 3, None, None, None) == _lib.P3D_ERR_ARG
 
 
+def test_inconsistent_ghosted_desc_is_refused():
+    """Host-side validation of a ghosted local-array descriptor, before any device call."""
+    L = _lib.lib()
+    d = _lib.MeshDesc()
+    assert L.p3d_mesh_desc_whole(4, 3, 5, 0, C.byref(d)) == 0
+    h = C.c_void_p()
+    d.ox = 2  # 2 + 2*4 + 1 > gx = 9
+    assert L.p3d_op_create(C.byref(d), 64, 0, C.byref(h)) == _lib.P3D_ERR_ARG
+    assert b"exceeds the ghosted lattice" in L.p3d_last_error()
+    d.ox, d.oy = 0, -1
+    assert L.p3d_op_create(C.byref(d), 64, 0, C.byref(h)) == _lib.P3D_ERR_ARG
+    d.oy = 0
+    assert L.p3d_op_create(C.byref(d), 16, 0, C.byref(h)) == _lib.P3D_ERR_ARG
+    assert b"precision" in L.p3d_last_error()
+
+
 def test_mesh_desc_whole():
     d = _lib.MeshDesc()
     assert _lib.lib().p3d_mesh_desc_whole(4, 5, 6, 7, C.byref(d)) == 0
