@@ -18,7 +18,7 @@ from multiprocessing import shared_memory
 import numpy as np
 
 
-def _worker(names, shapes, m, z0, z1, steps, warmup, barrier, out_q, rank):
+def _worker(names, shapes, m, z0, z1, steps, warmup, barrier, out_q, rank, collect):
     from oracle.oracle import Reference
     shm = [shared_memory.SharedMemory(name=n) for n in names]
     try:
@@ -37,14 +37,20 @@ def _worker(names, shapes, m, z0, z1, steps, warmup, barrier, out_q, rank):
         t0 = time.perf_counter()
         for _ in range(steps):
             F.a11_raw(xs, "avx", out=y)
-        out_q.put((rank, (time.perf_counter() - t0) / steps))
+        dt = (time.perf_counter() - t0) / max(1, steps)
+        if collect:
+            y[...] = 0.0
+            F.a11_raw(xs, "avx", out=y)
+        out_q.put((rank, dt, y if collect else None))
     finally:
         for b in shm:
             b.close()
 
 
-def slab_apply_time(coords, eta, x, m, nproc, steps=5, warmup=1, timeout=600):
-    """Seconds per apply of the whole m^3 mesh cut into nproc z-slabs."""
+def slab_apply_time(coords, eta, x, m, nproc, steps=5, warmup=1, timeout=600, collect=False):
+    """Seconds per apply of the whole m^3 mesh cut into nproc z-slabs; with
+    collect, also the assembled result (the slabs' partial sums added on the
+    node planes they share)."""
     nproc = max(1, min(nproc, m))
     arrays = [np.ascontiguousarray(a, dtype=np.float64) for a in (coords, np.asarray(eta).reshape(-1, 27), x)]
     shm = []
@@ -58,14 +64,17 @@ def slab_apply_time(coords, eta, x, m, nproc, steps=5, warmup=1, timeout=600):
         q = ctx.Queue()
         cuts = [round(r * m / nproc) for r in range(nproc + 1)]
         procs = [ctx.Process(target=_worker, args=([b.name for b in shm], [a.shape for a in arrays], m, cuts[r],
-                                                   cuts[r + 1], steps, warmup, barrier, q, r)) for r in range(nproc)]
+                                                   cuts[r + 1], steps, warmup, barrier, q, r, collect))
+                 for r in range(nproc)]
         for p in procs:
             p.start()
-        times, t_end = [], time.monotonic() + timeout
+        times, parts, t_end = [], {}, time.monotonic() + timeout
         try:
             while len(times) < nproc:
                 try:
-                    times.append(q.get(timeout=1.0)[1])
+                    rank, dt, ys = q.get(timeout=1.0)
+                    times.append(dt)
+                    parts[rank] = ys
                 except Exception:  # queue empty: stop if a worker died or time ran out
                     if any(p.exitcode not in (None, 0) for p in procs) or time.monotonic() > t_end:
                         raise RuntimeError("slab worker failed or timed out")
@@ -74,7 +83,13 @@ def slab_apply_time(coords, eta, x, m, nproc, steps=5, warmup=1, timeout=600):
                 p.join(timeout=10)
                 if p.is_alive():
                     p.terminate()
-        return max(times)
+        if not collect:
+            return max(times)
+        P = 3 * (2 * m + 1) ** 2
+        y = np.zeros(arrays[2].size)
+        for r, ys in parts.items():
+            y[2 * cuts[r] * P:(2 * cuts[r + 1] + 1) * P] += ys
+        return max(times), y
     finally:
         for b in shm:
             b.close()

@@ -59,3 +59,17 @@ def test_cpu_and_gpu_solvers_agree(cuda, reference_kernels):
     assert rtc <= 1e-9 and st["converged"]
     assert abs(st["iterations"] - itc) <= 0.15 * itc + 3
     assert rel(ug.cpu().numpy(), uc) <= 1e-6
+
+
+def test_slab_partitioned_reference_apply(reference_kernels):
+    """The slab layout of the CPU baseline computes the same MatMult as the
+    whole-mesh reference kernel (partial sums added on the shared planes)."""
+    from oracle.cpu_slabs import slab_apply_time
+    m = 6
+    c = M.perturb_interior(M.uniform_coords(m, m, m), m, m, m, frac=0.2, seed=2)
+    eta = 10 ** np.random.default_rng(1).uniform(-1, 1, size=(m ** 3, 27))
+    x = np.random.default_rng(2).uniform(-1, 1, size=c.size)
+    t, y = slab_apply_time(c, eta, x, m, 3, steps=1, warmup=0, collect=True)
+    assert t > 0.0
+    reference_kernels.setup((m, m, m), c, eta)
+    assert rel(y, reference_kernels.a11_raw(x, "avx")) <= 1e-12
