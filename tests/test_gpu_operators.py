@@ -371,3 +371,26 @@ def test_full_size_deformed_apply_matches_reference_kernel(cuda, reference_kerne
     xd = T(x)
     op.mult(xd, Ax)
     assert abs(float(xd @ Aa - a @ Ax)) <= 1e-11 * float(a.norm() * Ax.norm())
+
+
+@pytest.mark.parametrize("dims", [(13, 7, 5), (1, 1, 1), (9, 5, 3), (8, 4, 2)])
+def test_fp32_general_ragged(cuda, dims):
+    """The FP32 general A11 kernel on ragged meshes (bricks cut by the mesh
+    edges), in the MatMult and the raw (y +=) forms, against the FP64 operator."""
+    mx, my, mz = dims
+    c = M.perturb_interior(M.uniform_coords(mx, my, mz), mx, my, mz, frac=0.15, seed=sum(dims))
+    eta = 10 ** np.random.default_rng(1).uniform(-1, 1, size=(mx * my * mz, 27))
+    case = dict(dims=dims, coords=c, eta=eta, bits=M.FREE_SLIP)
+    op64, op32 = make_op(case), make_op(case, prec=PREC_F32)
+    assert op32.geometry_mode == GEOM_GENERAL
+    x = np.random.default_rng(2).uniform(-1, 1, size=c.size)
+    y64 = torch.empty(x.size, dtype=torch.float64, device="cuda")
+    y32 = torch.empty(x.size, dtype=torch.float32, device="cuda")
+    op64.mult(T(x), y64)
+    op32.mult(T(x, torch.float32), y32)
+    assert rel(host(y32), host(y64)) <= TOL32
+    y0 = np.random.default_rng(3).uniform(-1, 1, size=x.size)  # y += A x keeps the old y
+    z64, z32 = T(y0), T(y0, torch.float32)
+    op64.spmv(T(x), z64)
+    op32.spmv(T(x, torch.float32), z32)
+    assert rel(host(z32), host(z64)) <= TOL32
