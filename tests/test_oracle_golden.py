@@ -90,6 +90,25 @@ def test_restatement_vs_reference_kernels_random(restatement, reference_kernels,
             assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(b)
 
 
+def test_reference_avx_a12_and_fused_operator(restatement, reference_kernels):
+    """The AVX back end's A12 and fused [A11 A12; A21 0] (what the CPU solve
+    baseline calls) against the restatement."""
+    case = bump_case(4, 3, 5, eta_kind="random", seed=3)
+    d, c, eta = case["dims"], case["coords"], case["eta"]
+    rng = np.random.default_rng(6)
+    x = rng.uniform(-1, 1, size=c.size)
+    p = rng.uniform(-1, 1, size=4 * 60)
+    reference_kernels.setup(d, c, eta)
+    ya12 = reference_kernels.a12_avx_raw(p)
+    ref12 = restatement.a12_raw(d, c, p)
+    assert np.linalg.norm(ya12 - ref12) <= 1e-13 * np.linalg.norm(ref12)
+    yu, yp = reference_kernels.stokes_avx_raw(x, p)
+    ref_u = restatement.a11_raw(d, c, eta.reshape(-1), x) + ref12
+    ref_p = restatement.a21_raw(d, c, x)
+    assert np.linalg.norm(yu - ref_u) <= 1e-13 * np.linalg.norm(ref_u)
+    assert np.linalg.norm(yp - ref_p) <= 1e-13 * np.linalg.norm(ref_p)
+
+
 def test_element_matrix_consistent_with_apply(restatement):
     """The 81x81 element matrix reproduces the matrix-free element apply."""
     case = bump_case(1, 1, 1, eta_kind="random", seed=7)
