@@ -23,7 +23,8 @@ void v_cheb_init_res(size_t n, const double *dinv, const T *b, const T *Ax, T in
 template <typename T> void v_residual(size_t n, const T *b, const T *Ax, T *r, cudaStream_t s);
 template <typename T> void v_mask(int nx, int ny, int nz, uint32_t dir, T *v, cudaStream_t s);
 template <typename T>
-void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s);
+void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s,
+            double *self_out = nullptr); // self_out: also w . w
 template <typename T> void v_maxpy(size_t n, int k, const double *h, const T *const *V_dev, T *w, double sign, cudaStream_t s);
 template <typename T>
 void v_cg_xr(size_t n, const double *num, const double *den, T *x, T *r, const T *p, const T *q, bool update_r, cudaStream_t s);

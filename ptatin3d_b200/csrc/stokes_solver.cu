@@ -587,15 +587,32 @@ static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
       double *vj = V + (size_t)j * N, *zj = Z + (size_t)j * N, *vn = V + (size_t)(j + 1) * N;
       CK(run_pc(s, vj, zj));
       CK(stokes_op(s, zj, w));
-      // two passes of classical Gram-Schmidt, coefficients on the device
-      for (int pass = 0; pass < 2; pass++) {
+      // classical Gram-Schmidt, coefficients on the device.  The first pass
+      // also forms |w|^2.  When the projection removed less than half of it
+      // (|w - V h|^2 = |w|^2 - |h|^2 > |w|^2 / 2) a second pass is not needed
+      // ("twice is enough": Giraud, Langou, Rozloznik 2005) and |w - V h|
+      // follows from that difference; otherwise the second pass runs and the
+      // norm is formed directly.
+      v_mdot<double>(N, j + 1, (const double *const *)s->Vptr, w, s->part, s->hdev, s->st, s->hdev + j + 1);
+      v_maxpy<double>(N, j + 1, s->hdev, (const double *const *)s->Vptr, w, -1.0, s->st);
+      CU(cudaMemcpyAsync(s->hhost, s->hdev, (j + 2) * 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+      CU(cudaStreamSynchronize(s->st), "sync");
+      double hh = 0.0;
+      for (int i = 0; i <= j; i++) {
+        H[(size_t)i * m + j] = s->hhost[i];
+        hh += s->hhost[i] * s->hhost[i];
+      }
+      const double wb2 = s->hhost[j + 1];
+      double hn;
+      if (wb2 - hh > 0.5 * wb2) {
+        hn = std::sqrt(wb2 - hh);
+      } else {
         v_mdot<double>(N, j + 1, (const double *const *)s->Vptr, w, s->part, s->hdev, s->st);
         v_maxpy<double>(N, j + 1, s->hdev, (const double *const *)s->Vptr, w, -1.0, s->st);
-        CU(cudaMemcpyAsync(s->hhost + pass * s->hs, s->hdev, (j + 1) * 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+        CU(cudaMemcpyAsync(s->hhost + s->hs, s->hdev, (j + 1) * 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+        CK(norm2(s, w, N, &hn)); // synchronizes
+        for (int i = 0; i <= j; i++) H[(size_t)i * m + j] += s->hhost[s->hs + i];
       }
-      double hn;
-      CK(norm2(s, w, N, &hn)); // synchronizes
-      for (int i = 0; i <= j; i++) H[(size_t)i * m + j] = s->hhost[i] + s->hhost[s->hs + i];
       H[(size_t)(j + 1) * m + j] = hn;
       if (hn > 0) {
         CU(cudaMemcpyAsync(vn, w, N * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
@@ -759,8 +776,9 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
   s->hs = m + 1;
   if (!rc) rc = dev_alloc((void **)&s->Vptr, (size_t)(m + 2) * sizeof(double *), "V ptrs");
   // partials of the multi-dot kernels, then their ticket counter (zero between launches)
-  if (!rc) rc = dev_alloc((void **)&s->part, ((size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK + 2) * 8, "partials");
-  if (!rc) rc = cuda_check(cudaMemset(s->part, 0, ((size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK + 2) * 8), "partials");
+  const size_t npart = (size_t)P3D_MDOT_BLOCKS * (P3D_MDOT_CHUNK + 1) + 2;
+  if (!rc) rc = dev_alloc((void **)&s->part, npart * 8, "partials");
+  if (!rc) rc = cuda_check(cudaMemset(s->part, 0, npart * 8), "partials");
   if (!rc) rc = dev_alloc((void **)&s->hdev, (size_t)(2 * s->hs + 2) * 8, "h");
   if (!rc) rc = cuda_check(cudaMallocHost((void **)&s->hhost, (size_t)(2 * s->hs + 2) * 8), "pinned h");
   if (!rc) {

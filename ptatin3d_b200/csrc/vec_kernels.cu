@@ -108,12 +108,16 @@ __global__ void k_mask(int nx, int ny, int nz, uint32_t dir, T *__restrict__ v)
 // KC vectors per launch so that the accumulators stay in registers
 template <typename T, int KC>
 __global__ void k_mdot_partial(size_t n, const T *const *__restrict__ V, const T *__restrict__ w, double *__restrict__ part,
-                               unsigned int *__restrict__ ticket, double *__restrict__ out)
+                               unsigned int *__restrict__ ticket, double *__restrict__ out, double *__restrict__ self_out)
 {
-  __shared__ double red[32][KC];
+  // self_out (optional): also w . w, the (KC+1)-th output
+  constexpr int KS = KC + 1; // partials per block
+  __shared__ double red[32][KS];
   __shared__ bool last;
+  const bool self = self_out != nullptr;
+  const int nout = KC + (self ? 1 : 0);
   const T *v[KC];
-  double acc[KC];
+  double acc[KC], accs = 0.0;
 #pragma unroll
   for (int j = 0; j < KC; j++) {
     v[j] = V[j];
@@ -124,19 +128,21 @@ __global__ void k_mdot_partial(size_t n, const T *const *__restrict__ V, const T
     double wi = (double)w[i];
 #pragma unroll
     for (int j = 0; j < KC; j++) acc[j] += (double)v[j][i] * wi;
+    if (self) accs += wi * wi;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-  for (int j = 0; j < KC; j++) {
-    double x = acc[j];
+  for (int j = 0; j < KS; j++) {
+    if (j == KC && !self) break;
+    double x = j < KC ? acc[j] : accs;
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
     if (lane == 0) red[warp][j] = x;
   }
   __syncthreads();
-  if (threadIdx.x < KC) {
+  if (threadIdx.x < nout) {
     double x = 0.0;
     for (int q = 0; q < nw; q++) x += red[q][threadIdx.x];
-    part[(size_t)blockIdx.x * KC + threadIdx.x] = x;
+    part[(size_t)blockIdx.x * KS + threadIdx.x] = x;
   }
   // the last block to finish sums the partials in block order (deterministic)
   // and re-arms the ticket for the next launch on the stream
@@ -146,11 +152,14 @@ __global__ void k_mdot_partial(size_t n, const T *const *__restrict__ V, const T
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (warp < KC) {
+  if (warp < nout) {
     double x = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(part + (size_t)b * KC + warp);
+    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(part + (size_t)b * KS + warp);
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) out[warp] = x;
+    if (lane == 0) {
+      if (warp < KC) out[warp] = x;
+      else *self_out = x;
+    }
   }
   if (threadIdx.x == 0) *ticket = 0u;
 }
@@ -286,29 +295,32 @@ template <typename T> void v_mask(int nx, int ny, int nz, uint32_t dir, T *v, cu
   k_mask<<<vgrid((size_t)nx * ny * nz), 256, 0, s>>>(nx, ny, nz, dir, v);
   count_launch(1);
 }
-template <typename T, int KC> static void mdot_chunk(size_t n, const T *const *V_dev, const T *w, double *part, double *out, cudaStream_t s)
+template <typename T, int KC>
+static void mdot_chunk(size_t n, const T *const *V_dev, const T *w, double *part, double *out, double *self_out,
+                       cudaStream_t s)
 {
-  // part holds P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK partials, then the ticket counter
-  unsigned int *ticket = reinterpret_cast<unsigned int *>(part + (size_t)P3D_MDOT_BLOCKS * P3D_MDOT_CHUNK);
-  k_mdot_partial<T, KC><<<P3D_MDOT_BLOCKS, 256, 0, s>>>(n, V_dev, w, part, ticket, out);
+  // part holds P3D_MDOT_BLOCKS * (P3D_MDOT_CHUNK + 1) partials, then the ticket counter
+  unsigned int *ticket = reinterpret_cast<unsigned int *>(part + (size_t)P3D_MDOT_BLOCKS * (P3D_MDOT_CHUNK + 1));
+  k_mdot_partial<T, KC><<<P3D_MDOT_BLOCKS, 256, 0, s>>>(n, V_dev, w, part, ticket, out, self_out);
   count_launch(1);
 }
 template <typename T>
-void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s)
+void v_mdot(size_t n, int k, const T *const *V_dev, const T *w, double *part, double *out_dev, cudaStream_t s,
+            double *self_out)
 {
   for (int j0 = 0; j0 < k; j0 += P3D_MDOT_CHUNK) {
     const int kc = k - j0 < P3D_MDOT_CHUNK ? k - j0 : P3D_MDOT_CHUNK;
     const T *const *V = V_dev + j0;
-    double *o = out_dev + j0;
+    double *o = out_dev + j0, *so = j0 == 0 ? self_out : nullptr;
     switch (kc) {
-    case 1: mdot_chunk<T, 1>(n, V, w, part, o, s); break;
-    case 2: mdot_chunk<T, 2>(n, V, w, part, o, s); break;
-    case 3: mdot_chunk<T, 3>(n, V, w, part, o, s); break;
-    case 4: mdot_chunk<T, 4>(n, V, w, part, o, s); break;
-    case 5: mdot_chunk<T, 5>(n, V, w, part, o, s); break;
-    case 6: mdot_chunk<T, 6>(n, V, w, part, o, s); break;
-    case 7: mdot_chunk<T, 7>(n, V, w, part, o, s); break;
-    default: mdot_chunk<T, 8>(n, V, w, part, o, s); break;
+    case 1: mdot_chunk<T, 1>(n, V, w, part, o, so, s); break;
+    case 2: mdot_chunk<T, 2>(n, V, w, part, o, so, s); break;
+    case 3: mdot_chunk<T, 3>(n, V, w, part, o, so, s); break;
+    case 4: mdot_chunk<T, 4>(n, V, w, part, o, so, s); break;
+    case 5: mdot_chunk<T, 5>(n, V, w, part, o, so, s); break;
+    case 6: mdot_chunk<T, 6>(n, V, w, part, o, so, s); break;
+    case 7: mdot_chunk<T, 7>(n, V, w, part, o, so, s); break;
+    default: mdot_chunk<T, 8>(n, V, w, part, o, so, s); break;
     }
   }
 }
@@ -370,7 +382,7 @@ template void v_convert<float, double>(size_t, const float *, double *, cudaStre
   template void v_cheb_init_res<T>(size_t, const double *, const T *, const T *, T, T *, T *, cudaStream_t);          \
   template void v_residual<T>(size_t, const T *, const T *, T *, cudaStream_t);                                        \
   template void v_mask<T>(int, int, int, uint32_t, T *, cudaStream_t);                                                 \
-  template void v_mdot<T>(size_t, int, const T *const *, const T *, double *, double *, cudaStream_t);                 \
+  template void v_mdot<T>(size_t, int, const T *const *, const T *, double *, double *, cudaStream_t, double *);       \
   template void v_maxpy<T>(size_t, int, const double *, const T *const *, T *, double, cudaStream_t);              \
   template void v_cg_xr<T>(size_t, const double *, const double *, T *, T *, const T *, const T *, bool, cudaStream_t); \
   template void v_cg_p<T>(size_t, const double *, const double *, const T *, T *, cudaStream_t);
