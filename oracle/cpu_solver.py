@@ -3,7 +3,9 @@ CPU solve baseline of bench.py only; the product never imports it).
 
 The same algorithm as the device solve, on host cores:
 
-* outer FGMRES(m), right preconditioned, two-pass classical Gram-Schmidt;
+* outer FGMRES(m), right preconditioned, two-pass classical Gram-Schmidt (the
+  device skips the second pass when the first removed less than half of the
+  vector's norm squared; the basis is the same up to rounding);
 * block upper-triangular preconditioner: z_p = S^-1 r_p with the per-element
   4x4 viscosity-scaled pressure mass matrix
   (src/stokes_assembly.c:299-450; element geometric-mean viscosity when
