@@ -21,7 +21,7 @@
 //   re-associated through the Gauss-point values; it needs ~1/3 fewer flops
 //   and no cross-lane traffic except 2 shuffles per Gauss point.
 //   The nodal contributions are added into a shared node tile (shared-memory
-//   atomic adds, accumulate_phases), and the tile is written to y:
+//   atomic adds, accumulate_tile), and the tile is written to y:
 //   plain stores for nodes no other CTA touches, atomicAdd for nodes on brick
 //   faces shared with neighbouring bricks.
 //
@@ -255,7 +255,7 @@ template <typename T> __device__ __forceinline__ void stage_block(const T *__res
 // the hardware (measured faster than parity classes taking turns).  Must be
 // reached by every thread of the CTA.
 template <typename T, int NW>
-__device__ __forceinline__ void accumulate_phases(T *s_acc, const T r[27], int a, int bb, int c, int f, bool doit)
+__device__ __forceinline__ void accumulate_tile(T *s_acc, const T r[27], int a, int bb, int c, int f, bool doit)
 {
   using BK = Brick<NW>;
   T *base = s_acc + tile_node<NW>(a, bb, c, 0) + f;

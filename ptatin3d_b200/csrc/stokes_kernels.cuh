@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(32 * NW, (DA12 || DA21) ? (DA11 ? 2 : 3) : 4) 
   if (DA21) a21_moments(L, valid, src1, src2, ap0, ap1, ap2, ap3, A.yp + 4 * eg);
   if (NEEDY) {
     interp27T(r);
-    accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
+    accumulate_tile<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
   }
 }
@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
     T *s_acc = s_c;
     for (int i = threadIdx.x; i < BK::TILE; i += blockDim.x) s_acc[i] = (T)0;
     __syncthreads();
-    accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
+    accumulate_tile<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
   }
 }
@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
     T *s_acc = s_c;
     for (int i = threadIdx.x; i < BK::TILE; i += blockDim.x) s_acc[i] = (T)0;
     __syncthreads();
-    accumulate_phases<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
+    accumulate_tile<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
   }
 }
@@ -682,7 +682,7 @@ __global__ void __launch_bounds__(32 * NW) diag_general_kernel(TileArgs<T> A)
   T *s_acc = s_c;
   for (int i = threadIdx.x; i < BK::TILE; i += blockDim.x) s_acc[i] = (T)0;
   __syncthreads();
-  accumulate_phases<T, NW>(s_acc, dg, L.a, L.b, L.c, L.f, L.active && valid);
+  accumulate_tile<T, NW>(s_acc, dg, L.a, L.b, L.c, L.f, L.active && valid);
   write_tile<T, NW>(A, b, s_acc, s_y, 2);
 }
 
