@@ -162,6 +162,43 @@ int p3d_a11_apply_host_noalloc(p3d_op *op, const double *x_host, double *y_host)
 int p3d_mg_prolong(int prec, int cnx, int cny, int cnz, int ndof, const void *xc, void *xf, void *stream);
 int p3d_mg_restrict(int prec, int cnx, int cny, int cnz, int ndof, const void *xf, void *xc, void *stream);
 
+/* ------------------------------- material points -> Gauss points ---- */
+/* Viscosity and density of material points (markers) onto the 27 Gauss
+ * points of every element of one whole mx*my*mz mesh, by the projection types
+ * of the reference's rheology update (coefficient_projection_type in
+ * pTatin_EvaluateRheologyNonlinearities, src/rheology.c:150-185):
+ *   P3D_PROJ_NULL            keep the Gauss-point values (case -1)
+ *   P3D_PROJ_P0_ARITHMETIC   element average of the markers' eta (arithmetic,
+ *   P3D_PROJ_P0_HARMONIC     harmonic or geometric) and of rho (arithmetic) on
+ *   P3D_PROJ_P0_GEOMETRIC    all 27 points; an element without markers gets
+ *                            0/0 (MPntPStokesProj_P0,
+ *                            src/material_point_utils.c:2567-2808)
+ *   P3D_PROJ_Q1              nodal average on the Q2 lattice (Q1 weights at
+ *                            the element corners, 1 at the other Q2 nodes;
+ *                            nodes without weight get 0), then Q1
+ *                            interpolation of the corners clamped to the
+ *                            element's nodal range
+ *                            (SwarmUpdateGaussPropertiesLocalL2Projection_Q1_MPntPStokes,
+ *                            src/material_point_utils.c:604-891)
+ *   P3D_PROJ_ONE2ONE         marker p is Gauss point p, n == 27*nel
+ *                            (SwarmUpdateGaussPropertiesOne2OneMap_MPntPStokes, :803-840)
+ * Markers (device arrays, the fields of MPntStd / MPntPStokes): wil[n]
+ * element index (x fastest; markers outside [0, nel) are skipped), xi[3n]
+ * local coordinates in [-1,1]^3 (Q1 only), eta_p[n], rho_p[n].  Output:
+ * eta_q, rho_q [27*nel] device arrays (element-major, q = qi + 3qj + 9qk).
+ * `workspace`: device memory of p3d_marker_project_workspace bytes, 8-byte
+ * aligned (may be NULL when that is 0).  Asynchronous on `stream`. */
+#define P3D_PROJ_NULL (-1)
+#define P3D_PROJ_P0_ARITHMETIC 0
+#define P3D_PROJ_Q1 1
+#define P3D_PROJ_ONE2ONE 4
+#define P3D_PROJ_P0_HARMONIC 10
+#define P3D_PROJ_P0_GEOMETRIC 20
+int p3d_marker_project_workspace(int32_t mx, int32_t my, int32_t mz, int type, int64_t *bytes);
+int p3d_marker_project(int32_t mx, int32_t my, int32_t mz, int type, int64_t n, const int32_t *wil, const double *xi,
+                       const double *eta_p, const double *rho_p, double *eta_q, double *rho_q, void *workspace,
+                       void *stream);
+
 /* ------------------------------------------------------ Stokes solve --- */
 /* Device-resident solve of the Q2-P1disc Stokes system on one whole mesh:
  * outer FGMRES (FP64 residual and orthogonalisation) right-preconditioned by

@@ -1,10 +1,13 @@
 """ctypes front end of the CPU oracle (TEST INFRASTRUCTURE ONLY).
 
 Two independent checkers, both plain CPU code:
-  * ``Restatement`` -- oracle/liboracle.so, the C restatement in q2_oracle.c;
+  * ``Restatement`` -- oracle/liboracle.so, the C restatement in q2_oracle.c
+    (and ``marker_project``, a numpy restatement of the material-point
+    projections);
   * ``Reference``   -- oracle/_ref/libp3dref.so, the reference's own element
-    kernels (stokes_operators_{tensor,avx,mf}.c, element_utils_q2.c) compiled
-    unmodified against oracle/shim by ``make -C oracle ref``.
+    kernels (stokes_operators_{tensor,avx,mf}.c, element_utils_q2.c) and
+    material-point projections (material_point_utils.c, quadrature.c)
+    compiled unmodified against oracle/shim by ``make -C oracle ref``.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 module.  The product (ptatin3d_b200) never imports it.
@@ -140,6 +143,7 @@ class Reference:
         L.ref_a12_avx.argtypes = [_dp, _dp]
         L.ref_a_avx.argtypes = [_dp] * 4
         L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_marker_project.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int32), _dp, _dp, _dp, _dp, _dp]
         self.L = L
         self.dims = None
 
@@ -183,6 +187,22 @@ class Reference:
         assert self.L.ref_a12_avx(_p(np.ascontiguousarray(p, dtype=np.float64)), _p(y)) == 0
         return y
 
+    def marker_project(self, ptype, wil, xi, eta_p, rho_p, eta_q=None, rho_q=None):
+        """Gauss-point (eta, rho) [27*nel] of the mesh given to setup() from
+        markers, by the reference's projection ``ptype`` (src/rheology.c:150-185);
+        eta_q / rho_q are the values on the Gauss points before the update."""
+        nq = 27 * self.dims[0] * self.dims[1] * self.dims[2]
+        eq = np.zeros(nq) if eta_q is None else np.array(eta_q, dtype=np.float64).reshape(-1)
+        rq = np.zeros(nq) if rho_q is None else np.array(rho_q, dtype=np.float64).reshape(-1)
+        w = np.ascontiguousarray(wil, dtype=np.int32)
+        x = None if xi is None else np.ascontiguousarray(xi, dtype=np.float64).reshape(-1)
+        rc = self.L.ref_marker_project(int(ptype), int(w.size), w.ctypes.data_as(C.POINTER(C.c_int32)),
+                                       None if x is None else _p(x),
+                                       _p(np.ascontiguousarray(eta_p, dtype=np.float64)),
+                                       _p(np.ascontiguousarray(rho_p, dtype=np.float64)), _p(eq), _p(rq))
+        assert rc == 0, rc
+        return eq, rq
+
     def stokes_avx_raw(self, u, p):
         """MFStokesWrapper_A_AVX: [A11 u + A12 p; A21 u] without boundary conditions."""
         yu = np.zeros(self._coords.size)
@@ -190,6 +210,89 @@ class Reference:
         assert self.L.ref_a_avx(_p(np.ascontiguousarray(u, dtype=np.float64)), _p(np.ascontiguousarray(p, dtype=np.float64)),
                                 _p(yu), _p(yp)) == 0
         return yu, yp
+
+
+# ------------------------------------------- material points -> Gauss points ---
+# the reference's 3-point Gauss rule as it builds the volume quadrature, with
+# 15-digit constants (QuadratureCreateGauss_3pnt_3D, src/quadrature.c:121-147)
+_GP15 = np.array([-0.774596669241483, 0.0, 0.774596669241483])
+
+
+def _q1_corner_weights(xi):
+    """[..., 8] Q1 weights 0.125 (1 -+ xi)(1 -+ eta)(1 -+ zeta), corner bits (x, y, z)
+    (pTatinConstructNI_Q1_3D, src/material_point_utils.c:502-519)."""
+    xi = np.asarray(xi, dtype=np.float64)
+    out = []
+    for c in range(8):
+        w = 0.125 * (1.0 + xi[..., 0] if c & 1 else 1.0 - xi[..., 0])
+        w = w * (1.0 + xi[..., 1] if c & 2 else 1.0 - xi[..., 1])
+        w = w * (1.0 + xi[..., 2] if c & 4 else 1.0 - xi[..., 2])
+        out.append(w)
+    return np.stack(out, axis=-1)
+
+
+def _element_nodes(dims):
+    """[nel, 27] lattice node index of every element node (x fastest)."""
+    mx, my, mz = dims
+    nx, ny = 2 * mx + 1, 2 * my + 1
+    e = np.arange(mx * my * mz)
+    ex, ey, ez = e % mx, (e // mx) % my, e // (mx * my)
+    n = np.arange(27)
+    a, b, c = n % 3, (n // 3) % 3, n // 9
+    return (2 * ex[:, None] + a) + nx * ((2 * ey[:, None] + b) + ny * (2 * ez[:, None] + c))
+
+
+_CORNER_NODES = np.array([0, 2, 6, 8, 18, 20, 24, 26])
+
+
+def marker_project(dims, ptype, wil, xi, eta_p, rho_p, eta_q=None, rho_q=None):
+    """Numpy restatement of the projection types of src/rheology.c:150-185 on a
+    whole mesh: -1 keep, 0/10/20 P0 arithmetic/harmonic/geometric
+    (src/material_point_utils.c:2567-2808), 1 Q1 (:604-801), 4 one-to-one
+    (:803-840).  Returns Gauss-point (eta, rho) [27*nel]."""
+    mx, my, mz = dims
+    nel = mx * my * mz
+    eq = np.zeros(27 * nel) if eta_q is None else np.array(eta_q, dtype=np.float64).reshape(-1)
+    rq = np.zeros(27 * nel) if rho_q is None else np.array(rho_q, dtype=np.float64).reshape(-1)
+    w = np.asarray(wil, dtype=np.int64)
+    ve, vr = np.asarray(eta_p, dtype=np.float64), np.asarray(rho_p, dtype=np.float64)
+    if ptype == -1:
+        return eq, rq
+    if ptype == 4:
+        assert w.size == 27 * nel
+        return ve.copy(), vr.copy()
+    if ptype in (0, 10, 20):
+        f = {0: ve, 10: 1.0 / ve, 20: np.log(ve)}[ptype]
+        S, cnt, R = np.zeros(nel), np.zeros(nel), np.zeros(nel)
+        np.add.at(S, w, f)
+        np.add.at(cnt, w, 1.0)
+        np.add.at(R, w, vr)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            avg = {0: S / cnt, 10: cnt / S, 20: np.exp(S / cnt)}[ptype]
+            return np.repeat(avg, 27), np.repeat(R / cnt, 27)
+    if ptype != 1:
+        raise ValueError(f"projection type {ptype} not supported")
+    nn = (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1)
+    nodes = _element_nodes(dims)
+    A1, A2, B = np.zeros(nn), np.zeros(nn), np.zeros(nn)
+    Nw = np.ones((w.size, 27))
+    Nw[:, _CORNER_NODES] = _q1_corner_weights(np.asarray(xi, dtype=np.float64).reshape(-1, 3))
+    g = nodes[w]
+    np.add.at(A1, g, Nw * ve[:, None])
+    np.add.at(A2, g, Nw * vr[:, None])
+    np.add.at(B, g, Nw)
+    nz = B != 0.0
+    V1, V2 = np.zeros(nn), np.zeros(nn)
+    V1[nz], V2[nz] = A1[nz] / B[nz], A2[nz] / B[nz]
+    q = np.arange(27)
+    xq = np.stack([_GP15[q % 3], _GP15[(q // 3) % 3], _GP15[q // 9]], axis=-1)
+    Nq = _q1_corner_weights(xq)  # [27 points, 8 corners]
+    out = []
+    for V in (V1, V2):
+        Ve = V[nodes]
+        vals = Ve[:, _CORNER_NODES] @ Nq.T
+        out.append(np.clip(vals, Ve.min(axis=1)[:, None], Ve.max(axis=1)[:, None]).reshape(-1))
+    return out[0], out[1]
 
 
 # --------------------------------------------------- MatMult conventions ---

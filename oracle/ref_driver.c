@@ -10,6 +10,9 @@
  *   ref_a11(variant, x[3*nn], y[3*nn])   variant 0=tensor 1=avx 2=ref 3=low-order (MFStokesWrapper_A11PC)
  *   ref_diag(y[3*nn]), ref_a12(p[4*nel], yu[3*nn]), ref_a21(u[3*nn], yp[4*nel]),
  *   ref_a12_avx(p, yu), ref_a_avx(u, p, yu, yp)
+ *   ref_marker_project(type, n, wil, xi, eta_p, rho_p, eta_q, rho_q)
+ *       the material-point -> Gauss-point projections of the rheology update
+ *       (src/rheology.c:150-185; material_point_utils.c, quadrature.c)
  *
  * Each adds element contributions exactly as the reference's SpMVOp_MatMult
  * callback does (the caller zeroes y and applies Dirichlet rows/columns).
@@ -26,6 +29,9 @@
 #include "private/ptatin_impl.h"
 #include "ptatin3d_stokes.h"
 #include "stokes_operators.h"
+#include "MPntStd_def.h"
+#include "MPntPStokes_def.h"
+#include "material_point_utils.h"
 
 /* kernels provided by the reference objects */
 PetscErrorCode MFStokesWrapper_A11_Tensor(MatA11MF, Quadrature, DM, PetscScalar[], PetscScalar[]);
@@ -37,6 +43,9 @@ PetscErrorCode MFStokesWrapper_A12(Quadrature, DM, DM, PetscScalar[], PetscScala
 PetscErrorCode MFStokesWrapper_A21(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
 PetscErrorCode MFStokesWrapper_A12_AVX(Quadrature, DM, DM, PetscScalar[], PetscScalar[]);
 PetscErrorCode MFStokesWrapper_A_AVX(Quadrature, DM, PetscScalar[], DM, PetscScalar[], PetscScalar[], PetscScalar[]);
+/* projections provided by the reference objects (material_point_utils.c, quadrature.c) */
+PetscErrorCode MPntPStokesProj_P0(CoefficientAveragingType, const int, MPntStd[], MPntPStokes[], DM, Quadrature);
+void QuadratureCreateGauss_3pnt_3D(PetscInt *ngp, PetscReal **q_coor, PetscReal **q_weight);
 
 struct _p_shim_Vec {
   PetscScalar *a;
@@ -48,11 +57,13 @@ struct _p_shim_DM {
   PetscInt nel, npe;
   PetscInt *e;
   struct _p_shim_Vec coords;
+  int clone; /* made by DMDADuplicateLayout: shares e and coords, freed by DMDestroy */
 };
 
 static struct _p_shim_DM g_dau, g_dap;
 static struct _p_Quadrature g_Q;
 static QPntVolCoefStokes *g_cells = NULL;
+static PetscReal *g_qxi = NULL, *g_qw = NULL;
 
 /* ---------------------------------------------------------- accessors --- */
 PetscErrorCode PetscPrintf(MPI_Comm c, const char fmt[], ...) { (void)c; (void)fmt; return 0; }
@@ -182,6 +193,102 @@ PetscErrorCode DMDAGetScalarElementField(PetscScalar elfield[], PetscInt npe, Pe
   return 0;
 }
 
+/* DM / Vec calls of the material-point projections, for one process owning
+ * the whole lattice (local vectors = global vectors, no ghosts) */
+PetscErrorCode DMDADuplicateLayout(DM da1, PetscInt dof2, PetscInt sw2, DMDAStencilType st2, DM *da2)
+{
+  (void)st2;
+  DM d = (DM)malloc(sizeof(*d));
+  if (!d) return PETSC_ERR_MEM;
+  *d = *da1;
+  d->dof = dof2;
+  d->sw = sw2;
+  d->clone = 1;
+  *da2 = d;
+  return 0;
+}
+PetscErrorCode DMDestroy(DM *dm)
+{
+  if (dm && *dm && (*dm)->clone) free(*dm);
+  if (dm) *dm = NULL;
+  return 0;
+}
+PetscErrorCode DMDASetElementType_Q2(DM dm) { (void)dm; return 0; }
+PetscErrorCode DMDAGetRefinementFactor(DM dm, PetscInt *rx, PetscInt *ry, PetscInt *rz)
+{
+  (void)dm;
+  if (rx) *rx = 2;
+  if (ry) *ry = 2;
+  if (rz) *rz = 2;
+  return 0;
+}
+PetscErrorCode DMDAGetLocalSizeElementQ2(DM dm, PetscInt *mx, PetscInt *my, PetscInt *mz)
+{
+  if (mx) *mx = (dm->M - 1) / 2;
+  if (my) *my = (dm->N - 1) / 2;
+  if (mz) *mz = (dm->P - 1) / 2;
+  return 0;
+}
+static PetscErrorCode shim_vec_new(DM dm, Vec *v)
+{
+  Vec x = (Vec)malloc(sizeof(*x));
+  if (!x) return PETSC_ERR_MEM;
+  x->n = (long)dm->dof * dm->M * dm->N * dm->P;
+  x->a = (PetscScalar *)calloc((size_t)x->n, sizeof(PetscScalar));
+  *v = x;
+  return x->a ? 0 : PETSC_ERR_MEM;
+}
+static PetscErrorCode shim_vec_free(Vec *v)
+{
+  if (v && *v) {
+    free((*v)->a);
+    free(*v);
+    *v = NULL;
+  }
+  return 0;
+}
+PetscErrorCode DMGetGlobalVector(DM dm, Vec *v) { return shim_vec_new(dm, v); }
+PetscErrorCode DMGetLocalVector(DM dm, Vec *v) { return shim_vec_new(dm, v); }
+PetscErrorCode DMRestoreGlobalVector(DM dm, Vec *v) { (void)dm; return shim_vec_free(v); }
+PetscErrorCode DMRestoreLocalVector(DM dm, Vec *v) { (void)dm; return shim_vec_free(v); }
+PetscErrorCode PetscObjectSetName(PetscObject o, const char name[]) { (void)o; (void)name; return 0; }
+PetscErrorCode VecZeroEntries(Vec v)
+{
+  memset(v->a, 0, sizeof(PetscScalar) * (size_t)v->n);
+  return 0;
+}
+PetscErrorCode DMLocalToGlobalBegin(DM dm, Vec l, InsertMode mode, Vec g)
+{
+  (void)dm;
+  for (long i = 0; i < g->n; i++) g->a[i] = (mode == ADD_VALUES) ? g->a[i] + l->a[i] : l->a[i];
+  return 0;
+}
+PetscErrorCode DMLocalToGlobalEnd(DM dm, Vec l, InsertMode mode, Vec g) { (void)dm; (void)l; (void)mode; (void)g; return 0; }
+PetscErrorCode DMGlobalToLocalBegin(DM dm, Vec g, InsertMode mode, Vec l)
+{
+  (void)dm; (void)mode;
+  memcpy(l->a, g->a, sizeof(PetscScalar) * (size_t)l->n);
+  return 0;
+}
+PetscErrorCode DMGlobalToLocalEnd(DM dm, Vec g, InsertMode mode, Vec l) { (void)dm; (void)g; (void)mode; (void)l; return 0; }
+/* PETSc's VecPointwiseDivide sets w_i = 0 where y_i = 0 */
+PetscErrorCode VecPointwiseDivide(Vec w, Vec x, Vec y)
+{
+  for (long i = 0; i < w->n; i++) w->a[i] = (y->a[i] != 0.0) ? x->a[i] / y->a[i] : 0.0;
+  return 0;
+}
+PetscErrorCode Q2GetElementLocalIndicesDOF(PetscInt idx[], PetscInt ndof, PetscInt elnid[])
+{
+  for (int d = 0; d < ndof; d++)
+    for (int n = 0; n < 27; n++) idx[ndof * n + d] = ndof * elnid[n] + d;
+  return 0;
+}
+PetscErrorCode DMDASetValuesLocalStencil_AddValues_DOF(PetscScalar *F, PetscInt ndof, PetscInt eqn[], PetscScalar Fe[])
+{
+  for (int k = 0; k < 27 * ndof; k++) F[eqn[k]] += Fe[k];
+  return 0;
+}
+
 /* ------------------------------------------------------------- entry --- */
 void ref_teardown(void)
 {
@@ -189,6 +296,8 @@ void ref_teardown(void)
   free(g_dap.e); g_dap.e = NULL;
   free(g_dau.coords.a); g_dau.coords.a = NULL;
   free(g_cells); g_cells = NULL;
+  free(g_qxi); g_qxi = NULL;
+  free(g_qw); g_qw = NULL;
 }
 
 /* Build the one-process mesh: node lattice (2mx+1)x(2my+1)x(2mz+1), the
@@ -226,6 +335,10 @@ int ref_setup(int mx, int my, int mz, const double *coords, const double *eta)
   memset(&g_Q, 0, sizeof g_Q);
   g_Q.dim = 3; g_Q.type = VOLUME_QUAD; g_Q.npoints = 27; g_Q.n_elements = (PetscInt)nel;
   g_Q.shim_cells = g_cells;
+  PetscInt ngp = 0;
+  QuadratureCreateGauss_3pnt_3D(&ngp, &g_qxi, &g_qw); /* the Gauss rule of the volume quadrature */
+  g_Q.q_xi_coor = g_qxi;
+  g_Q.q_weight = g_qw;
   return 0;
 }
 
@@ -246,5 +359,43 @@ int ref_a21(double *u, double *yp) { return MFStokesWrapper_A21(&g_Q, &g_dau, &g
  * MatMult_MFStokes_A call when __AVX__ is defined, src/stokes_operators.c:927,1323) */
 int ref_a12_avx(double *p, double *yu) { return MFStokesWrapper_A12_AVX(&g_Q, &g_dau, &g_dap, p, yu); }
 int ref_a_avx(double *u, double *p, double *yu, double *yp) { return MFStokesWrapper_A_AVX(&g_Q, &g_dau, u, &g_dap, p, yu, yp); }
+/* Gauss-point eta / rho [27*nel] from n markers by the reference's projection
+ * `type` (-1 none, 0/10/20 P0 arithmetic/harmonic/geometric, 1 Q1, 4 one-to-one;
+ * src/rheology.c:150-185).  eta_q / rho_q hold the current values on entry. */
+int ref_marker_project(int type, int n, const int *wil, const double *xi, const double *eta_p, const double *rho_p,
+                       double *eta_q, double *rho_q)
+{
+  const long nq = (long)g_Q.n_elements * 27;
+  for (long k = 0; k < nq; k++) {
+    g_cells[k].eta = eta_q[k];
+    g_cells[k].rho = rho_q[k];
+  }
+  MPntStd *std = (MPntStd *)calloc((size_t)(n > 0 ? n : 1), sizeof(MPntStd));
+  MPntPStokes *stk = (MPntPStokes *)calloc((size_t)(n > 0 ? n : 1), sizeof(MPntPStokes));
+  if (!std || !stk) { free(std); free(stk); return PETSC_ERR_MEM; }
+  for (int p = 0; p < n; p++) {
+    std[p].wil = wil[p];
+    if (xi) for (int d = 0; d < 3; d++) std[p].xi[d] = xi[3 * p + d];
+    stk[p].eta = eta_p[p];
+    stk[p].rho = rho_p[p];
+  }
+  int rc;
+  switch (type) {
+  case -1: rc = 0; break;
+  case 0: rc = MPntPStokesProj_P0(CoefAvgARITHMETIC, n, std, stk, &g_dau, &g_Q); break;
+  case 10: rc = MPntPStokesProj_P0(CoefAvgHARMONIC, n, std, stk, &g_dau, &g_Q); break;
+  case 20: rc = MPntPStokesProj_P0(CoefAvgGEOMETRIC, n, std, stk, &g_dau, &g_Q); break;
+  case 1: rc = SwarmUpdateGaussPropertiesLocalL2Projection_Q1_MPntPStokes(n, std, stk, &g_dau, &g_Q); break;
+  case 4: rc = SwarmUpdateGaussPropertiesOne2OneMap_MPntPStokes(n, std, stk, &g_Q); break;
+  default: rc = PETSC_ERR_SUP;
+  }
+  for (long k = 0; k < nq; k++) {
+    eta_q[k] = g_cells[k].eta;
+    rho_q[k] = g_cells[k].rho;
+  }
+  free(std);
+  free(stk);
+  return rc;
+}
 int ref_set_threads(int n) { omp_set_num_threads(n); return 0; }
 int ref_max_threads(void) { return omp_get_max_threads(); }

@@ -1,6 +1,7 @@
 /*
  * Minimal PETSc stand-in used ONLY to compile the reference's element-kernel
- * sources (stokes_operators_{tensor,avx,mf}.c, element_utils_q2.c) into the
+ * sources (stokes_operators_{tensor,avx,mf}.c, element_utils_q2.c) and its
+ * material-point projections (material_point_utils.c, quadrature.c) into the
  * CPU oracle under oracle/_ref.  Nothing here is PETSc; it declares just the
  * types, macros and accessor functions those files name.  The accessors are
  * implemented by oracle/ref_driver.c over plain arrays.
@@ -56,7 +57,8 @@ typedef enum { DM_BOUNDARY_NONE } DMBoundaryType;
 typedef enum { INSERT_VALUES, ADD_VALUES } InsertMode;
 typedef enum { PETSC_ERR_SUP = 56, PETSC_ERR_ARG_SIZ = 60, PETSC_ERR_ARG_WRONG = 62,
                PETSC_ERR_ARG_CORRUPT = 64, PETSC_ERR_USER = 83, PETSC_ERR_ARG_NULL = 85,
-               PETSC_ERR_MEM = 55, PETSC_ERR_ARG_OUTOFRANGE = 63 } PetscErrorCodeEnum;
+               PETSC_ERR_MEM = 55, PETSC_ERR_ARG_OUTOFRANGE = 63, PETSC_ERR_LIB = 76 } PetscErrorCodeEnum;
+typedef enum { PETSC_VIEWER_DEFAULT = 0, PETSC_VIEWER_ASCII_VTK } PetscViewerFormat;
 
 #define PETSC_EXTERN extern
 #define PETSC_STATIC_INLINE static inline

@@ -23,6 +23,7 @@ MAX_RESTART = 120
 COARSE_MAX_DOFS = 16384
 GEOM_AUTO, GEOM_GENERAL, GEOM_AFFINE = 0, 1, 2
 BC_NONE, BC_MATMULT = 0, 1
+PROJ_NULL, PROJ_P0_ARITHMETIC, PROJ_Q1, PROJ_ONE2ONE, PROJ_P0_HARMONIC, PROJ_P0_GEOMETRIC = -1, 0, 1, 4, 10, 20
 FACE_IMIN, FACE_IMAX, FACE_JMIN, FACE_JMAX, FACE_KMIN, FACE_KMAX = range(6)
 
 
@@ -116,6 +117,8 @@ _SIGS = {
     "p3d_a11_apply_host_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_mg_prolong": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_mg_restrict": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_marker_project_workspace": ([C.c_int32, C.c_int32, C.c_int32, C.c_int, C.POINTER(C.c_int64)], C.c_int),
+    "p3d_marker_project": ([C.c_int32, C.c_int32, C.c_int32, C.c_int, C.c_int64] + [C.c_void_p] * 8, C.c_int),
 }
 
 

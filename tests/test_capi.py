@@ -83,3 +83,25 @@ def test_solver_options_defaults_and_checks():
     assert b"dense limit" in L.p3d_last_error()
     o.nlevels, o.schur_eta = 3, 7
     assert L.p3d_solver_create(C.byref(d), C.byref(o), 0, C.byref(h)) == _lib.P3D_ERR_ARG
+
+
+def test_marker_projection_arguments_checked_on_host():
+    """Workspace sizes and argument errors of p3d_marker_project need no device."""
+    L = _lib.lib()
+    nb = C.c_int64()
+    assert L.p3d_marker_project_workspace(3, 2, 4, _lib.PROJ_Q1, C.byref(nb)) == 0
+    assert nb.value == 3 * 7 * 5 * 9 * 8  # three node-lattice fields
+    assert L.p3d_marker_project_workspace(3, 2, 4, _lib.PROJ_P0_GEOMETRIC, C.byref(nb)) == 0
+    assert nb.value == 3 * 24 * 8  # three sums per element
+    assert L.p3d_marker_project_workspace(3, 2, 4, _lib.PROJ_ONE2ONE, C.byref(nb)) == 0 and nb.value == 0
+    assert L.p3d_marker_project_workspace(3, 2, 4, 2, C.byref(nb)) == _lib.P3D_ERR_ARG  # Q2: not supported
+    assert L.p3d_marker_project(3, 2, 4, _lib.PROJ_NULL, 0, *([None] * 8)) == 0
+    assert L.p3d_marker_project(3, 2, 4, 3, 0, *([None] * 8)) == _lib.P3D_ERR_ARG
+    assert b"unknown projection type" in L.p3d_last_error()
+    buf = (C.c_double * 4)()
+    ptr = C.cast(buf, C.c_void_p)
+    assert L.p3d_marker_project(3, 2, 4, _lib.PROJ_ONE2ONE, 5, ptr, None, ptr, ptr, ptr, ptr, None, None) \
+        == _lib.P3D_ERR_ARG
+    assert b"27 markers per element" in L.p3d_last_error()
+    assert L.p3d_marker_project(3, 2, 4, _lib.PROJ_Q1, 5, ptr, None, ptr, ptr, ptr, ptr, ptr, None) \
+        == _lib.P3D_ERR_ARG  # Q1 needs xi
