@@ -336,6 +336,69 @@ def solve_c4_leg(device, coords, m=96, seed=4):
             "p_diff_mixed_vs_fp64": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))}
 
 
+def lattice_markers(m, per_dir=2, seed=5):
+    """per_dir^3 markers per element of an m^3 mesh, element-major (the
+    reference's lattice layout of new markers), local coordinates jittered by
+    +-0.25 around the lattice sites, log10 eta uniform in [-3, 3], rho ~ 1."""
+    rng = np.random.default_rng(seed)
+    nel, k = m ** 3, per_dir ** 3
+    s = (np.arange(per_dir) + 0.5) * (2.0 / per_dir) - 1.0
+    site = np.stack(np.meshgrid(s, s, s, indexing="ij")[::-1], axis=-1).reshape(-1, 3)
+    xi = np.clip(np.tile(site, (nel, 1)) + rng.uniform(-0.25, 0.25, size=(nel * k, 3)), -1.0, 1.0)
+    wil = np.repeat(np.arange(nel, dtype=np.int32), k)
+    return wil, xi, 10.0 ** rng.uniform(-3.0, 3.0, size=nel * k), rng.uniform(0.99, 1.01, size=nel * k)
+
+
+def markers_leg(device, m=96, per_dir=2, reps=10, cpu_m=48):
+    """Material points onto Gauss points (p3d_marker_project) for the P0
+    geometric and Q1 projections on an m^3 mesh, device-timed with CUDA
+    events; beside it the reference's own compiled projection on a bounded
+    cpu_m^3 sample, one host thread."""
+    import torch
+
+    from ptatin3d_b200.markers import PROJ_P0_GEOMETRIC, PROJ_Q1, update_gauss_properties
+    wil, xi, eta, rho = lattice_markers(m, per_dir)
+    n = wil.size
+    dev = torch.device("cuda", device)
+    w, x = torch.from_numpy(wil).to(dev), torch.from_numpy(xi).to(dev)
+    e, r = torch.from_numpy(eta).to(dev), torch.from_numpy(rho).to(dev)
+    eq = torch.empty(m ** 3, 27, dtype=torch.float64, device=dev)
+    rq = torch.empty_like(eq)
+    out = {"workload": f"{n} markers ({per_dir}^3 per element, element-major) on a {m}^3 mesh", "markers": n}
+    st = torch.cuda.current_stream()
+    for name, t in (("p0_geometric", PROJ_P0_GEOMETRIC), ("q1", PROJ_Q1)):
+        for _ in range(3):
+            update_gauss_properties((m, m, m), t, w, x, e, r, eq, rq)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(st)
+        for _ in range(reps):
+            update_gauss_properties((m, m, m), t, w, x, e, r, eq, rq)
+        t1.record(st)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1) / reps
+        out[name] = {"ms": ms, "Gmarkers/s": n / (ms * 1e-3) / 1e9}
+    try:
+        from oracle.oracle import Reference, build
+        if not Reference.available():
+            build()
+        from ptatin3d_b200 import mesh as M
+        cw, cx, ce, cr = lattice_markers(cpu_m, per_dir)
+        R = Reference()
+        R.setup((cpu_m,) * 3, M.uniform_coords(cpu_m, cpu_m, cpu_m), np.ones(27 * cpu_m ** 3))
+        cpu = {"kind": "reference", "cores": 1,
+               "sample": f"the reference's compiled projection, {cw.size} markers on a {cpu_m}^3 mesh, 1 thread"}
+        for name, t in (("p0_geometric", 20), ("q1", 1)):
+            t0 = time.perf_counter()
+            R.marker_project(t, cw, cx, ce, cr)
+            cpu[name] = {"s": time.perf_counter() - t0}
+            cpu[name]["Gmarkers/s"] = cw.size / cpu[name]["s"] / 1e9
+        out["cpu_baseline"] = cpu
+    except Exception as exc:  # reported, not required
+        out["cpu_baseline"] = {"failed": str(exc)}
+    return out
+
+
 SERVE_SIZES = (8, 12, 16, 24, 32, 48)
 
 
@@ -582,6 +645,12 @@ def run_b200(args):
     serving = None
     if rank == 0 and args.serve_requests > 0:
         serving = serve_leg(local, args.serve_requests)
+    markers = None
+    if rank == 0 and not args.no_markers:
+        try:
+            markers = markers_leg(local, m)
+        except Exception as exc:  # reported, not required
+            markers = {"failed": str(exc)}
 
     if rank == 0:
         line = {"metric": metric_name(m, wl["kind"]), "value": value, "unit": UNIT, "n_gpus": world,
@@ -603,7 +672,8 @@ def run_b200(args):
                 "fp64_alu": {"flop_per_element": REF_FLOPS_PER_EL,
                              "TFLOP/s": REF_FLOPS_PER_EL * m ** 3 / (kern_ms * 1e-3) / 1e12},
                 "solve": solve,
-                "serving": serving}
+                "serving": serving,
+                "markers": markers}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -714,6 +784,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-solve", action="store_true", help="skip the FP64 vs mixed-precision Stokes solve leg")
     ap.add_argument("--serve-requests", type=int, default=32, help="requests of the served-stream leg (0: skip)")
+    ap.add_argument("--no-markers", action="store_true", help="skip the marker-projection leg")
     ap.add_argument("--slabs", action="store_true", help="run the multi-GPU z-slab path on a single rank")
     ap.add_argument("--size", type=int, default=96, help="elements per direction")
     ap.add_argument("--workload", default="deformed", choices=["deformed", "layered"])
