@@ -24,7 +24,7 @@ import torch
 
 from ._lib import (PROJ_NULL, PROJ_ONE2ONE, PROJ_P0_ARITHMETIC, PROJ_P0_GEOMETRIC, PROJ_P0_HARMONIC, PROJ_Q1,
                    check, lib)
-from .operators import _ptr, _stream
+from .operators import _check_size, _ptr, _stream
 
 __all__ = ["update_gauss_properties", "PROJ_NULL", "PROJ_P0_ARITHMETIC", "PROJ_P0_HARMONIC", "PROJ_P0_GEOMETRIC",
            "PROJ_Q1", "PROJ_ONE2ONE"]
@@ -42,13 +42,16 @@ def update_gauss_properties(m, projection_type, wil, xi, eta_p, rho_p, eta_q=Non
         eta_q = torch.zeros(nel, 27, dtype=torch.float64, device=dev)
     if rho_q is None:
         rho_q = torch.zeros(nel, 27, dtype=torch.float64, device=dev)
-    if wil.dtype != torch.int32 or eta_p.dtype != torch.float64 or rho_p.dtype != torch.float64:
-        raise TypeError("markers: wil int32, eta/rho float64")
     n = wil.numel()
     nb = C.c_int64()
     check(lib().p3d_marker_project_workspace(mx, my, mz, projection_type, C.byref(nb)))
     ws = torch.empty(max(1, nb.value // 8), dtype=torch.float64, device=dev)
     xc = xi.contiguous() if xi is not None else None  # kept alive until the launch is queued
-    check(lib().p3d_marker_project(mx, my, mz, projection_type, n, _ptr(wil), _ptr(xc) if xc is not None else None,
+    for t, k, dt, name in ((wil, n, torch.int32, "wil"), (xc, 3 * n, torch.float64, "xi"),
+                           (eta_p, n, torch.float64, "eta_p"), (rho_p, n, torch.float64, "rho_p"),
+                           (eta_q, 27 * nel, torch.float64, "eta_q"), (rho_q, 27 * nel, torch.float64, "rho_q")):
+        if t is not None:
+            _check_size(t, k, dt, name)
+    check(lib().p3d_marker_project(mx, my, mz, projection_type, n, _ptr(wil), None if xc is None else _ptr(xc),
                                    _ptr(eta_p), _ptr(rho_p), _ptr(eta_q), _ptr(rho_q), _ptr(ws), _stream()))
     return eta_q, rho_q

@@ -38,6 +38,19 @@ def _stream():
     return C.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+def _check_size(t: torch.Tensor, n: int, dtype, name: str):
+    """Raise unless t holds exactly n elements of dtype (the library reads or
+    writes n elements through its pointer)."""
+    if t.dtype != dtype or t.numel() != n:
+        raise _lib.P3DError(_lib.P3D_ERR_ARG, f"{name}: expected {n} x {dtype}, got {t.numel()} x {t.dtype}")
+
+
+def _sized(t: torch.Tensor, n: int, dtype, name: str):
+    """Pointer of a contiguous CUDA tensor of exactly n elements of dtype."""
+    _check_size(t, n, dtype, name)
+    return _ptr(t)
+
+
 def mesh_desc_whole(mx, my, mz, dirichlet=0) -> MeshDesc:
     d = MeshDesc()
     check(lib().p3d_mesh_desc_whole(mx, my, mz, dirichlet, C.byref(d)))
@@ -61,16 +74,19 @@ class _Op:
 
     def set_coefficients(self, coords, eta, geom=GEOM_AUTO):
         """coords: (3*gx*gy*gz,) float64, eta: (nel*27,) float64 -- host numpy or CUDA tensors."""
+        nc = 3 * self.desc.gx * self.desc.gy * self.desc.gz
+        ne = 27 * self.desc.mx * self.desc.my * self.desc.mz
         if isinstance(coords, torch.Tensor) and coords.is_cuda:
             c = coords.to(torch.float64).contiguous()
-            e = eta.to(torch.float64).contiguous()
-            check(lib().p3d_op_set_coefficients_device(self.h, _ptr(c), _ptr(e), geom))
+            e = eta.to(device=c.device, dtype=torch.float64).contiguous()
+            check(lib().p3d_op_set_coefficients_device(self.h, _sized(c, nc, torch.float64, "coords"),
+                                                       _sized(e, ne, torch.float64, "eta"), geom))
         else:
             c = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1)
             e = np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)
-            if c.size != 3 * self.desc.gx * self.desc.gy * self.desc.gz:
+            if c.size != nc:
                 raise _lib.P3DError(_lib.P3D_ERR_ARG, f"coords has {c.size} entries")
-            if e.size != 27 * self.desc.mx * self.desc.my * self.desc.mz:
+            if e.size != ne:
                 raise _lib.P3DError(_lib.P3D_ERR_ARG, f"eta has {e.size} entries")
             check(lib().p3d_op_set_coefficients(self.h, c.ctypes.data_as(C.c_void_p),
                                                 e.ctypes.data_as(C.c_void_p), geom))
@@ -85,9 +101,7 @@ class _Op:
         check(lib().p3d_op_set_bc_mode(self.h, mode))
 
     def _vec(self, t, n, name):
-        if t.dtype != self.dtype or t.numel() != n:
-            raise _lib.P3DError(_lib.P3D_ERR_ARG, f"{name}: expected {n} x {self.dtype}, got {t.numel()} x {t.dtype}")
-        return _ptr(t)
+        return _sized(t, n, self.dtype, name)
 
     def destroy(self):
         if getattr(self, "h", None) is not None and self.h.value:
@@ -177,17 +191,33 @@ class MatStokesMF(MatA11MF):
         u_d, p_d, fu_d, fp_d, phi_d = dev(u), dev(p), dev(fu), dev(fp), dev(phi)
         ru = torch.empty(self.n_velocity, dtype=torch.float64, device=self.device)
         rp = torch.empty(self.n_pressure, dtype=torch.float64, device=self.device)
-        ptr = lambda t: None if t is None else _ptr(t)
+        nel = self.desc.mx * self.desc.my * self.desc.mz
+        opt = lambda t, n, name: None if t is None else _sized(t, n, torch.float64, name)
         check(lib().p3d_stokes_residual(self.h, self._vec(u_d, self.n_velocity, "u"), self._vec(p_d, self.n_pressure, "p"),
-                                        ptr(phi_d), ptr(fu_d), ptr(fp_d), _ptr(ru), _ptr(rp), _stream()))
+                                        opt(phi_d, self.n_velocity, "phi"), opt(fu_d, 81 * nel, "fu"),
+                                        opt(fp_d, 27 * nel, "fp"), _ptr(ru), _ptr(rp), _stream()))
         return ru, rp
 
 
+def _transfer_sizes(cn, ndof):
+    nc = ndof * cn[0] * cn[1] * cn[2]
+    nf = ndof * (2 * cn[0] - 1) * (2 * cn[1] - 1) * (2 * cn[2] - 1)
+    return nc, nf
+
+
 def mg_prolong(xc: torch.Tensor, xf: torch.Tensor, cn, ndof=3):
+    """xf = P xc on the node lattice, cn coarse nodes per direction."""
     prec = PREC_F64 if xc.dtype == torch.float64 else PREC_F32
-    check(lib().p3d_mg_prolong(prec, cn[0], cn[1], cn[2], ndof, _ptr(xc), _ptr(xf), _stream()))
+    nc, nf = _transfer_sizes(cn, ndof)
+    _check_size(xf, nf, xc.dtype, "xf")
+    check(lib().p3d_mg_prolong(prec, cn[0], cn[1], cn[2], ndof, _sized(xc, nc, xc.dtype, "xc"),
+                               _sized(xf, nf, xc.dtype, "xf"), _stream()))
 
 
 def mg_restrict(xf: torch.Tensor, xc: torch.Tensor, cn, ndof=3):
+    """xc = P^T xf on the node lattice, cn coarse nodes per direction."""
     prec = PREC_F64 if xf.dtype == torch.float64 else PREC_F32
-    check(lib().p3d_mg_restrict(prec, cn[0], cn[1], cn[2], ndof, _ptr(xf), _ptr(xc), _stream()))
+    nc, nf = _transfer_sizes(cn, ndof)
+    _check_size(xc, nc, xf.dtype, "xc")
+    check(lib().p3d_mg_restrict(prec, cn[0], cn[1], cn[2], ndof, _sized(xf, nf, xf.dtype, "xf"),
+                                _sized(xc, nc, xf.dtype, "xc"), _stream()))

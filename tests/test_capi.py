@@ -105,3 +105,25 @@ def test_marker_projection_arguments_checked_on_host():
     assert b"27 markers per element" in L.p3d_last_error()
     assert L.p3d_marker_project(3, 2, 4, _lib.PROJ_Q1, 5, ptr, None, ptr, ptr, ptr, ptr, ptr, None) \
         == _lib.P3D_ERR_ARG  # Q1 needs xi
+
+
+def test_python_wrappers_refuse_wrong_sizes():
+    """The torch-facing wrappers check every buffer's element count and type
+    before a pointer reaches the library, so a wrong size is an error on the
+    host and never an out-of-bounds access on the device."""
+    import pytest
+    import torch
+
+    from ptatin3d_b200.markers import PROJ_Q1, update_gauss_properties
+    from ptatin3d_b200.operators import mg_prolong
+    wil = torch.zeros(5, dtype=torch.int32)
+    one = torch.ones(5, dtype=torch.float64)
+    with pytest.raises(_lib.P3DError, match="xi"):
+        update_gauss_properties((2, 2, 2), PROJ_Q1, wil, torch.zeros(4, 3, dtype=torch.float64), one, one)
+    with pytest.raises(_lib.P3DError, match="eta_q"):
+        update_gauss_properties((2, 2, 2), PROJ_Q1, wil, torch.zeros(5, 3, dtype=torch.float64), one, one,
+                                torch.zeros(7, 27, dtype=torch.float64), torch.zeros(8, 27, dtype=torch.float64))
+    with pytest.raises(_lib.P3DError, match="wil"):
+        update_gauss_properties((2, 2, 2), PROJ_Q1, wil.long(), torch.zeros(5, 3, dtype=torch.float64), one, one)
+    with pytest.raises(_lib.P3DError, match="xf"):
+        mg_prolong(torch.zeros(3 * 8, dtype=torch.float64), torch.zeros(3 * 26, dtype=torch.float64), (2, 2, 2))
