@@ -14,7 +14,7 @@ import torch
 
 from . import _lib
 from ._lib import PREC_F32, PREC_F64, SolverOpts, SolveStats, check, lib
-from .operators import _ptr, mesh_desc_whole
+from .operators import _check_size, _ptr, mesh_desc_whole
 
 
 def default_opts(**kw) -> SolverOpts:
@@ -48,26 +48,32 @@ class StokesSolver:
         self.np = 4 * mx * my * mz
         self.device = torch.device("cuda", device)
 
-    def _dev(self, a):
+    def _dev(self, a, n=None, name="array"):
+        """FP64 contiguous copy on the solver's device; n: required element count."""
         if isinstance(a, torch.Tensor):
-            return a.to(device=self.device, dtype=torch.float64).contiguous()
-        return torch.tensor(np.ascontiguousarray(a, dtype=np.float64).reshape(-1), device=self.device)
+            t = a.to(device=self.device, dtype=torch.float64).contiguous()
+        else:
+            t = torch.tensor(np.ascontiguousarray(a, dtype=np.float64).reshape(-1), device=self.device)
+        if n is not None:
+            _check_size(t, n, torch.float64, name)
+        return t
 
     def setup(self, coords, eta):
-        c, e = self._dev(coords), self._dev(eta)
+        nel = self.dims[0] * self.dims[1] * self.dims[2]
+        c, e = self._dev(coords, self.nu, "coords"), self._dev(eta, 27 * nel, "eta")
         check(lib().p3d_solver_setup(self.h, _ptr(c), _ptr(e)))
 
     def set_rhs_body_force(self, rho, g=(0.0, 0.0, -1.0)):
-        r = self._dev(rho)
+        r = self._dev(rho, 27 * self.dims[0] * self.dims[1] * self.dims[2], "rho")
         check(lib().p3d_solver_set_rhs_body_force(self.h, _ptr(r), *map(float, g)))
 
     def set_rhs(self, bu, bp):
-        bu_d, bp_d = self._dev(bu), self._dev(bp)  # keep both alive across the call
+        bu_d, bp_d = self._dev(bu, self.nu, "bu"), self._dev(bp, self.np, "bp")  # both alive across the call
         check(lib().p3d_solver_set_rhs(self.h, _ptr(bu_d), _ptr(bp_d)))
 
     def solve(self, u=None, p=None, raise_on_noconv=True):
-        u = torch.zeros(self.nu, dtype=torch.float64, device=self.device) if u is None else self._dev(u)
-        p = torch.zeros(self.np, dtype=torch.float64, device=self.device) if p is None else self._dev(p)
+        u = torch.zeros(self.nu, dtype=torch.float64, device=self.device) if u is None else self._dev(u, self.nu, "u")
+        p = torch.zeros(self.np, dtype=torch.float64, device=self.device) if p is None else self._dev(p, self.np, "p")
         st = SolveStats()
         rc = lib().p3d_solver_solve(self.h, _ptr(u), _ptr(p), C.byref(st))
         if rc != 0 and (raise_on_noconv or rc != _lib.P3D_ERR_NOCONV):
@@ -78,13 +84,15 @@ class StokesSolver:
     def apply_pc(self, ru, rp):
         zu = torch.empty(self.nu, dtype=torch.float64, device=self.device)
         zp = torch.empty(self.np, dtype=torch.float64, device=self.device)
-        ru_d, rp_d = self._dev(ru), self._dev(rp)  # keep both alive across the call
+        ru_d, rp_d = self._dev(ru, self.nu, "ru"), self._dev(rp, self.np, "rp")  # both alive across the call
         check(lib().p3d_solver_apply_pc(self.h, _ptr(ru_d), _ptr(rp_d), _ptr(zu), _ptr(zp)))
         return zu, zp
 
     def level_apply(self, level, x):
         """FP64 velocity operator of multigrid level `level` (0 = coarsest)."""
-        xd = self._dev(x)
+        f = 1 << (self.opts.nlevels - 1 - int(level))
+        n = 3 * (2 * (self.dims[0] // f) + 1) * (2 * (self.dims[1] // f) + 1) * (2 * (self.dims[2] // f) + 1)
+        xd = self._dev(x, n, "x")
         y = torch.empty_like(xd)
         check(lib().p3d_solver_level_apply(self.h, int(level), _ptr(xd), _ptr(y)))
         return y
