@@ -127,3 +127,34 @@ def test_python_wrappers_refuse_wrong_sizes():
         update_gauss_properties((2, 2, 2), PROJ_Q1, wil.long(), torch.zeros(5, 3, dtype=torch.float64), one, one)
     with pytest.raises(_lib.P3DError, match="xf"):
         mg_prolong(torch.zeros(3 * 8, dtype=torch.float64), torch.zeros(3 * 26, dtype=torch.float64), (2, 2, 2))
+
+
+def test_c_caller_links_and_runs(tmp_path):
+    """The header compiles as C99 and a C program links libp3d_b200.so and
+    calls it with plain pointers (the entry points that need no device)."""
+    import shutil
+
+    import pytest
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    exe = str(tmp_path / "capi_host")
+    _lib.lib()  # the CUDA runtime this process resolved for the library
+    maps = open("/proc/self/maps").read().split()
+    cuda_rt = next((os.path.dirname(f) for f in maps if "libcudart.so" in f), None)
+    cmd = ["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "capi_host.c"), "-L", libdir, "-lp3d_b200", f"-Wl,-rpath,{libdir}", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    env = dict(os.environ)
+    if cuda_rt:
+        env["LD_LIBRARY_PATH"] = cuda_rt + ":" + env.get("LD_LIBRARY_PATH", "")
+    out = subprocess.run([exe], capture_output=True, text=True, env=env)
+    assert out.returncode == 0, out.stderr
+    lines = dict(l.split(" ", 1) for l in out.stdout.strip().splitlines())
+    assert lines["desc"] == "0 4 9 7 11 0 0 1 63"
+    assert lines["bad_desc"] == f"{_lib.P3D_ERR_ARG} msg"
+    assert lines["ws_q1"] == f"0 {3 * 9 * 7 * 11 * 8}"
+    assert lines["ws_p0"] == f"0 {3 * 60 * 8}"
+    assert lines["solver"] == "0 4 0 1"
+    assert lines["version"].startswith("p3d_b200")
