@@ -297,6 +297,54 @@ SOLVE_C4_WORKLOAD = ("Stokes solve, Q2-P1disc 96^3 deformed mesh (interior nodes
                      "Galerkin GMG, Chebyshev(3)/Jacobi, rtol 1e-6")
 
 
+SOLVE_C3_WORKLOAD = ("Stokes solve, Q2-P1disc 64^3 unit cube, layered eta (6 layers, log10 eta in [-3,3], 16 "
+                     "inclusions), 8 sinkers of density +1%, g=-z, free slip walls/base, free surface top; FGMRES(30) "
+                     "+ Schur upper (geometric mean) + 5-level Galerkin GMG, Chebyshev(3)/Jacobi, rtol 1e-6, at most "
+                     "{max_it} iterations")
+
+
+def solve_c3_leg(device, m=64, seed=4, max_it=600):
+    """FP64 and mixed-precision solves of the layered 64^3 field (eta over six
+    decades), each bounded to max_it outer iterations: this preconditioner
+    family stagnates on it (the CPU restatement too), so the leg records the
+    residual reached and the time per iteration of both precisions."""
+    import torch
+
+    from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
+    from ptatin3d_b200 import mesh as M
+    from ptatin3d_b200.solver import StokesSolver
+    bits = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
+    c = M.uniform_coords(m, m, m)
+    qp = M.qp_coords(c, m, m, m)
+    eta = M.layered_eta(qp, seed=seed)
+    cen, r = M.random_sinkers(8, 1, 0.1)
+    rho = M.sinker_density(qp, cen, r, 1.0, 1.01)
+    out, sols = {}, {}
+    for name, prec in (("fp64", PREC_F64), ("mixed", PREC_F32)):
+        S = StokesSolver(m, m, m, bits, device=device, nlevels=5, rtol=1e-6, max_it=max_it, mg_precision=prec,
+                         schur_eta=SCHUR_ETA_GEOMEAN)
+        S.setup(c, eta)
+        S.set_rhs_body_force(rho)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, p, st = S.solve(raise_on_noconv=False)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        sols[name] = (u.cpu().numpy(), p.cpu().numpy())
+        out[name] = {"s": dt, "iterations": st["iterations"], "ms_per_iteration": 1e3 * dt / max(1, st["iterations"]),
+                     "converged": bool(st["converged"]), "rel_residual": st["rfinal"] / st["r0"],
+                     "setup_s": st["setup_ms"] * 1e-3}
+        S.destroy()
+        del S, u, p
+        torch.cuda.empty_cache()
+    (u64, p64), (u32, p32) = sols["fp64"], sols["mixed"]
+    return {"workload": SOLVE_C3_WORKLOAD.format(max_it=max_it), "unit": "s", "fp64": out["fp64"],
+            "mixed": out["mixed"],
+            "ms_per_iteration_ratio_fp64_vs_mixed": out["fp64"]["ms_per_iteration"] / out["mixed"]["ms_per_iteration"],
+            "u_diff_mixed_vs_fp64": float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64)),
+            "p_diff_mixed_vs_fp64": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))}
+
+
 def solve_c4_leg(device, coords, m=96, seed=4):
     """FP64 vs mixed-precision solve on the deformed 96^3 mesh of the apply
     benchmark.  The apply's sigma = 2 decades field spans 12 decades of eta,
@@ -642,6 +690,10 @@ def run_b200(args):
                 solve["deformed_96"] = solve_c4_leg(local, wl["coords"])
             except Exception as exc:  # reported, not required
                 solve["deformed_96"] = {"failed": str(exc)}
+            try:
+                solve["layered_64"] = solve_c3_leg(local)
+            except Exception as exc:  # reported, not required
+                solve["layered_64"] = {"failed": str(exc)}
     serving = None
     if rank == 0 and args.serve_requests > 0:
         serving = serve_leg(local, args.serve_requests)
