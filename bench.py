@@ -297,7 +297,7 @@ SOLVE_C4_WORKLOAD = ("Stokes solve, Q2-P1disc 96^3 deformed mesh (interior nodes
                      "Galerkin GMG, Chebyshev(3)/Jacobi, rtol 1e-6")
 
 
-SOLVE_C3_WORKLOAD = ("Stokes solve, Q2-P1disc 64^3 unit cube, layered eta (6 layers, log10 eta in [-3,3], 16 "
+SOLVE_C3_WORKLOAD = ("Stokes solve, Q2-P1disc {m}^3 unit cube, layered eta (6 layers, log10 eta in [-3,3], 16 "
                      "inclusions), 8 sinkers of density +1%, g=-z, free slip walls/base, free surface top; FGMRES(30) "
                      "+ Schur upper (geometric mean) + 5-level Galerkin GMG, Chebyshev(3)/Jacobi, rtol 1e-6, at most "
                      "{max_it} iterations")
@@ -338,7 +338,7 @@ def solve_c3_leg(device, m=64, seed=4, max_it=600):
         del S, u, p
         torch.cuda.empty_cache()
     (u64, p64), (u32, p32) = sols["fp64"], sols["mixed"]
-    return {"workload": SOLVE_C3_WORKLOAD.format(max_it=max_it), "unit": "s", "fp64": out["fp64"],
+    return {"workload": SOLVE_C3_WORKLOAD.format(m=m, max_it=max_it), "unit": "s", "fp64": out["fp64"],
             "mixed": out["mixed"],
             "ms_per_iteration_ratio_fp64_vs_mixed": out["fp64"]["ms_per_iteration"] / out["mixed"]["ms_per_iteration"],
             "u_diff_mixed_vs_fp64": float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64)),
