@@ -5,9 +5,11 @@ Two independent checkers, both plain CPU code:
     (and ``marker_project``, a numpy restatement of the material-point
     projections);
   * ``Reference``   -- oracle/_ref/libp3dref.so, the reference's own element
-    kernels (stokes_operators_{tensor,avx,mf}.c, element_utils_q2.c) and
-    material-point projections (material_point_utils.c, quadrature.c)
-    compiled unmodified against oracle/shim by ``make -C oracle ref``.
+    kernels (stokes_operators_{tensor,avx,mf}.c, element_utils_q2.c),
+    material-point projections (material_point_utils.c, quadrature.c), error
+    norms (inorms.c) and SolCx analytic solution
+    (models/analytics_vv/SolCxSolution.c), compiled unmodified against
+    oracle/shim by ``make -C oracle ref``.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 module.  The product (ptatin3d_b200) never imports it.
@@ -144,6 +146,8 @@ class Reference:
         L.ref_a_avx.argtypes = [_dp] * 4
         L.ref_set_threads.argtypes = [C.c_int]
         L.ref_marker_project.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int32), _dp, _dp, _dp, _dp, _dp]
+        L.ref_solcx_norms.argtypes = [C.c_double] * 3 + [C.c_int] + [_dp] * 3
+        L.ref_solcx_exact.argtypes = [C.c_double] * 3 + [C.c_int] + [_dp] * 3
         self.L = L
         self.dims = None
 
@@ -202,6 +206,26 @@ class Reference:
                                        _p(np.ascontiguousarray(rho_p, dtype=np.float64)), _p(eq), _p(rq))
         assert rc == 0, rc
         return eq, rq
+
+    def solcx_norms(self, eta0, eta1, xc, n, u, p):
+        """[||v - v_ex||_L2, |E - E_ex|_H1s, H1, ||p - p_ex||_L2] of a discrete
+        solution on the mesh given to setup() against the SolCx analytic
+        solution, by the reference's Evaluate_uL2_symuH1_pL2 (src/inorms.c:188-363)
+        and SolCxSolution (src/models/analytics_vv/SolCxSolution.c)."""
+        out = np.zeros(4)
+        rc = self.L.ref_solcx_norms(float(eta0), float(eta1), float(xc), int(n),
+                                    _p(np.ascontiguousarray(u, dtype=np.float64)),
+                                    _p(np.ascontiguousarray(p, dtype=np.float64)), _p(out))
+        assert rc == 0, rc
+        return out
+
+    def solcx_exact(self, eta0, eta1, xc, n, pos):
+        """SolCx analytic velocity [3] and pressure at pos [3]."""
+        v, pr = np.zeros(3), np.zeros(1)
+        rc = self.L.ref_solcx_exact(float(eta0), float(eta1), float(xc), int(n),
+                                    _p(np.ascontiguousarray(pos, dtype=np.float64)), _p(v), _p(pr))
+        assert rc == 0, rc
+        return v, float(pr[0])
 
     def stokes_avx_raw(self, u, p):
         """MFStokesWrapper_A_AVX: [A11 u + A12 p; A21 u] without boundary conditions."""

@@ -13,6 +13,10 @@
  *   ref_marker_project(type, n, wil, xi, eta_p, rho_p, eta_q, rho_q)
  *       the material-point -> Gauss-point projections of the rheology update
  *       (src/rheology.c:150-185; material_point_utils.c, quadrature.c)
+ *   ref_solcx_norms(eta0, eta1, xc, n, u, p, norms[4])
+ *       error norms of a discrete solution against the SolCx analytic
+ *       solution, as the verification model prints them
+ *       (src/models/analytics_vv/analytics_vv.c:313-357, src/inorms.c:188-363)
  *
  * Each adds element contributions exactly as the reference's SpMVOp_MatMult
  * callback does (the caller zeroes y and applies Dirichlet rows/columns).
@@ -32,6 +36,8 @@
 #include "MPntStd_def.h"
 #include "MPntPStokes_def.h"
 #include "material_point_utils.h"
+#include "inorms.h"
+#include "models/analytics_vv/SolCxSolution.h"
 
 /* kernels provided by the reference objects */
 PetscErrorCode MFStokesWrapper_A11_Tensor(MatA11MF, Quadrature, DM, PetscScalar[], PetscScalar[]);
@@ -396,6 +402,30 @@ int ref_marker_project(int type, int n, const int *wil, const double *xi, const 
   free(std);
   free(stk);
   return rc;
+}
+/* [v_L2, symmetric-gradient H1 seminorm, H1, p_L2] errors of (u [3*nn], p [4*nel])
+ * against SolCx(eta0, eta1, xc, n) on the mesh given to ref_setup */
+int ref_solcx_norms(double eta0, double eta1, double xc, int n, double *u, double *p, double *norms)
+{
+  ParamsSolCx prm;
+  int rc = SolCxParamsSetValues(&prm, eta0, eta1, xc, n);
+  if (rc) return rc;
+  struct _p_shim_Vec sv, sp;
+  sv.a = u;
+  sv.n = (long)g_dau.dof * g_dau.M * g_dau.N * g_dau.P;
+  sp.a = p;
+  sp.n = (long)g_dap.dof * g_dap.M * g_dap.N * g_dap.P;
+  return Evaluate_uL2_symuH1_pL2(&g_dau, &g_dap, &sv, &sp, &g_Q, EvaluateV_SolCx, EvaluateE_SolCx, EvaluateP_SolCx,
+                                 (void *)&prm, &norms[0], &norms[1], &norms[2], &norms[3]);
+}
+/* the analytic velocity [3] and pressure at a point */
+int ref_solcx_exact(double eta0, double eta1, double xc, int n, double *pos, double *vel, double *pressure)
+{
+  ParamsSolCx prm;
+  int rc = SolCxParamsSetValues(&prm, eta0, eta1, xc, n);
+  if (rc) return rc;
+  if ((rc = EvaluateV_SolCx(pos, vel, (void *)&prm))) return rc;
+  return EvaluateP_SolCx(pos, pressure, (void *)&prm);
 }
 int ref_set_threads(int n) { omp_set_num_threads(n); return 0; }
 int ref_max_threads(void) { return omp_get_max_threads(); }

@@ -36,6 +36,8 @@ typedef int MPI_Op;
 #define PETSC_COMM_SELF 0
 #define MPIU_INT MPI_INT
 #define MPIU_REAL MPI_DOUBLE
+#define MPIU_SUM MPI_SUM
+#define PetscObjectComm(o) 0
 
 typedef struct _p_shim_DM  *DM;
 typedef struct _p_shim_Vec *Vec;
@@ -85,6 +87,8 @@ typedef enum { PETSC_VIEWER_DEFAULT = 0, PETSC_VIEWER_ASCII_VTK } PetscViewerFor
 #define PetscRealPart(a) (a)
 #define PetscPowReal(a, b) pow(a, b)
 #define PetscExpReal(a) exp(a)
+#define PetscSinReal(a) sin(a)
+#define PetscCosReal(a) cos(a)
 #define PETSC_PI 3.14159265358979323846
 #define PETSC_MAX_REAL 1.7976931348623157e+308
 #define PETSC_MACHINE_EPSILON 2.2204460492503131e-16

@@ -37,3 +37,18 @@ def sinker_case(m, seed=1, nsph=8, radius=0.1, eta1=1e3, deform=0.0):
 def rel(a, b):
     a = np.asarray(a); b = np.asarray(b)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def solcx_case(mx, my, mz, eta0, eta1, xc=0.5, n=2):
+    """The reference's SolCx verification model (src/models/analytics_vv/analytics_vv.c):
+    unit cube, free slip on all six faces (:68-83), gravity (0, -1, 0) (:115-125),
+    markers on the Gauss points mapped one to one (projection type 4), eta = eta0
+    for x <= xc else eta1 and rho = -cos(pi x) sin(n pi y) at each point (:221-257)."""
+    c = M.uniform_coords(mx, my, mz)
+    qp = M.qp_coords(c, mx, my, mz)
+    x, y = qp[..., 0], qp[..., 1]
+    eta = np.where(x <= xc, eta0, eta1)
+    rho = -np.cos(np.pi * x) * np.sin(n * np.pi * y)
+    bits = M.FREE_SLIP
+    return dict(dims=(mx, my, mz), coords=c, eta=eta, rho=rho, bits=bits, mask=M.dirichlet_mask(mx, my, mz, bits),
+                g=(0.0, -1.0, 0.0))
