@@ -109,8 +109,8 @@ class CpuStokesSolver:
                  restart=30, threads=None, schur_geomean=True, g=(0.0, 0.0, -1.0)):
         t0 = time.perf_counter()
         self.K, self.lo, self.hi, self.restart = cheb_its, cheb_lo, cheb_hi, restart
-        dims = (m, m, m)
-        nf = (2 * m + 1,) * 3
+        dims = tuple(m) if isinstance(m, (tuple, list)) else (m, m, m)  # elements per direction
+        nf = tuple(2 * d + 1 for d in dims)
         coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1)
         eta = np.ascontiguousarray(eta, dtype=np.float64).reshape(-1, 27)
         self.ref = Reference()
@@ -154,7 +154,7 @@ class CpuStokesSolver:
         self.Binv = np.linalg.inv(R.schur_mass(dims, coords, e_s.reshape(-1)))
         bu = body_force(R, dims, coords, np.asarray(rho, dtype=np.float64).reshape(-1), g)
         bu[mask] = 0.0
-        self.nu, self.npr = coords.size, 4 * m ** 3
+        self.nu, self.npr = coords.size, 4 * dims[0] * dims[1] * dims[2]
         self.b = np.concatenate([bu, np.zeros(self.npr)])
         self.setup_s = time.perf_counter() - t0
 

@@ -58,6 +58,19 @@ def solve_dense(restatement, case):
     return x[:c.size], x[c.size:]
 
 
+def pressure_fitted_norms(reference_kernels, prm, u, p):
+    """Error norms with the free constant pressure set to minimise the pressure
+    error: the constant mode is the first P1disc basis function of every
+    element, and ||p_h + s - p_ex||^2 is quadratic in s, so three evaluations
+    give its minimum."""
+    def norms(shift):
+        q = np.array(p, dtype=np.float64).copy()
+        q[0::4] += shift
+        return reference_kernels.solcx_norms(*prm, u, q)
+    f0, f1, fm = norms(0.0)[3] ** 2, norms(1.0)[3] ** 2, norms(-1.0)[3] ** 2
+    return norms(-(f1 - fm) / 2.0 / (f1 + fm - 2.0 * f0))
+
+
 @pytest.mark.parametrize("name", sorted(n for n in GOLD if GOLD[n]["mx"] * GOLD[n]["my"] * GOLD[n]["mz"] <= 72))
 def test_discrete_solution_reproduces_reference_error_norms(restatement, reference_kernels, name):
     rec = GOLD[name]
@@ -65,17 +78,27 @@ def test_discrete_solution_reproduces_reference_error_norms(restatement, referen
     case = solcx_case(rec["mx"], rec["my"], rec["mz"], *prm)
     u, p = solve_dense(restatement, case)
     reference_kernels.setup(case["dims"], case["coords"], case["eta"].reshape(-1))
-
-    def norms(shift):
-        q = p.copy()
-        q[0::4] += shift  # the constant pressure mode: first P1disc basis function of every element
-        return reference_kernels.solcx_norms(*prm, u, q)
-
-    # ||p_h + s - p_ex||^2 is quadratic in s: its minimum from three evaluations
-    f0, f1, fm = norms(0.0)[3] ** 2, norms(1.0)[3] ** 2, norms(-1.0)[3] ** 2
-    s = -(f1 - fm) / 2.0 / (f1 + fm - 2.0 * f0)
-    got = norms(s)
+    got = pressure_fitted_norms(reference_kernels, prm, u, p)
     want = [float(v) for v in rec["inorms"]]
     assert abs(want[0] - 1.0 / rec["mx"]) <= 1e-12
     for g, w in zip(got, want[1:]):
+        assert abs(g - w) <= 1e-8 * abs(w), (name, got, want)
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_cpu_solver_reproduces_reference_error_norms(reference_kernels, name):
+    """The solver restated on the host (the device solver's algorithm: FGMRES,
+    Schur upper, Galerkin multigrid with Chebyshev/Jacobi) on every SolCx case,
+    12x12x2 included, solved to 1e-11: the reference's printed norms."""
+    from oracle.cpu_solver import CpuStokesSolver
+    rec = GOLD[name]
+    prm = (rec["eta0"], rec["eta1"], rec["xc"], rec["n"])
+    case = solcx_case(rec["mx"], rec["my"], rec["mz"], *prm)
+    S = CpuStokesSolver(case["dims"], case["coords"], case["eta"], case["rho"], case["bits"], nlevels=2, g=case["g"])
+    u, p, its, rt, _ = S.solve(rtol=1e-11, max_it=500)
+    assert rt <= 1e-11
+    reference_kernels.setup(case["dims"], case["coords"], case["eta"].reshape(-1))
+    got = pressure_fitted_norms(reference_kernels, prm, u, p)
+    want = [float(v) for v in rec["inorms"][1:]]
+    for g, w in zip(got, want):
         assert abs(g - w) <= 1e-8 * abs(w), (name, got, want)
