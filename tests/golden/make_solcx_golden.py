@@ -1,7 +1,10 @@
 """Extract the SolCx verification values of the reference's own test suite
-(tests/verification/linear/solcx_*/{test.py,expected,more.opts} and the
+(tests/verification/linear/sol{c,k}x_*/{test.py,expected,more.opts} and the
 options files they launch, src/models/analytics_vv/examples/*.opts) into
-solcx_expected.json.  Run in a checkout that has the pTatin3d tree:
+solcx_expected.json.  The solkx_* tests run the same model: it registers the
+SolCx material geometry and error norms (src/models/analytics_vv/analytics_vv.c:
+320-352, 414-416), with the SolCx parameters at their defaults.  Run in a
+checkout that has the pTatin3d tree:
 
     python tests/golden/make_solcx_golden.py /path/to/pTatin3d
 
@@ -31,12 +34,13 @@ def options(path):
 
 
 out = {}
-for d in sorted(glob.glob(os.path.join(ref, "tests/verification/linear/solcx_*"))):
+DEFAULTS = {"solcx_eta0": "1.0", "solcx_eta1": "1.0", "solcx_xc": "0.5", "solcx_n": "2"}  # analytics_vv.c:320-326
+for d in sorted(glob.glob(os.path.join(ref, "tests/verification/linear/sol[ck]x_*"))):
     test = open(os.path.join(d, "test.py")).read()
     if re.search(r"ranks\s*=\s*1\b", test) is None:
         continue  # one-process runs only
-    opts = {}
-    for f in re.findall(r"'(analytics-solcx-[a-z0-9]+\.opts)'", test):
+    opts = dict(DEFAULTS)
+    for f in re.findall(r"'(analytics-sol[ck]x-[a-z0-9]+\.opts)'", test):
         opts.update(options(os.path.join(ref, "src/models/analytics_vv/examples", f)))
     if os.path.exists(os.path.join(d, "more.opts")) and "more.opts" in test:
         opts.update(options(os.path.join(d, "more.opts")))
