@@ -52,3 +52,33 @@ def solcx_case(mx, my, mz, eta0, eta1, xc=0.5, n=2):
     bits = M.FREE_SLIP
     return dict(dims=(mx, my, mz), coords=c, eta=eta, rho=rho, bits=bits, mask=M.dirichlet_mask(mx, my, mz, bits),
                 g=(0.0, -1.0, 0.0))
+
+
+def _q2_1d(x):
+    return np.stack([0.5 * x * (x - 1.0), 1.0 - x * x, 0.5 * x * (x + 1.0)], axis=-1)
+
+
+def sinker_markers(case, eta0=1.0, eta1=10.0, rho0=0.0, rho1=1.0, per_dir=2):
+    """Material points of the reference's viscous-sinker operator tests on the
+    mesh of `case`: per_dir^3 markers per element on the lattice
+    xi = -1 + (2/per_dir)(i + 1/2) (SwarmMPntStd_CoordAssignment_LatticeLayout3d,
+    src/material_point_std_utils.c:100-200; 2^3 by default, src/ptatin3d.c:473,
+    the tests set -lattice_layout_perturb 0), placed through the element's Q2
+    map, eta1 / -rho1 inside the sphere of diameter 0.5 about the box centre and
+    eta0 / -rho0 outside (src/models/viscous_sinker/model_viscous_sinker_ops.c:
+    70-85, 755-770).  Returns (wil, xi [n,3], eta, rho)."""
+    mx, my, mz = case["dims"]
+    c = np.asarray(case["coords"]).reshape(-1, 3)
+    nx, ny = 2 * mx + 1, 2 * my + 1
+    s = -1.0 + (2.0 / per_dir) * (np.arange(per_dir) + 0.5)
+    xi = np.array([(s[i], s[j], s[k]) for k in range(per_dir) for j in range(per_dir) for i in range(per_dir)])
+    Ni = (_q2_1d(xi[:, 0])[:, None, None, :] * _q2_1d(xi[:, 1])[:, None, :, None]
+          * _q2_1d(xi[:, 2])[:, :, None, None]).reshape(len(xi), 27)
+    e = np.arange(mx * my * mz)
+    ex, ey, ez = e % mx, (e // mx) % my, e // (mx * my)
+    n = np.arange(27)
+    nodes = (2 * ex[:, None] + n % 3) + nx * ((2 * ey[:, None] + (n // 3) % 3) + ny * (2 * ez[:, None] + n // 9))
+    pos = np.einsum("pn,enk->epk", Ni, c[nodes]).reshape(-1, 3)
+    inside = (((pos - 0.5) / 0.25) ** 2).sum(axis=1) < 1.0
+    wil = np.repeat(e, len(xi)).astype(np.int32)
+    return (wil, np.tile(xi, (len(e), 1)), np.where(inside, eta1, eta0), np.where(inside, -rho1, -rho0))

@@ -5,7 +5,10 @@ tests/golden/reference_expected.json by tests/golden/make_golden.py).
 
 Exact pins: A12 and A21 do not depend on viscosity; A11 and diag(A11) are
 pinned where the test's viscosity field is uniform (default sinker with
-eta1 = 1, and the 1x1x3 mesh whose Gauss points never sample the inclusion).
+eta1 = 1, and the 1x1x3 mesh whose Gauss points never sample the inclusion),
+and, for the eta1 = 10 sinker, with the Gauss-point viscosity the reference
+computes from its material points: a 2^3 marker lattice per element and the
+Q1 projection (tests/cases.py:sinker_markers, projection type 1).
 The reference harness compares at 1e-13; the values are printed with 9
 significant digits, so agreement is checked to 5e-9 relative.
 """
@@ -16,8 +19,8 @@ import os
 import numpy as np
 import pytest
 
-from cases import bump_case
-from oracle.oracle import get_diagonal, matmult_a11, matmult_a12, matmult_a21
+from cases import bump_case, sinker_markers
+from oracle.oracle import get_diagonal, marker_project, matmult_a11, matmult_a12, matmult_a21
 
 GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_expected.json")))
 
@@ -68,6 +71,41 @@ def test_reference_kernels_match_reference_expected(reference_kernels, name, op,
     reference_kernels.setup(case["dims"], case["coords"], case["eta"])
     impl = {"a11": lambda v: reference_kernels.a11_raw(v, "tensor"), "diag": reference_kernels.diag_raw,
             "a21": reference_kernels.a21_raw, "a12": reference_kernels.a12_raw}
+    _check(_yy(impl, op, case), gold)
+
+
+def _marker_pins(max_nel=None):
+    out = []
+    for name, rec in GOLD.items():
+        dims = (rec["mx"], rec["my"], rec["mz"])
+        if rec["eta1"] == 1.0 or (max_nel and dims[0] * dims[1] * dims[2] > max_nel):
+            continue
+        for op in ("A11", "diagA11"):
+            out.append(pytest.param(name, op, dims, rec["eta1"], float(rec[op]), id=f"{name}-{op}-markers"))
+    return out
+
+
+@pytest.mark.parametrize("name,op,dims,eta1,gold", _marker_pins())
+def test_restatement_with_marker_viscosity_matches_reference_expected(restatement, name, op, dims, eta1, gold):
+    """eta1 = 10 sinker: markers -> Q1 projection (numpy restatement) -> A11 / diag(A11)."""
+    case = bump_case(*dims)
+    wil, xi, eta_p, rho_p = sinker_markers(case, eta1=eta1)
+    eta, _ = marker_project(dims, 1, wil, xi, eta_p, rho_p)
+    d, c = case["dims"], case["coords"]
+    impl = {"a11": lambda v: restatement.a11_raw(d, c, eta, v), "diag": lambda: restatement.diag_raw(d, c, eta)}
+    _check(_yy(impl, op, case), gold)
+
+
+@pytest.mark.parametrize("name,op,dims,eta1,gold", _marker_pins(max_nel=1500))
+def test_reference_projection_and_kernels_match_reference_expected(reference_kernels, name, op, dims, eta1, gold):
+    """The same with the reference's own compiled projection and kernels throughout."""
+    case = bump_case(*dims)
+    wil, xi, eta_p, rho_p = sinker_markers(case, eta1=eta1)
+    nel = dims[0] * dims[1] * dims[2]
+    reference_kernels.setup(dims, case["coords"], np.ones(27 * nel))
+    eta, _ = reference_kernels.marker_project(1, wil, xi, eta_p, rho_p)
+    reference_kernels.setup(dims, case["coords"], eta)
+    impl = {"a11": lambda v: reference_kernels.a11_raw(v, "tensor"), "diag": reference_kernels.diag_raw}
     _check(_yy(impl, op, case), gold)
 
 

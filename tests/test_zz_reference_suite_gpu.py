@@ -1,0 +1,74 @@
+"""The device path against values the reference's own test suite prints.
+
+* Operator tests with the eta1 = 10 viscous sinker
+  (tests/integration/operator/**/expected): the markers go through the device
+  Q1 projection (p3d_marker_project) into the device operator, whose A11 and
+  diag(A11) y.y equal the printed values.
+* SolCx verification tests (tests/verification/linear/sol{c,k}x_*): the
+  device solver (p3d_solver_*), solved to a relative residual of 1e-11, gives
+  velocity, strain-rate and pressure error norms against the analytic
+  solution -- computed by the reference's own Evaluate_uL2_symuH1_pL2 and
+  SolCx code (oracle/_ref) -- equal to the printed ones, as the host
+  restatement of the same solver does (tests/test_solcx_verification.py).
+
+Collected last (file name) so a failure here does not hide the rest of the
+suite.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from cases import bump_case, sinker_markers, solcx_case
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = json.load(open(os.path.join(HERE, "golden", "solcx_expected.json")))
+OPS = json.load(open(os.path.join(HERE, "golden", "reference_expected.json")))
+
+
+@pytest.mark.parametrize("name", sorted(n for n, r in OPS.items() if r["eta1"] != 1.0))
+def test_device_projection_and_operator_match_reference_expected(cuda, name):
+    import torch
+
+    from ptatin3d_b200.markers import PROJ_Q1, update_gauss_properties
+    from ptatin3d_b200.operators import MatStokesMF, mesh_desc_whole
+    rec = OPS[name]
+    case = bump_case(rec["mx"], rec["my"], rec["mz"])
+    wil, xi, eta_p, rho_p = sinker_markers(case, eta1=rec["eta1"])
+    t = lambda a, dt: torch.tensor(np.ascontiguousarray(a), dtype=dt, device=cuda)
+    eta_q, _ = update_gauss_properties(case["dims"], PROJ_Q1, t(wil, torch.int32), t(xi, torch.float64),
+                                       t(eta_p, torch.float64), t(rho_p, torch.float64))
+    op = MatStokesMF(mesh_desc_whole(*case["dims"], case["bits"]))
+    op.set_coefficients(t(case["coords"], torch.float64), eta_q)
+    x = t(case["x"], torch.float64)
+    y = torch.empty_like(x)
+    op.mult(x, y)
+    d = torch.empty_like(x)
+    op.get_diagonal(d)
+    for val, key in ((float(y @ y), "A11"), (float(d @ d), "diagA11")):
+        gold = float(rec[key])
+        assert abs(val - gold) <= 5e-9 * abs(gold), (name, key, val, gold)
+
+
+@pytest.mark.parametrize("name", sorted(GOLD))
+def test_device_solver_reproduces_reference_error_norms(cuda, reference_kernels, name):
+    from ptatin3d_b200.solver import StokesSolver
+    from test_solcx_verification import pressure_fitted_norms
+    rec = GOLD[name]
+    prm = (rec["eta0"], rec["eta1"], rec["xc"], rec["n"])
+    case = solcx_case(rec["mx"], rec["my"], rec["mz"], *prm)
+    S = StokesSolver(*case["dims"], case["bits"], nlevels=2, rtol=1e-11, max_it=500)
+    S.setup(case["coords"], case["eta"])
+    S.set_rhs_body_force(case["rho"], g=case["g"])
+    u, p, st = S.solve(raise_on_noconv=False)
+    S.destroy()
+    assert st["converged"] and st["rfinal"] <= 1e-11 * st["r0"], st
+    reference_kernels.setup(case["dims"], case["coords"], case["eta"].reshape(-1))
+    got = pressure_fitted_norms(reference_kernels, prm, u.cpu().numpy(), p.cpu().numpy())
+    want = [float(v) for v in rec["inorms"][1:]]
+    for g, w in zip(got, want):
+        assert abs(g - w) <= 1e-7 * abs(w), (name, got, want)
+    assert np.isfinite(got).all()
