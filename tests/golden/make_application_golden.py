@@ -1,0 +1,45 @@
+"""Extract the initial Stokes residual of the reference's viscous-sinker
+application tests (tests/application/linear/**/{opts,expected}) into
+application_expected.json.  Run in a checkout that has the pTatin3d tree:
+
+    python tests/golden/make_application_golden.py /path/to/pTatin3d
+
+The outer Krylov solve starts from zero velocity and pressure
+(ModelInitialCondition_ViscousSinker, src/models/viscous_sinker/
+model_viscous_sinker_ops.c:1181-1220), so its first printed residual norm,
+"0 KSP Residual norm", is the norm of the right-hand side: the body force of
+the material points' density after their projection onto the Gauss points.
+Each record keeps the mesh, the options the model reads and that value as
+printed (6 significant digits).
+"""
+import glob
+import json
+import os
+import re
+import sys
+
+ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+out = {}
+for opts_file in sorted(glob.glob(os.path.join(ref, "tests/application/linear/**/opts"), recursive=True)):
+    d = os.path.dirname(opts_file)
+    opts = {}
+    for line in open(opts_file):
+        line = line.split("#", 1)[0].strip()
+        if line.startswith("-"):
+            parts = line.split(None, 1)
+            opts[parts[0][1:]] = parts[1] if len(parts) > 1 else ""
+    if opts.get("ptatin_model") != "viscous_sinker":
+        continue
+    m = re.search(r"^\s*0 KSP Residual norm (\S+)", open(os.path.join(d, "expected")).read(), re.M)
+    out[os.path.relpath(d, os.path.join(ref, "tests/application/linear"))] = {
+        "mx": int(opts["mx"]), "my": int(opts["my"]), "mz": int(opts["mz"]),
+        "eta0": float(opts.get("model_viscous_sinker_eta0", "1.0")),
+        "eta1": float(opts.get("model_viscous_sinker_eta1", "1.0")),
+        "rho0": float(opts.get("model_viscous_sinker_rho0", "0.0")),
+        "rho1": float(opts.get("model_viscous_sinker_rho1", "1.0")),
+        "lattice_layout_perturb": float(opts.get("lattice_layout_perturb", "0.1")),
+        "projection": int(opts.get("coefficient_projection_type", "1")),
+        "r0": m.group(1), "source": os.path.relpath(os.path.join(d, "expected"), ref)}
+json.dump(out, open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "application_expected.json"), "w"),
+          indent=1, sort_keys=True)
+print(len(out), "records")

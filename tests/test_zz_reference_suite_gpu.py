@@ -4,6 +4,10 @@
   (tests/integration/operator/**/expected): the markers go through the device
   Q1 projection (p3d_marker_project) into the device operator, whose A11 and
   diag(A11) y.y equal the printed values.
+* Viscous-sinker application tests (tests/application/linear/**/expected):
+  the first printed residual, from zero velocity and pressure, is the norm of
+  the body force; the device projection of the markers' density and the
+  device residual (p3d_stokes_residual) reproduce it.
 * SolCx verification tests (tests/verification/linear/sol{c,k}x_*): the
   device solver (p3d_solver_*), solved to a relative residual of 1e-11, gives
   velocity, strain-rate and pressure error norms against the analytic
@@ -27,6 +31,36 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLD = json.load(open(os.path.join(HERE, "golden", "solcx_expected.json")))
 OPS = json.load(open(os.path.join(HERE, "golden", "reference_expected.json")))
+APP = json.load(open(os.path.join(HERE, "golden", "application_expected.json")))
+
+
+def _device(cuda, a, dt):
+    import torch
+    return torch.tensor(np.ascontiguousarray(a), dtype=dt, device=cuda)
+
+
+@pytest.mark.parametrize("name", sorted(APP))
+def test_device_rhs_matches_reference_application(cuda, name):
+    import torch
+
+    from ptatin3d_b200.markers import PROJ_Q1, update_gauss_properties
+    from ptatin3d_b200.operators import MatStokesMF, mesh_desc_whole
+    rec = APP[name]
+    case = bump_case(rec["mx"], rec["my"], rec["mz"])
+    wil, xi, eta_p, rho_p = sinker_markers(case, rec["eta0"], rec["eta1"], rec["rho0"], rec["rho1"])
+    eta_q, rho_q = update_gauss_properties(case["dims"], PROJ_Q1, _device(cuda, wil, torch.int32),
+                                           _device(cuda, xi, torch.float64), _device(cuda, eta_p, torch.float64),
+                                           _device(cuda, rho_p, torch.float64))
+    op = MatStokesMF(mesh_desc_whole(*case["dims"], case["bits"]))
+    op.set_coefficients(_device(cuda, case["coords"], torch.float64), eta_q)
+    fu = torch.zeros(rho_q.shape[0], 27, 3, dtype=torch.float64, device=cuda)
+    fu[..., 1] = rho_q  # gravity (0, 1, 0), the reference's default (src/ptatin3d.c:94-104)
+    u = torch.zeros(op.n_velocity, dtype=torch.float64, device=cuda)
+    p = torch.zeros(op.n_pressure, dtype=torch.float64, device=cuda)
+    ru, rp = op.residual(u, p, fu=fu)
+    val = float(torch.sqrt(ru @ ru + rp @ rp))
+    gold = float(rec["r0"])
+    assert abs(val - gold) <= 5e-6 * gold, (name, val, gold)
 
 
 @pytest.mark.parametrize("name", sorted(n for n, r in OPS.items() if r["eta1"] != 1.0))
