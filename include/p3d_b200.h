@@ -187,7 +187,9 @@ int p3d_mg_restrict(int prec, int cnx, int cny, int cnz, int ndof, const void *x
  * local coordinates in [-1,1]^3 (Q1 only), eta_p[n], rho_p[n].  Output:
  * eta_q, rho_q [27*nel] device arrays (element-major, q = qi + 3qj + 9qk).
  * `workspace`: device memory of p3d_marker_project_workspace bytes, 8-byte
- * aligned (may be NULL when that is 0).  Asynchronous on `stream`. */
+ * aligned (may be NULL when that is 0).  After P3D_PROJ_Q1 it holds the nodal
+ * viscosity [nn] followed by the nodal density [nn], nn = (2mx+1)(2my+1)(2mz+1)
+ * (the input of p3d_solver_setup_nodal).  Asynchronous on `stream`. */
 #define P3D_PROJ_NULL (-1)
 #define P3D_PROJ_P0_ARITHMETIC 0
 #define P3D_PROJ_Q1 1
@@ -277,6 +279,14 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
 /* Device FP64 arrays: coords 3*nn, eta 27*nel.  Builds the hierarchy, the
  * operators, smoother bounds, the coarse inverse and the Schur blocks. */
 int p3d_solver_setup(p3d_solver *s, const double *coords_dev, const double *eta_dev);
+/* The same with the finest level's nodal viscosity [nn] given: the Q1
+ * coefficient hierarchy (coarse_op P3D_COARSE_REDISC, coarse_eta
+ * P3D_COARSE_ETA_Q1) restricts it instead of a projection of eta_dev.  This is
+ * the reference's hierarchy for projection type 1, whose nodal field comes from
+ * the markers (SwarmUpdateGaussPropertiesLocalL2Projection_Q1_MPntPStokes_Hierarchy,
+ * src/material_point_utils.c:1267-1360); p3d_marker_project leaves that field
+ * in its workspace.  Other options return P3D_ERR_ARG. */
+int p3d_solver_setup_nodal(p3d_solver *s, const double *coords_dev, const double *eta_dev, const double *eta_nodes_dev);
 /* Right-hand side from a Gauss-point density field and gravity vector
  * (Dirichlet rows zero); or set b directly (device arrays). */
 int p3d_solver_set_rhs_body_force(p3d_solver *s, const double *rho_dev, double gx, double gy, double gz);

@@ -114,6 +114,25 @@ class Restatement:
             v = vc
         return out
 
+    def eta_hierarchy_from_nodes(self, dims, eta, v, nlevels):
+        """The same hierarchy started from a given finest-level nodal field v
+        (the reference's projection type 1: v is the markers' Q1 nodal field,
+        src/material_point_utils.c:1267-1360)."""
+        for f in ("o_eta_restrict_nodes", "o_eta_nodes_to_qp"):
+            getattr(self.L, f).argtypes = [C.c_int] * 3 + [_dp] * 2
+        mx, my, mz = dims
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        out = [np.ascontiguousarray(eta, dtype=np.float64).reshape(-1)]
+        for _ in range(nlevels - 1):
+            mx, my, mz = mx // 2, my // 2, mz // 2
+            vc = np.zeros((2 * mx + 1) * (2 * my + 1) * (2 * mz + 1))
+            self.L.o_eta_restrict_nodes(2 * mx + 1, 2 * my + 1, 2 * mz + 1, _p(v), _p(vc))
+            e = np.zeros(27 * mx * my * mz)
+            self.L.o_eta_nodes_to_qp(mx, my, mz, _p(vc), _p(e))
+            out.append(e)
+            v = vc
+        return out
+
     def prolong(self, cn, ndof, xc):
         fn = [2 * c - 1 for c in cn]
         xf = np.zeros(fn[0] * fn[1] * fn[2] * ndof)
@@ -269,7 +288,7 @@ def _element_nodes(dims):
 _CORNER_NODES = np.array([0, 2, 6, 8, 18, 20, 24, 26])
 
 
-def marker_project(dims, ptype, wil, xi, eta_p, rho_p, eta_q=None, rho_q=None):
+def marker_project(dims, ptype, wil, xi, eta_p, rho_p, eta_q=None, rho_q=None, nodal=False):
     """Numpy restatement of the projection types of src/rheology.c:150-185 on a
     whole mesh: -1 keep, 0/10/20 P0 arithmetic/harmonic/geometric
     (src/material_point_utils.c:2567-2808), 1 Q1 (:604-801), 4 one-to-one
@@ -316,6 +335,8 @@ def marker_project(dims, ptype, wil, xi, eta_p, rho_p, eta_q=None, rho_q=None):
         Ve = V[nodes]
         vals = Ve[:, _CORNER_NODES] @ Nq.T
         out.append(np.clip(vals, Ve.min(axis=1)[:, None], Ve.max(axis=1)[:, None]).reshape(-1))
+    if nodal:  # also the nodal viscosity, the start of the type-1 coefficient hierarchy
+        return out[0], out[1], V1
     return out[0], out[1]
 
 

@@ -82,6 +82,7 @@ _SIGS = {
     "p3d_solver_default_opts": ([C.POINTER(SolverOpts)], C.c_int),
     "p3d_solver_create": ([C.POINTER(MeshDesc), C.POINTER(SolverOpts), C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "p3d_solver_setup": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_solver_setup_nodal": ([C.c_void_p] * 4, C.c_int),
     "p3d_solver_set_rhs_body_force": ([C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double], C.c_int),
     "p3d_solver_set_rhs": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_solver_solve": ([C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(SolveStats)], C.c_int),

@@ -456,7 +456,9 @@ static void free_level(Level &L)
   L.b = L.x = L.r = L.d = L.t = nullptr;
 }
 
-static int solver_setup(p3d_solver *s, const double *coords, const double *eta)
+// eta_nodes: optional finest-level nodal viscosity for the Q1 coefficient
+// hierarchy (nullptr: projected from the Gauss-point values)
+static int solver_setup(p3d_solver *s, const double *coords, const double *eta, const double *eta_nodes)
 {
   double t0 = now_ms();
   const int nlev = (int)s->lv.size();
@@ -488,7 +490,10 @@ static int solver_setup(p3d_solver *s, const double *coords, const double *eta)
       if (l == nlev - 1) {
         CU(cudaMemcpyAsync(L.coords, coords, 3 * nn * 8, cudaMemcpyDeviceToDevice, s->st), "coords");
         CU(cudaMemcpyAsync(L.eta, eta, 27 * nel * 8, cudaMemcpyDeviceToDevice, s->st), "eta");
-        if (q1) s_eta_project(L.m[0], L.m[1], L.m[2], eta, L.vnode, L.vden, s->st);
+        if (q1 && eta_nodes)
+          CU(cudaMemcpyAsync(L.vnode, eta_nodes, nn * 8, cudaMemcpyDeviceToDevice, s->st), "nodal eta");
+        else if (q1)
+          s_eta_project(L.m[0], L.m[1], L.m[2], eta, L.vnode, L.vden, s->st);
       } else {
         Level &F = s->lv[l + 1];
         s_inject_coords(L.n[0], L.n[1], L.n[2], F.coords, L.coords, s->st);
@@ -813,7 +818,17 @@ int p3d_solver_setup(p3d_solver *s, const double *coords, const double *eta)
 {
   if (!s || !coords || !eta) return set_error(P3D_ERR_ARG, "solver_setup: null argument");
   cudaSetDevice(s->device);
-  return solver_setup(s, coords, eta);
+  return solver_setup(s, coords, eta, nullptr);
+}
+
+int p3d_solver_setup_nodal(p3d_solver *s, const double *coords, const double *eta, const double *eta_nodes)
+{
+  if (!s || !coords || !eta || !eta_nodes) return set_error(P3D_ERR_ARG, "solver_setup_nodal: null argument");
+  if (s->o.coarse_op != P3D_COARSE_REDISC || s->o.coarse_eta != P3D_COARSE_ETA_Q1 || s->lv.size() < 2)
+    return set_error(P3D_ERR_ARG, "solver_setup_nodal: the nodal viscosity feeds only the Q1 coefficient hierarchy "
+                                  "(coarse_op P3D_COARSE_REDISC, coarse_eta P3D_COARSE_ETA_Q1, nlevels >= 2)");
+  cudaSetDevice(s->device);
+  return solver_setup(s, coords, eta, eta_nodes);
 }
 
 int p3d_solver_set_rhs_body_force(p3d_solver *s, const double *rho, double gx, double gy, double gz)

@@ -30,11 +30,13 @@ __all__ = ["update_gauss_properties", "PROJ_NULL", "PROJ_P0_ARITHMETIC", "PROJ_P
            "PROJ_Q1", "PROJ_ONE2ONE"]
 
 
-def update_gauss_properties(m, projection_type, wil, xi, eta_p, rho_p, eta_q=None, rho_q=None):
+def update_gauss_properties(m, projection_type, wil, xi, eta_p, rho_p, eta_q=None, rho_q=None, nodal=False):
     """Gauss-point viscosity and density [nel, 27] of the mesh m = (mx, my, mz)
     from n markers: wil int32 [n], xi float64 [n, 3], eta_p / rho_p float64 [n]
     (CUDA tensors).  eta_q / rho_q are updated in place when given (PROJ_NULL
-    leaves them unchanged), else allocated."""
+    leaves them unchanged), else allocated.  nodal=True (PROJ_Q1) also returns
+    the nodal viscosity on the Q2 lattice, the input of the solver's Q1
+    coefficient hierarchy (StokesSolver.setup(..., eta_nodes=...))."""
     mx, my, mz = m
     nel = mx * my * mz
     dev = eta_p.device
@@ -54,4 +56,9 @@ def update_gauss_properties(m, projection_type, wil, xi, eta_p, rho_p, eta_q=Non
             _check_size(t, k, dt, name)
     check(lib().p3d_marker_project(mx, my, mz, projection_type, n, _ptr(wil), None if xc is None else _ptr(xc),
                                    _ptr(eta_p), _ptr(rho_p), _ptr(eta_q), _ptr(rho_q), _ptr(ws), _stream()))
+    if nodal:
+        if projection_type != PROJ_Q1:
+            raise ValueError("the nodal field exists for the Q1 projection only")
+        nn = (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1)
+        return eta_q, rho_q, ws[:nn]
     return eta_q, rho_q

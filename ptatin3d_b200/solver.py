@@ -58,10 +58,16 @@ class StokesSolver:
             _check_size(t, n, torch.float64, name)
         return t
 
-    def setup(self, coords, eta):
+    def setup(self, coords, eta, eta_nodes=None):
+        """eta_nodes: the finest level's nodal viscosity for the Q1 coefficient
+        hierarchy (the reference's projection type 1), else None."""
         nel = self.dims[0] * self.dims[1] * self.dims[2]
         c, e = self._dev(coords, self.nu, "coords"), self._dev(eta, 27 * nel, "eta")
-        check(lib().p3d_solver_setup(self.h, _ptr(c), _ptr(e)))
+        if eta_nodes is None:
+            check(lib().p3d_solver_setup(self.h, _ptr(c), _ptr(e)))
+        else:
+            v = self._dev(eta_nodes, self.nu // 3, "eta_nodes")
+            check(lib().p3d_solver_setup_nodal(self.h, _ptr(c), _ptr(e), _ptr(v)))
 
     def set_rhs_body_force(self, rho, g=(0.0, 0.0, -1.0)):
         r = self._dev(rho, 27 * self.dims[0] * self.dims[1] * self.dims[2], "rho")

@@ -83,3 +83,30 @@ def test_restatement_vs_reference_random(reference_kernels):
         er, rr = reference_kernels.marker_project(t, wil, xi, eta, rho)
         en, rn = marker_project(dims, t, wil, xi, eta, rho)
         assert close(en, er, 1e-13) and close(rn, rr, 1e-13)
+
+
+def test_restated_type1_hierarchy_starts_from_marker_nodes(restatement):
+    """The type-1 hierarchy restricts the markers' nodal field; when that field
+    is the nodal projection of the Gauss-point values, it equals the hierarchy
+    built from those values."""
+    dims = (8, 8, 8)
+    rng = np.random.default_rng(3)
+    nel = 512
+    n = 10 * nel
+    wil = rng.integers(0, nel, size=n).astype(np.int32)
+    xi = rng.uniform(-1, 1, size=(n, 3))
+    eta, rho = 10.0 ** rng.uniform(-2, 2, size=n), np.ones(n)
+    eq, _, v = marker_project(dims, 1, wil, xi, eta, rho, nodal=True)
+    assert v.size == 17 ** 3 and np.all(v > 0)
+    lv = restatement.eta_hierarchy_from_nodes(dims, eq, v, 3)
+    assert [a.size for a in lv] == [27 * 512, 27 * 64, 27 * 8]
+    assert np.array_equal(lv[0], eq)
+    # started from the Gauss-point projection, the two hierarchies agree
+    qp = restatement.eta_hierarchy(dims, eq, 3)
+    import ctypes as C
+    from oracle.oracle import _dp, _p
+    restatement.L.o_eta_project_nodes.argtypes = [C.c_int] * 3 + [_dp] * 2
+    vq = np.zeros(17 ** 3)
+    restatement.L.o_eta_project_nodes(8, 8, 8, _p(np.ascontiguousarray(eq)), _p(vq))
+    for a, b in zip(restatement.eta_hierarchy_from_nodes(dims, eq, vq, 3), qp):
+        assert np.allclose(a, b, rtol=1e-14, atol=0)

@@ -106,3 +106,42 @@ def test_device_solver_reproduces_reference_error_norms(cuda, reference_kernels,
     for g, w in zip(got, want):
         assert abs(g - w) <= 1e-7 * abs(w), (name, got, want)
     assert np.isfinite(got).all()
+
+
+def test_device_marker_hierarchy_levels_match_oracle(cuda, restatement):
+    """The reference's projection type 1 end to end on the device: markers ->
+    Q1 projection -> the nodal viscosity feeds the solver's Q1 coefficient
+    hierarchy (p3d_solver_setup_nodal); every level operator equals the
+    oracle's MatMult with the restated hierarchy started from the same nodal
+    field (src/material_point_utils.c:1267-1420)."""
+    import torch
+
+    from oracle.oracle import marker_project, matmult_a11
+    from ptatin3d_b200 import COARSE_ETA_Q1, COARSE_REDISC
+    from ptatin3d_b200 import mesh as M
+    from ptatin3d_b200.markers import PROJ_Q1, update_gauss_properties
+    from ptatin3d_b200.solver import StokesSolver
+    m, nlev = 8, 3
+    case = bump_case(m, m, m)
+    wil, xi, eta_p, rho_p = sinker_markers(case, eta0=1.0, eta1=100.0)
+    eta_q, _, v = update_gauss_properties(case["dims"], PROJ_Q1, _device(cuda, wil, torch.int32),
+                                          _device(cuda, xi, torch.float64), _device(cuda, eta_p, torch.float64),
+                                          _device(cuda, rho_p, torch.float64), nodal=True)
+    bits = M.FREE_SLIP
+    S = StokesSolver(m, m, m, bits, nlevels=nlev, coarse_op=COARSE_REDISC, coarse_eta=COARSE_ETA_Q1)
+    S.setup(case["coords"], eta_q, eta_nodes=v)
+    e_ref, _, v_ref = marker_project(case["dims"], 1, wil, xi, eta_p, rho_p, nodal=True)
+    etas = restatement.eta_hierarchy_from_nodes(case["dims"], e_ref, v_ref, nlev)
+    rng = np.random.default_rng(6)
+    cl = np.asarray(case["coords"])
+    for depth in range(nlev):
+        mm = m >> depth
+        if depth:
+            nf = 2 * (2 * mm) + 1
+            cl = cl.reshape(nf, nf, nf, 3)[::2, ::2, ::2].reshape(-1).copy()  # injection
+        x = rng.uniform(-1, 1, size=3 * (2 * mm + 1) ** 3)
+        y = S.level_apply(nlev - 1 - depth, x).cpu().numpy()
+        mask = M.dirichlet_mask(mm, mm, mm, bits)
+        ref = matmult_a11(lambda w: restatement.a11_raw((mm, mm, mm), cl, etas[depth], w), x, mask)
+        assert np.linalg.norm(y - ref) <= 1e-12 * np.linalg.norm(ref), depth
+    S.destroy()
