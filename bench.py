@@ -626,6 +626,7 @@ def run_b200(args):
     e1.record(stream)
     torch.cuda.synchronize()
     f32_ms = e0.elapsed_time(e1) / args.steps
+    f32_err = float((y32.double() - y).norm() / y.norm())  # y = A x from the last FP64 step
     del op32, x32, y32
 
     # end to end through the reference-facing host-buffer call (x in, y out each step)
@@ -643,6 +644,17 @@ def run_b200(args):
         check(L.p3d_a11_apply_host(op.h, xhp, yhp))
     e2e_s = reduce_max((time.perf_counter() - t0) / ne2e, world)
     e2e_value = world * ndof / e2e_s / 1e9
+    # the same call on pageable host arrays, as a PETSc MatShell callback hands
+    # over its local vectors (the copies go through the driver's staging)
+    xpg = np.ascontiguousarray(wl["x"], dtype=np.float64)
+    ypg = np.zeros(ndof)
+    xpp, ypp = C.c_void_p(xpg.ctypes.data), C.c_void_p(ypg.ctypes.data)
+    check(L.p3d_a11_apply_host(op.h, xpp, ypp))
+    t0 = time.perf_counter()
+    npg = max(3, ne2e // 4)
+    for _ in range(npg):
+        check(L.p3d_a11_apply_host(op.h, xpp, ypp))
+    pg_value = world * ndof / reduce_max((time.perf_counter() - t0) / npg, world) / 1e9
     # the pipelined host-buffer result is the device MatMult's
     check(L.p3d_a11_mult(op.h, xp, yp, sp))
     torch.cuda.synchronize()
@@ -716,11 +728,14 @@ def run_b200(args):
                              "algorithmic_bytes": ab, "kernel_ms": kern_ms},
                 "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof,
-                        "rel_diff_vs_device": e2e_diff},
+                        "rel_diff_vs_device": e2e_diff, "host_buffers": "pinned",
+                        "pageable": {"value": pg_value, "unit": UNIT, "steps": npg,
+                                     "sample": "the same call on pageable numpy arrays"}},
                 "gpu_launches": launches,
                 "clocks": clk.summary(),
                 "fp32_apply": {"ms": f32_ms, "GDoF/s": ndof / (f32_ms * 1e-3) / 1e9,
-                               "hbm_frac": algorithmic_bytes(m, 4) / (f32_ms * 1e-3) / 1e9 / peak},
+                               "hbm_frac": algorithmic_bytes(m, 4) / (f32_ms * 1e-3) / 1e9 / peak,
+                               "rel_err_vs_fp64": f32_err},
                 "fp64_alu": {"flop_per_element": REF_FLOPS_PER_EL,
                              "TFLOP/s": REF_FLOPS_PER_EL * m ** 3 / (kern_ms * 1e-3) / 1e12},
                 "solve": solve,
@@ -826,6 +841,35 @@ def run_slabs(args, rank, world, local):
     return 0
 
 
+def profile_solve(spec):
+    """One short C2-construction solve for profiling its kernel mix:
+    spec = "m,iterations,precision" (precision 64 or 32).  Unit cube, 8
+    sinkers of radius 0.1, viscosity contrast 1e4, density +1 %, free slip
+    walls and base, free surface top, 4 Galerkin levels, Chebyshev(3)/Jacobi,
+    geometric-mean Schur weighting; stops after `iterations` FGMRES
+    iterations.  Prints one line, no JSON (not a benchmark number)."""
+    import torch
+
+    from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
+    from ptatin3d_b200 import mesh as M
+    from ptatin3d_b200.solver import StokesSolver, max_levels
+    m, its, prec = (int(v) for v in spec.split(","))
+    bits = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
+    c = M.uniform_coords(m, m, m)
+    qp = M.qp_coords(c, m, m, m)
+    cen, r = M.random_sinkers(8, 1, 0.1)
+    S = StokesSolver(m, m, m, bits, nlevels=min(4, max_levels(m)), rtol=1e-12, max_it=its,
+                     mg_precision=PREC_F32 if prec == 32 else PREC_F64, schur_eta=SCHUR_ETA_GEOMEAN)
+    S.setup(c, M.sinker_eta(qp, cen, r, 1.0, 1e4))
+    S.set_rhs_body_force(M.sinker_density(qp, cen, r, 1.0, 1.01))
+    u, p, st = S.solve(raise_on_noconv=False)
+    torch.cuda.synchronize()
+    print(f"{st['iterations']} iterations, |r|/|r0| = {st['rfinal'] / st['r0']:.3e}, "
+          f"setup {st['setup_ms']:.1f} ms, solve {st['solve_ms']:.1f} ms")
+    S.destroy()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -840,7 +884,11 @@ def main():
     ap.add_argument("--slabs", action="store_true", help="run the multi-GPU z-slab path on a single rank")
     ap.add_argument("--size", type=int, default=96, help="elements per direction")
     ap.add_argument("--workload", default="deformed", choices=["deformed", "layered"])
+    ap.add_argument("--profile-solve", default=None, metavar="M,ITS,PREC",
+                    help="run one short solve for profiling its launches, print one line, no benchmark")
     args = ap.parse_args()
+    if args.profile_solve:
+        return profile_solve(args.profile_solve)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -149,8 +149,10 @@ int p3d_op_set_host_chunks(p3d_op *op, int chunks);
  * device array of P3D_NOALLOC_MAX_DOFS doubles each, resident on every device
  * that loads the library until the process exits; larger meshes return
  * P3D_ERR_ARG.  The first call on a device looks up that array's address
- * (cudaGetSymbolAddress), so make it before any stream capture.  Calls share
- * the array: calls whose work overlaps on the GPU race. */
+ * (cudaGetSymbolAddress), so make it before any stream capture; that address
+ * is kept, so do not use this entry point again after resetting the device
+ * (cudaDeviceReset) in the same process.  Calls share the array: calls whose
+ * work overlaps on the GPU race. */
 #define P3D_NOALLOC_MAX_DOFS 107811 /* 3 * 33^3: a 16^3-element Q2 mesh */
 int p3d_a11_apply_host_noalloc(p3d_op *op, const double *x_host, double *y_host);
 

@@ -34,12 +34,17 @@ _u8 = C.POINTER(C.c_uint8)
 
 
 def build(ref_dir: str | None = None, quiet: bool = True) -> None:
-    """Compile liboracle.so, and oracle/_ref when the pTatin3d tree is present."""
+    """Compile liboracle.so, and oracle/_ref from the pTatin3d source tree at
+    ref_dir (or $P3D_REFERENCE_DIR).  Without either, only the restatement is
+    built; a ref_dir that holds no src/ directory is an error."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=out)
-    ref_dir = ref_dir or os.environ.get("P3D_REFERENCE_DIR", "/root/reference")
-    if os.path.isdir(os.path.join(ref_dir, "src")):
-        subprocess.run(["make", "-C", HERE, "ref", f"REF_DIR={ref_dir}"], check=True, stdout=out)
+    ref_dir = ref_dir or os.environ.get("P3D_REFERENCE_DIR")
+    if not ref_dir:
+        return
+    if not os.path.isdir(os.path.join(ref_dir, "src")):
+        raise FileNotFoundError(f"pTatin3d source tree not found: {ref_dir}/src")
+    subprocess.run(["make", "-C", HERE, "ref", f"REF_DIR={ref_dir}"], check=True, stdout=out)
 
 
 def _p(a):

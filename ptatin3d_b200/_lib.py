@@ -21,6 +21,7 @@ SCHUR_ETA_QP, SCHUR_ETA_GEOMEAN = 0, 1
 COARSE_ETA_GEOMEAN, COARSE_ETA_Q1 = 0, 1
 MAX_RESTART = 120
 COARSE_MAX_DOFS = 16384
+NOALLOC_MAX_DOFS = 107811  # P3D_NOALLOC_MAX_DOFS
 GEOM_AUTO, GEOM_GENERAL, GEOM_AFFINE = 0, 1, 2
 BC_NONE, BC_MATMULT = 0, 1
 PROJ_NULL, PROJ_P0_ARITHMETIC, PROJ_Q1, PROJ_ONE2ONE, PROJ_P0_HARMONIC, PROJ_P0_GEOMETRIC = -1, 0, 1, 4, 10, 20

@@ -13,7 +13,9 @@
 // resident until the process exits.  Its device address is obtained with
 // cudaGetSymbolAddress the first time the entry point runs on a device (with
 // that device current); that first call should therefore come before any CUDA
-// stream capture.  All calls on a device share the one array, so calls whose
+// stream capture.  The address is kept for the life of the device's primary
+// context: a caller that resets the device (cudaDeviceReset) must not use this
+// entry point afterwards in the same process.  All calls on a device share the one array, so calls whose
 // work overlaps on the GPU (other host threads, other streams) race; the
 // entry point itself is synchronous.
 #include <cuda_runtime.h>
@@ -69,9 +71,10 @@ extern "C" int p3d_a11_apply_host_noalloc(p3d_op *op, const double *x_host, doub
   double *dx = scr, *dy = scr + P3D_NOALLOC_MAX_DOFS;
   cudaStream_t st = op->stream;
   if ((rc = cuda_check(cudaMemcpyAsync(dx, x_host, n * 8, cudaMemcpyHostToDevice, st), "H2D x"))) return rc;
-  // the array keeps the previous call's contents: y must start at zero
+  // the array keeps the previous call's contents: y must start at zero (nodes
+  // on brick faces are accumulated atomically; the rest are stored, y = A x)
   if ((rc = cuda_check(cudaMemsetAsync(dy, 0, n * 8, st), "zero y"))) return rc;
-  if ((rc = launch_a11<double>(op, dx, dy, st))) return rc;
+  if ((rc = launch_a11<double>(op, dx, dy, st, true))) return rc;
   if ((rc = cuda_check(cudaMemcpyAsync(y_host, dy, n * 8, cudaMemcpyDeviceToHost, st), "D2H y"))) return rc;
   return cuda_check(cudaStreamSynchronize(st), "noalloc apply sync");
 }

@@ -12,6 +12,10 @@ int set_error(int code, const char *fmt, ...);
 int cuda_check(cudaError_t e, const char *what);
 void count_launch(int n);
 int dev_alloc(void **p, size_t bytes, const char *what);
+// Entry points that read caller device arrays on a library stream first wait
+// for all work the caller queued on the device (any stream), so that the
+// arrays are complete when the library's copies read them.
+int order_after_caller();
 } // namespace p3d
 
 struct p3d_op {
@@ -47,4 +51,7 @@ int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_
                    int tzb = 0, int tze = -1);
 // brick layer height along z of the A11 path the operator uses
 int a11_brick_height(const p3d_op *op);
+// coefficient setup from device FP64 arrays on op->stream (no ordering against
+// other streams: the caller orders the arrays' producers first)
+int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geom_mode);
 } // namespace p3d

@@ -35,6 +35,7 @@ int cuda_check(cudaError_t e, const char *what)
   return set_error(P3D_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 void count_launch(int n) { g_launches += n; }
+int order_after_caller() { return cuda_check(cudaDeviceSynchronize(), "wait for the caller's device work"); }
 
 static std::once_flag g_tables_once;
 static int upload_tables()
@@ -394,6 +395,7 @@ int p3d_op_set_coefficients_device(p3d_op *op, const double *coords, const doubl
   if (!op || !coords || !eta) return set_error(P3D_ERR_ARG, "set_coefficients: null argument");
   if (geom_mode < P3D_GEOM_AUTO || geom_mode > P3D_GEOM_AFFINE) return set_error(P3D_ERR_ARG, "bad geometry mode");
   cudaSetDevice(op->device);
+  if (int rc = order_after_caller()) return rc; // coords/eta may still be being written on the caller's stream
   return op_setup_device(op, coords, eta, geom_mode);
 }
 
@@ -408,7 +410,8 @@ int p3d_op_set_coefficients(p3d_op *op, const double *coords, const double *eta,
   if (!rc) rc = dev_alloc(&de, 27 * nel * 8, "eta staging");
   if (!rc) rc = cuda_check(cudaMemcpyAsync(dc, coords, 3 * nn * 8, cudaMemcpyHostToDevice, op->stream), "H2D coords");
   if (!rc) rc = cuda_check(cudaMemcpyAsync(de, eta, 27 * nel * 8, cudaMemcpyHostToDevice, op->stream), "H2D eta");
-  if (!rc) rc = p3d_op_set_coefficients_device(op, (const double *)dc, (const double *)de, geom_mode);
+  if (!rc && (geom_mode < P3D_GEOM_AUTO || geom_mode > P3D_GEOM_AFFINE)) rc = set_error(P3D_ERR_ARG, "bad geometry mode");
+  if (!rc) rc = op_setup_device(op, (const double *)dc, (const double *)de, geom_mode); // same stream as the copies
   cudaStreamSynchronize(op->stream);
   if (dc) cudaFree(dc);
   if (de) cudaFree(de);

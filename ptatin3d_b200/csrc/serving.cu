@@ -27,6 +27,7 @@
 
 #include "p3d_b200.h"
 #include "p3d_internal.h"
+#include "solver_internal.h"
 
 namespace p3d {
 
@@ -117,11 +118,11 @@ static int run_request(Slot *s, const p3d_request &r, p3d_result &res)
   if (!rc) rc = cuda_check(cudaMemsetAsync(s->u, 0, 3 * nn * 8, io), "zero u");
   if (!rc) rc = cuda_check(cudaMemsetAsync(s->p, 0, 4 * nel * 8, io), "zero p");
   if (!rc) rc = cuda_check(cudaStreamSynchronize(io), "h2d sync");
-  if (!rc) rc = p3d_solver_setup(s->solver, s->coords, s->eta);
-  if (!rc) rc = p3d_solver_set_rhs_body_force(s->solver, s->rho, r.gx, r.gy, r.gz);
+  if (!rc) rc = solver_setup_nowait(s->solver, s->coords, s->eta); // ordered by the io sync above
+  if (!rc) rc = solver_rhs_body_force_nowait(s->solver, s->rho, r.gx, r.gy, r.gz);
   p3d_solve_stats st;
   memset(&st, 0, sizeof st);
-  int srv = rc ? rc : p3d_solver_solve(s->solver, s->u, s->p, &st);
+  int srv = rc ? rc : solver_solve_nowait(s->solver, s->u, s->p, &st);
   if (!rc && (srv == P3D_OK || srv == P3D_ERR_NOCONV)) {
     rc = cuda_check(cudaMemcpyAsync(r.u, s->u, 3 * nn * 8, cudaMemcpyDeviceToHost, io), "d2h u");
     if (!rc) rc = cuda_check(cudaMemcpyAsync(r.p, s->p, 4 * nel * 8, cudaMemcpyDeviceToHost, io), "d2h p");

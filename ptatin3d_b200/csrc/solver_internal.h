@@ -56,6 +56,15 @@ void g_dirichlet(int nx, int ny, int nz, uint32_t dir, double *G, cudaStream_t s
 void g_diag(int nx, int ny, int nz, const double *G, double *d, cudaStream_t s);
 void g_dense(int nx, int ny, int nz, const double *G, double *M, cudaStream_t s);
 
+// stokes_solver.cu: the solver entry points without the wait for the
+// caller's device work (the server orders its own copies first)
+} // namespace p3d
+struct p3d_solver;
+namespace p3d {
+int solver_setup_nowait(p3d_solver *s, const double *coords, const double *eta);
+int solver_rhs_body_force_nowait(p3d_solver *s, const double *rho, double gx, double gy, double gz);
+int solver_solve_nowait(p3d_solver *s, double *u, double *p, struct p3d_solve_stats *stats);
+
 // dense_inverse.cu (coarse-grid operator, in place, blocked Gauss-Jordan)
 size_t dense_inverse_scratch(int n);
 int dense_inverse_spd(int n, double *A, double *scratch, cudaStream_t s);

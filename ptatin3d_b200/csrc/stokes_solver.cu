@@ -513,11 +513,11 @@ static int solver_setup(p3d_solver *s, const double *coords, const double *eta, 
       p3d_mesh_desc d;
       p3d_mesh_desc_whole(L.m[0], L.m[1], L.m[2], s->mesh.dirichlet, &d);
       if (!L.op64) CK(p3d_op_create(&d, P3D_PREC_F64, s->device, &L.op64));
-      CK(p3d_op_set_coefficients_device(L.op64, L.coords, L.eta, P3D_GEOM_AUTO));
+      CK(op_setup_device(L.op64, L.coords, L.eta, P3D_GEOM_AUTO)); // level arrays written on s->st, synchronized above
       CK(p3d_op_set_bc_mode(L.op64, P3D_BC_MATMULT));
       if (mixed && l > 0) {
         if (!L.op32) CK(p3d_op_create(&d, P3D_PREC_F32, s->device, &L.op32));
-        CK(p3d_op_set_coefficients_device(L.op32, L.coords, L.eta, P3D_GEOM_AUTO));
+        CK(op_setup_device(L.op32, L.coords, L.eta, P3D_GEOM_AUTO));
         CK(p3d_op_set_bc_mode(L.op32, P3D_BC_MATMULT));
       }
       CU(cudaMemsetAsync(L.t, 0, L.nv * 8, s->st), "memset");
@@ -818,6 +818,7 @@ int p3d_solver_setup(p3d_solver *s, const double *coords, const double *eta)
 {
   if (!s || !coords || !eta) return set_error(P3D_ERR_ARG, "solver_setup: null argument");
   cudaSetDevice(s->device);
+  CK(order_after_caller());
   return solver_setup(s, coords, eta, nullptr);
 }
 
@@ -828,10 +829,49 @@ int p3d_solver_setup_nodal(p3d_solver *s, const double *coords, const double *et
     return set_error(P3D_ERR_ARG, "solver_setup_nodal: the nodal viscosity feeds only the Q1 coefficient hierarchy "
                                   "(coarse_op P3D_COARSE_REDISC, coarse_eta P3D_COARSE_ETA_Q1, nlevels >= 2)");
   cudaSetDevice(s->device);
+  CK(order_after_caller());
   return solver_setup(s, coords, eta, eta_nodes);
 }
 
 int p3d_solver_set_rhs_body_force(p3d_solver *s, const double *rho, double gx, double gy, double gz)
+{
+  if (!s || !rho) return set_error(P3D_ERR_ARG, "set_rhs_body_force: null argument");
+  cudaSetDevice(s->device);
+  CK(order_after_caller());
+  return solver_rhs_body_force_nowait(s, rho, gx, gy, gz);
+}
+
+int p3d_solver_set_rhs(p3d_solver *s, const double *bu, const double *bp)
+{
+  if (!s || !bu || !bp) return set_error(P3D_ERR_ARG, "set_rhs: null argument");
+  cudaSetDevice(s->device);
+  CK(order_after_caller());
+  CU(cudaMemcpyAsync(s->bvec, bu, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "rhs u");
+  CU(cudaMemcpyAsync(s->bvec + s->nu, bp, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "rhs p");
+  s->rhs_set = true;
+  return cuda_check(cudaStreamSynchronize(s->st), "rhs");
+}
+
+int p3d_solver_solve(p3d_solver *s, double *u, double *p, p3d_solve_stats *stats)
+{
+  if (!s || !u || !p) return set_error(P3D_ERR_ARG, "solve: null argument");
+  cudaSetDevice(s->device);
+  CK(order_after_caller()); // the initial guess may still be being written on the caller's stream
+  return solver_solve_nowait(s, u, p, stats);
+}
+
+} // extern "C"
+
+namespace p3d {
+
+int solver_setup_nowait(p3d_solver *s, const double *coords, const double *eta)
+{
+  if (!s || !coords || !eta) return set_error(P3D_ERR_ARG, "solver_setup: null argument");
+  cudaSetDevice(s->device);
+  return solver_setup(s, coords, eta, nullptr);
+}
+
+int solver_rhs_body_force_nowait(p3d_solver *s, const double *rho, double gx, double gy, double gz)
 {
   if (!s || !rho) return set_error(P3D_ERR_ARG, "set_rhs_body_force: null argument");
   if (!s->setup_done) return set_error(P3D_ERR_STATE, "set_rhs_body_force before setup");
@@ -844,16 +884,7 @@ int p3d_solver_set_rhs_body_force(p3d_solver *s, const double *rho, double gx, d
   return cuda_check(cudaStreamSynchronize(s->st), "rhs");
 }
 
-int p3d_solver_set_rhs(p3d_solver *s, const double *bu, const double *bp)
-{
-  if (!s || !bu || !bp) return set_error(P3D_ERR_ARG, "set_rhs: null argument");
-  CU(cudaMemcpyAsync(s->bvec, bu, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "rhs u");
-  CU(cudaMemcpyAsync(s->bvec + s->nu, bp, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "rhs p");
-  s->rhs_set = true;
-  return cuda_check(cudaStreamSynchronize(s->st), "rhs");
-}
-
-int p3d_solver_solve(p3d_solver *s, double *u, double *p, p3d_solve_stats *stats)
+int solver_solve_nowait(p3d_solver *s, double *u, double *p, p3d_solve_stats *stats)
 {
   if (!s || !u || !p) return set_error(P3D_ERR_ARG, "solve: null argument");
   if (!s->setup_done || !s->rhs_set) return set_error(P3D_ERR_STATE, "solve before setup / rhs");
@@ -879,10 +910,16 @@ int p3d_solver_solve(p3d_solver *s, double *u, double *p, p3d_solve_stats *stats
   return P3D_OK;
 }
 
+} // namespace p3d
+
+extern "C" {
+
 int p3d_solver_apply_pc(p3d_solver *s, const double *ru, const double *rp, double *zu, double *zp)
 {
   if (!s || !ru || !rp || !zu || !zp) return set_error(P3D_ERR_ARG, "apply_pc: null argument");
   if (!s->setup_done) return set_error(P3D_ERR_STATE, "apply_pc before setup");
+  cudaSetDevice(s->device);
+  CK(order_after_caller());
   CU(cudaMemcpyAsync(s->pc_in, ru, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
   CU(cudaMemcpyAsync(s->pc_in + s->nu, rp, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "copy");
   CK(run_pc(s, s->pc_in, s->w));
@@ -897,6 +934,7 @@ int p3d_solver_level_apply(p3d_solver *s, int level, const double *x, double *y)
   if (!s->setup_done) return set_error(P3D_ERR_STATE, "level_apply before setup");
   if (level < 0 || level >= (int)s->lv.size()) return set_error(P3D_ERR_ARG, "level_apply: no level %d", level);
   cudaSetDevice(s->device);
+  CK(order_after_caller());
   CK(a11<double>(s, s->lv[level], x, y));
   return cuda_check(cudaStreamSynchronize(s->st), "level_apply");
 }

@@ -13,7 +13,9 @@ import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {sys.argv[0]} <pTatin3d source tree>")
+ref = sys.argv[1]
 out = {}
 for exp in sorted(glob.glob(os.path.join(ref, "tests/integration/operator/**/expected"), recursive=True)):
     d = os.path.dirname(exp)

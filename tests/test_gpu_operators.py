@@ -373,6 +373,54 @@ def test_full_size_deformed_apply_matches_reference_kernel(cuda, reference_kerne
     assert abs(float(xd @ Aa - a @ Ax)) <= 1e-11 * float(a.norm() * Ax.norm())
 
 
+def test_c1_sinker_apply_matches_reference_kernel(cuda, reference_kernels):
+    """The plain-apply configuration exactly: a 16^3 mesh of affine hexahedra
+    (107,811 dofs), eta 1 with 1e3 inside 8 spheres of radius 0.1 whose centres
+    are uniform from the seed, x uniform in [-1, 1] from the same seed, free
+    slip on all six faces; the GPU MatMult (Dirichlet columns zeroed, rows
+    y_k = x_k) against MatMult_MFStokes_A11 over the reference's own
+    MFStokesWrapper_A11_AVX (src/stokes_operators.c:1142-1205,
+    src/stokes_operators_avx.c:206-315) on the same inputs."""
+    case = sinker_case(16, seed=1, nsph=8, radius=0.1, eta1=1e3)
+    assert case["x"].size == 107811
+    op = make_op(case)
+    assert op.geometry_mode == GEOM_AFFINE
+    y = torch.full((case["x"].size,), float("nan"), dtype=torch.float64, device="cuda")
+    op.mult(T(case["x"]), y)
+    reference_kernels.setup(case["dims"], case["coords"], case["eta"])
+    ref = matmult_a11(lambda v: reference_kernels.a11_raw(v, "avx"), case["x"], case["mask"])
+    assert rel(host(y), ref) <= TOL64
+    # the raw element apply (SpMVOp contract, y += A x) as well
+    y0 = np.random.default_rng(2).uniform(-1, 1, size=case["x"].size)
+    z = T(y0)
+    op.spmv(T(case["x"]), z)
+    assert rel(host(z), y0 + reference_kernels.a11_raw(case["x"], "avx")) <= TOL64
+
+
+def test_c3_layered_apply_matches_reference_kernel(cuda, reference_kernels):
+    """The layered 64^3 configuration (6.4M dofs; log10 eta uniform in [-3, 3]
+    per each of 6 horizontal layers plus 16 inclusions) on the affine path, in
+    FP64 against the reference's MFStokesWrapper_A11_AVX, and the FP32
+    operator against the FP64 one."""
+    m = 64
+    c = M.uniform_coords(m, m, m)
+    eta = M.layered_eta(M.qp_coords(c, m, m, m), seed=4)
+    case = dict(dims=(m, m, m), coords=c, eta=eta, bits=M.FREE_SLIP, mask=M.dirichlet_mask(m, m, m, M.FREE_SLIP))
+    x = np.random.default_rng(4).uniform(-1.0, 1.0, size=c.size)
+    op = make_op(case)
+    assert op.geometry_mode == GEOM_AFFINE
+    y = torch.empty(x.size, dtype=torch.float64, device="cuda")
+    op.mult(T(x), y)
+    y64 = host(y)
+    reference_kernels.setup((m, m, m), c, eta)
+    ref = matmult_a11(lambda v: reference_kernels.a11_raw(v, "avx"), x, case["mask"])
+    assert rel(y64, ref) <= TOL64
+    op32 = make_op(case, prec=PREC_F32)
+    y32 = torch.empty(x.size, dtype=torch.float32, device="cuda")
+    op32.mult(T(x, torch.float32), y32)
+    assert rel(host(y32), y64) <= TOL32
+
+
 @pytest.mark.parametrize("dims", [(13, 7, 5), (1, 1, 1), (9, 5, 3), (8, 4, 2)])
 def test_fp32_general_ragged(cuda, dims):
     """The FP32 general A11 kernel on ragged meshes (bricks cut by the mesh
