@@ -655,6 +655,14 @@ def run_b200(args):
     for _ in range(npg):
         check(L.p3d_a11_apply_host(op.h, xpp, ypp))
     pg_value = world * ndof / reduce_max((time.perf_counter() - t0) / npg, world) / 1e9
+    # and with the operator page-locking those arrays on first use (kept across calls)
+    check(L.p3d_op_set_host_register(op.h, 1))
+    check(L.p3d_a11_apply_host(op.h, xpp, ypp))  # registers
+    t0 = time.perf_counter()
+    for _ in range(ne2e):
+        check(L.p3d_a11_apply_host(op.h, xpp, ypp))
+    pgr_value = world * ndof / reduce_max((time.perf_counter() - t0) / ne2e, world) / 1e9
+    check(L.p3d_op_set_host_register(op.h, 0))
     # the pipelined host-buffer result is the device MatMult's
     check(L.p3d_a11_mult(op.h, xp, yp, sp))
     torch.cuda.synchronize()
@@ -730,7 +738,10 @@ def run_b200(args):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * ndof, "d2h_bytes_per_step": 8 * ndof,
                         "rel_diff_vs_device": e2e_diff, "host_buffers": "pinned",
                         "pageable": {"value": pg_value, "unit": UNIT, "steps": npg,
-                                     "sample": "the same call on pageable numpy arrays"}},
+                                     "sample": "the same call on pageable numpy arrays"},
+                        "pageable_registered": {"value": pgr_value, "unit": UNIT, "steps": ne2e,
+                                                "sample": "pageable numpy arrays page-locked by the operator on "
+                                                          "first use (p3d_op_set_host_register), kept across calls"}},
                 "gpu_launches": launches,
                 "clocks": clk.summary(),
                 "fp32_apply": {"ms": f32_ms, "GDoF/s": ndof / (f32_ms * 1e-3) / 1e9,

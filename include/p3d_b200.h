@@ -141,6 +141,16 @@ int p3d_a11_apply_host(p3d_op *op, const double *x_host, double *y_host);
  * automatic: 16 for meshes of 4M dofs and more, else 1) whose host->device
  * copies, applies and device->host copies overlap on three streams. */
 int p3d_op_set_host_chunks(p3d_op *op, int chunks);
+/* enable != 0: p3d_a11_apply_host page-locks (cudaHostRegister) each host
+ * array it is given that is not page-locked yet, once, and keeps it so, which
+ * lets the copies of every later apply run at full PCIe speed.  The reference
+ * backend copies PETSc's pageable local arrays on every MatMult
+ * (src/stokes_operators_cuda.cu:403,453); a MatShell binding that reuses the
+ * DM's local vectors turns this on once.  Registered arrays must stay
+ * allocated until the operator is destroyed or this is called with enable = 0,
+ * which unregisters them (at most 16 ranges per operator; beyond that, and
+ * where registration fails, the copies go the pageable way). */
+int p3d_op_set_host_register(p3d_op *op, int enable);
 
 /* Same result as p3d_a11_apply_host, without allocating any device memory
  * (no counterpart in the reference).  For callers that may not call

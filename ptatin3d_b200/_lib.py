@@ -117,6 +117,7 @@ _SIGS = {
     "p3d_stokes_apply": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_a11_apply_host": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_a11_apply_host_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "p3d_op_set_host_register": ([C.c_void_p, C.c_int], C.c_int),
     "p3d_mg_prolong": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_mg_restrict": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_marker_project_workspace": ([C.c_int32, C.c_int32, C.c_int32, C.c_int, C.POINTER(C.c_int64)], C.c_int),

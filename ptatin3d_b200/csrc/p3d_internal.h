@@ -36,6 +36,10 @@ struct p3d_op {
   cudaStream_t s_h2d = nullptr, s_d2h = nullptr; // host-apply copy streams
   cudaEvent_t ev[32] = {};                      // host-apply chunk events (16 chunks x {x in, y done})
   int host_chunks = 0;                           // 0: automatic
+  bool host_register = false;                    // page-lock the host arrays p3d_a11_apply_host is given
+  int n_reg = 0;                                 // host ranges this operator registered
+  void *reg_ptr[16] = {};
+  size_t reg_bytes[16] = {};
   void *res_u = nullptr;                         // residual: u with the Dirichlet values inserted
   cudaStream_t stream = nullptr;     // setup / host-apply stream
 };

@@ -372,6 +372,7 @@ int p3d_op_destroy(p3d_op *op)
 {
   if (!op) return P3D_OK;
   cudaSetDevice(op->device);
+  p3d_op_set_host_register(op, 0);
   free_dev(op->coords);
   free_dev(op->kgen);
   free_dev(op->kgq);
@@ -546,6 +547,48 @@ int p3d_op_set_host_chunks(p3d_op *op, int chunks)
   return P3D_OK;
 }
 
+int p3d_op_set_host_register(p3d_op *op, int enable)
+{
+  if (!op) return set_error(P3D_ERR_ARG, "set_host_register: null operator");
+  if (!enable) {
+    cudaSetDevice(op->device);
+    for (int i = 0; i < op->n_reg; i++) cudaHostUnregister(op->reg_ptr[i]);
+    op->n_reg = 0;
+  }
+  op->host_register = enable != 0;
+  return P3D_OK;
+}
+
+} // extern "C"
+
+namespace p3d {
+// Page-lock [p, p + bytes) once, so that the copies of later applies run at
+// full PCIe speed instead of through the driver's pageable staging.  Memory
+// that is already page-locked (by the caller or an earlier call) is left
+// alone; a failed registration is not an error (the copy then goes the
+// pageable way).
+static void host_register_range(p3d_op *op, const void *p, size_t bytes)
+{
+  const char *c = (const char *)p;
+  for (int i = 0; i < op->n_reg; i++) {
+    const char *r = (const char *)op->reg_ptr[i];
+    if (c >= r && c + bytes <= r + op->reg_bytes[i]) return;
+  }
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type != cudaMemoryTypeUnregistered) return;
+  cudaGetLastError();
+  if (op->n_reg >= 16) return;
+  if (cudaHostRegister(const_cast<void *>(p), bytes, cudaHostRegisterDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  op->reg_ptr[op->n_reg] = const_cast<void *>(p);
+  op->reg_bytes[op->n_reg++] = bytes;
+}
+} // namespace p3d
+
+extern "C" {
+
 int p3d_a11_apply_host(p3d_op *op, const double *xh, double *yh)
 {
   P3D_REQUIRE_SETUP(op);
@@ -555,6 +598,10 @@ int p3d_a11_apply_host(p3d_op *op, const double *xh, double *yh)
   const p3d_mesh_desc &m = op->m;
   const size_t P = 3ull * m.gx * m.gy, n = P * m.gz; // doubles per lattice plane, in total
   int rc;
+  if (op->host_register) {
+    host_register_range(op, xh, n * 8);
+    host_register_range(op, yh, n * 8);
+  }
   if (!op->hx && (rc = dev_alloc(&op->hx, n * 8, "host-apply x"))) return rc;
   if (!op->hy && (rc = dev_alloc(&op->hy, n * 8, "host-apply y"))) return rc;
   if (!op->s_h2d) {

@@ -265,6 +265,29 @@ def test_host_apply_chunked_pipeline(cuda, restatement, dims, deform, chunks):
     assert rel(y, ref) <= TOL64
 
 
+def test_host_apply_registered_pageable(cuda, restatement):
+    """p3d_a11_apply_host on pageable arrays, with the operator page-locking
+    them on first use: the same result as without, on repeated calls, and the
+    arrays are released again when registration is switched off."""
+    from ptatin3d_b200 import _lib
+    case = sinker_case(10, deform=0.2)
+    op = make_op(case)
+    _lib.check(_lib.lib().p3d_op_set_bc_mode(op.h, _lib.BC_MATMULT))
+    x = np.ascontiguousarray(case["x"])
+    y0 = np.full(x.size, np.nan)
+    op.mult_host(x, y0, boundary=True)
+    y = np.empty(x.size)  # registered arrays stay allocated until registration is switched off
+    _lib.check(_lib.lib().p3d_op_set_host_register(op.h, 1))
+    for _ in range(3):
+        y[:] = np.nan
+        op.mult_host(x, y, boundary=True)
+        assert not np.isnan(y).any()
+        assert rel(y, y0) <= 1e-15
+    _lib.check(_lib.lib().p3d_op_set_host_register(op.h, 0))
+    d, c, e = case["dims"], case["coords"], case["eta"].reshape(-1)
+    assert rel(y0, matmult_a11(lambda v: restatement.a11_raw(d, c, e, v), x, case["mask"])) <= TOL64
+
+
 def test_operator_properties_large(cuda):
     """Size-independent properties at 64^3 (6.4M dofs): symmetry and linearity."""
     m = 64

@@ -263,3 +263,35 @@ def test_solver_rejects_bad_sizes(cuda):
         StokesSolver(8, 8, 8, BITS, restart=200)
     with pytest.raises(P3DError):
         StokesSolver(16, 16, 16, BITS, nlevels=1)  # coarse level too large for the dense inverse
+
+
+def test_setup_waits_for_arrays_written_on_the_callers_stream(cuda, restatement):
+    """Coordinates, viscosity and density produced on the caller's (torch's)
+    stream just before the calls, with a long queue of unrelated work ahead of
+    them: the library reads them on its own stream only after that work, so
+    the operators and the right-hand side equal those set up from host arrays."""
+    m = 8
+    c, eta, rho = sinker(m, deform=0.1)
+    busy = torch.rand(1 << 26, dtype=torch.float64, device="cuda")
+    for _ in range(40):  # ~0.1 s of queued work on the current stream
+        busy.mul_(1.0000001)
+    c_d = torch.tensor(c.reshape(-1), device="cuda") * 1.0  # written by kernels behind that queue
+    e_d = torch.tensor(eta.reshape(-1), device="cuda") * 1.0
+    r_d = torch.tensor(rho.reshape(-1), device="cuda") * 1.0
+    S = StokesSolver(m, m, m, BITS, nlevels=2, rtol=1e-9, max_it=200)
+    S.setup(c_d, e_d)
+    S.set_rhs_body_force(r_d)
+    u_d, p_d, _ = S.solve()
+    H = StokesSolver(m, m, m, BITS, nlevels=2, rtol=1e-9, max_it=200)
+    H.setup(c, eta)
+    H.set_rhs_body_force(rho)
+    u_h, p_h, _ = H.solve()
+    x = np.random.default_rng(0).uniform(-1, 1, size=c.size)
+    yd, yh = S.level_apply(1, x), H.level_apply(1, x)
+    assert rel(yd.cpu().numpy(), yh.cpu().numpy()) <= 1e-14  # brick-face atomics: rounding-order differences only
+    # both solves stop at rtol 1e-9 on the same system; their iterates differ by
+    # the summation order of the atomics, amplified by the conditioning
+    assert rel(u_d.cpu().numpy(), u_h.cpu().numpy()) <= 1e-5
+    assert rel(p_d.cpu().numpy(), p_h.cpu().numpy()) <= 1e-5
+    S.destroy()
+    H.destroy()
