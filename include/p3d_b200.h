@@ -245,8 +245,7 @@ typedef struct p3d_solver_opts {
   int32_t inner_its;    /* velocity-block solve inside the preconditioner: 0 = one
                            V-cycle; k > 0 = k conjugate-gradient iterations on A11
                            preconditioned by the V-cycle (the reference's inner
-                           -fieldsplit_u_ksp, run for a fixed count so that it
-                           stays inside the captured graph)                       */
+                           -fieldsplit_u_ksp); with inner_rtol > 0, at most k    */
   int32_t coarse_op;    /* operators of the coarse levels: P3D_COARSE_GALERKIN
                            (P^T A P, 27-point block stencils probed from the
                            finer level) or P3D_COARSE_REDISC (matrix-free
@@ -261,6 +260,13 @@ typedef struct p3d_solver_opts {
                            finer Gauss points) or P3D_COARSE_ETA_Q1 (the
                            reference's Q1 projection hierarchy: nodal projection,
                            scaled restriction, clamped interpolation)            */
+  double inner_rtol;    /* > 0: the inner conjugate gradients stop once
+                           |b - A11 x| <= inner_rtol |b| (-fieldsplit_u_ksp_rtol,
+                           1e-2 in the reference's sinker tests) or after
+                           inner_its iterations.  The loop runs on the device: a
+                           conditional WHILE node of the captured preconditioner
+                           graph, its condition set from the device-held residual.
+                           0: a fixed inner_its iterations                        */
 } p3d_solver_opts;
 
 #define P3D_COARSE_ETA_GEOMEAN 0
@@ -280,6 +286,8 @@ typedef struct p3d_solve_stats {
   double setup_ms, solve_ms;
   double lmax_fine;     /* estimated lmax(D^{-1}A) on the finest level              */
   int32_t coarse_dofs;
+  int32_t inner_iterations; /* inner conjugate-gradient iterations of the solve
+                               (tolerance-driven inner solves; 0 otherwise)      */
 } p3d_solve_stats;
 
 int p3d_solver_default_opts(p3d_solver_opts *opts);

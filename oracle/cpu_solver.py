@@ -106,8 +106,9 @@ class _Level:
 
 class CpuStokesSolver:
     def __init__(self, m, coords, eta, rho, bits, nlevels=4, cheb_its=3, cheb_lo=0.2, cheb_hi=1.1, esteig=10,
-                 restart=30, threads=None, schur_geomean=True, g=(0.0, 0.0, -1.0)):
+                 restart=30, threads=None, schur_geomean=True, g=(0.0, 0.0, -1.0), inner_rtol=0.0, inner_its=0):
         t0 = time.perf_counter()
+        self.inner_rtol, self.inner_its, self.inner_total = inner_rtol, inner_its, 0
         self.K, self.lo, self.hi, self.restart = cheb_its, cheb_lo, cheb_hi, restart
         dims = tuple(m) if isinstance(m, (tuple, list)) else (m, m, m)  # elements per direction
         nf = tuple(2 * d + 1 for d in dims)
@@ -239,11 +240,34 @@ class CpuStokesSolver:
         yu[m] = u[m]
         return np.concatenate([yu, yp])
 
+    def velocity(self, b):
+        """A11^-1 b: one V-cycle, or (inner_rtol > 0) conjugate gradients on
+        A11 preconditioned by the V-cycle until |b - A x| <= inner_rtol |b| or
+        inner_its iterations, in the device's order of operations (p starts at
+        0 with rz_old = 1, so the first direction is z)."""
+        if self.inner_rtol <= 0.0:
+            return self.vcycle(b)
+        A = self.lv[-1].A
+        x, r, p = np.zeros_like(b), b.copy(), np.zeros_like(b)
+        tol2 = self.inner_rtol ** 2 * (b @ b)
+        rz_old, rr, k = 1.0, b @ b, 0
+        while rr > tol2 and k < self.inner_its:
+            z = self.vcycle(r)
+            rz = r @ z
+            p = z + (rz / rz_old) * p
+            q = A(p)
+            a = rz / (p @ q)
+            x += a * p
+            r -= a * q
+            rr, rz_old, k = r @ r, rz, k + 1
+        self.inner_total += k
+        return x
+
     def pc(self, x):
         ru, rp = x[:self.nu], x[self.nu:]
         zp = np.einsum("eij,ej->ei", self.Binv, rp.reshape(-1, 4)).reshape(-1)
         t = ru - matmult_a12(self.ref.a12_avx_raw, zp, self.mask_u8)
-        return np.concatenate([self.vcycle(t), zp])
+        return np.concatenate([self.velocity(t), zp])
 
     def solve(self, rtol=1e-6, max_it=1000):
         """FGMRES from x = 0; returns (u, p, iterations, |r|/|r0|, seconds)."""

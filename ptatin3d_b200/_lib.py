@@ -50,7 +50,7 @@ class SolverOpts(C.Structure):
                 ("esteig_its", C.c_int32), ("mg_precision", C.c_int32), ("restart", C.c_int32),
                 ("max_it", C.c_int32), ("rtol", C.c_double), ("atol", C.c_double), ("use_graph", C.c_int32),
                 ("verbose", C.c_int32), ("inner_its", C.c_int32), ("coarse_op", C.c_int32),
-                ("schur_eta", C.c_int32), ("coarse_eta", C.c_int32)]
+                ("schur_eta", C.c_int32), ("coarse_eta", C.c_int32), ("inner_rtol", C.c_double)]
 
 
 class Request(C.Structure):
@@ -74,7 +74,7 @@ class ServerStats(C.Structure):
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("r0", C.c_double), ("rfinal", C.c_double),
                 ("setup_ms", C.c_double), ("solve_ms", C.c_double), ("lmax_fine", C.c_double),
-                ("coarse_dofs", C.c_int32)]
+                ("coarse_dofs", C.c_int32), ("inner_iterations", C.c_int32)]
 
 
 _lib = None

@@ -66,7 +66,8 @@ struct p3d_solver {
   // inner conjugate gradient on A11 (MG precision vectors, device-held scalars)
   void *cg_r = nullptr, *cg_z = nullptr, *cg_p = nullptr, *cg_q = nullptr;
   void **cg_ptr = nullptr; // device pointers {p, r} for the dot kernels
-  double *cg_sc = nullptr; // {rz (2 slots, alternating), pq}
+  double *cg_sc = nullptr; // fixed count: {rz (2 slots, alternating), pq}; tolerance: see CG_* below
+  cudaStream_t st_body = nullptr; // side stream on which the inner loop's body is captured
   // preconditioner buffers (fixed for graph capture)
   double *pc_in = nullptr, *pc_out = nullptr, *pc_t = nullptr;
   double *xsol = nullptr; // [u; p] iterate of a solve
@@ -173,8 +174,10 @@ template <typename T> static int vcycle(p3d_solver *s, int l, const T *b, T *x)
 // coarse solve), x_0 = 0.  The step lengths never leave the device, so the
 // whole solve is one captured graph.  b may be overwritten (it is the CG
 // residual when it aliases cg_r).
+template <typename T> static int velocity_solve_rtol(p3d_solver *s, const T *b, T *x);
 template <typename T> static int velocity_solve(p3d_solver *s, const T *b, T *x)
 {
+  if (s->o.inner_rtol > 0.0) return velocity_solve_rtol<T>(s, b, x);
   const int top = (int)s->lv.size() - 1;
   const int K = s->o.inner_its;
   if (K <= 0) return vcycle<T>(s, top, b, x);
@@ -201,6 +204,130 @@ template <typename T> static int velocity_solve(p3d_solver *s, const T *b, T *x)
     v_cg_p<T>(n, rz_new, rz, z, p, s->st);
   }
   return P3D_OK;
+}
+
+// Scalars of the tolerance-driven inner CG (device memory, doubles).
+enum { CG_RZ_OLD = 0, CG_RZ_NEW, CG_PQ, CG_RR, CG_TOL2, CG_K, CG_TOTAL, CG_CONT, CG_NSC };
+
+// Start of the inner solve: |b|^2 is in sc[CG_RR].  Sets the stopping
+// threshold rtol^2 |b|^2, rz_old = 1 (p starts at 0, so the first direction
+// is z whatever beta is) and the loop condition.
+__global__ void k_cg_begin(double *sc, double rtol2, int kmax, cudaGraphConditionalHandle h, int use_handle)
+{
+  const double bb = sc[CG_RR];
+  sc[CG_TOL2] = rtol2 * bb;
+  sc[CG_RZ_OLD] = 1.0;
+  sc[CG_K] = 0.0;
+  const unsigned cont = (bb > 0.0 && isfinite(bb) && kmax > 0) ? 1u : 0u;
+  sc[CG_CONT] = (double)cont;
+  if (use_handle) cudaGraphSetConditional(h, cont);
+}
+// End of one inner iteration: |r|^2 is in sc[CG_RR].  Continue while
+// |r| > rtol |b| and fewer than kmax iterations ran (the loop always ends).
+__global__ void k_cg_end(double *sc, int kmax, cudaGraphConditionalHandle h, int use_handle)
+{
+  sc[CG_RZ_OLD] = sc[CG_RZ_NEW];
+  const double k = sc[CG_K] + 1.0;
+  sc[CG_K] = k;
+  sc[CG_TOTAL] += 1.0;
+  const double rr = sc[CG_RR];
+  const unsigned cont = (rr > sc[CG_TOL2] && isfinite(rr) && k < (double)kmax) ? 1u : 0u;
+  sc[CG_CONT] = (double)cont;
+  if (use_handle) cudaGraphSetConditional(h, cont);
+}
+
+// One iteration of the tolerance-driven inner CG (preconditioned by the V-cycle):
+//   z = MG(r); beta = r.z / rz_old; p = z + beta p; q = A p; alpha = r.z / p.q;
+//   x += alpha p; r -= alpha q; |r|^2
+template <typename T> static int inner_cg_body(p3d_solver *s, T *x, cudaGraphConditionalHandle h, int use_handle)
+{
+  const int top = (int)s->lv.size() - 1;
+  Level &F = s->lv.back();
+  const size_t n = F.nv;
+  T *r = (T *)s->cg_r, *z = (T *)s->cg_z, *p = (T *)s->cg_p, *q = (T *)s->cg_q;
+  const T *const *pp = (const T *const *)s->cg_ptr;     // {p}
+  const T *const *pr = (const T *const *)s->cg_ptr + 1; // {r}
+  double *sc = s->cg_sc;
+  CK(vcycle<T>(s, top, r, z));
+  v_mdot<T>(n, 1, pr, z, s->part, sc + CG_RZ_NEW, s->st);
+  v_cg_p<T>(n, sc + CG_RZ_NEW, sc + CG_RZ_OLD, z, p, s->st);
+  CK(a11<T>(s, F, p, q));
+  v_mdot<T>(n, 1, pp, q, s->part, sc + CG_PQ, s->st);
+  v_cg_xr<T>(n, sc + CG_RZ_NEW, sc + CG_PQ, x, r, p, q, true, s->st);
+  v_mdot<T>(n, 1, pr, r, s->part, sc + CG_RR, s->st);
+  k_cg_end<<<1, 1, 0, s->st>>>(sc, s->o.inner_its, h, use_handle);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "inner cg end");
+}
+
+// Velocity block solved to a relative tolerance: CG on A11 preconditioned by
+// the V-cycle until |b - A x| <= inner_rtol |b| or inner_its iterations (the
+// reference's inner -fieldsplit_u_ksp with -fieldsplit_u_ksp_rtol, there an
+// FGMRES; with a symmetric positive definite V-cycle CG needs no basis).
+// Inside a stream capture the loop becomes a conditional WHILE node whose
+// condition a one-thread kernel sets from the device-held residual, so the
+// whole preconditioner stays one graph; eagerly the host reads the
+// condition after each iteration.
+template <typename T> static int velocity_solve_rtol(p3d_solver *s, const T *b, T *x)
+{
+  Level &F = s->lv.back();
+  const size_t n = F.nv;
+  T *r = (T *)s->cg_r, *p = (T *)s->cg_p;
+  const T *const *pr = (const T *const *)s->cg_ptr + 1; // {r}
+  double *sc = s->cg_sc;
+  const double rtol2 = s->o.inner_rtol * s->o.inner_rtol;
+  const int kmax = s->o.inner_its;
+  cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+  CU(cudaStreamIsCapturing(s->st, &cst), "capture status");
+  const bool capturing = cst == cudaStreamCaptureStatusActive;
+  cudaGraphConditionalHandle h = 0;
+  cudaGraph_t g = nullptr;
+  if (capturing) {
+    CU(cudaStreamGetCaptureInfo(s->st, &cst, nullptr, &g, nullptr, nullptr), "capture info");
+    CU(cudaGraphConditionalHandleCreate(&h, g, 0, 0), "conditional handle");
+  }
+  if ((const void *)b != (const void *)r) CU(cudaMemcpyAsync(r, b, n * sizeof(T), cudaMemcpyDeviceToDevice, s->st), "copy");
+  CU(cudaMemsetAsync(x, 0, n * sizeof(T), s->st), "memset");
+  CU(cudaMemsetAsync(p, 0, n * sizeof(T), s->st), "memset");
+  v_mdot<T>(n, 1, pr, r, s->part, sc + CG_RR, s->st); // |b|^2
+  k_cg_begin<<<1, 1, 0, s->st>>>(sc, rtol2, kmax, h, capturing ? 1 : 0);
+  count_launch(1);
+  CU(cudaGetLastError(), "inner cg begin");
+  if (!capturing) {
+    for (int k = 0; k < kmax; k++) {
+      double cont = 0.0;
+      CU(cudaMemcpyAsync(&cont, sc + CG_CONT, 8, cudaMemcpyDeviceToHost, s->st), "d2h");
+      CU(cudaStreamSynchronize(s->st), "sync");
+      if (cont == 0.0) break;
+      CK(inner_cg_body<T>(s, x, h, 0));
+    }
+    return P3D_OK;
+  }
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  CU(cudaStreamGetCaptureInfo(s->st, &cst, nullptr, &g, &deps, &nd), "capture info");
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional}; // the other members zero
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cn = nullptr;
+  CU(cudaGraphAddNode(&cn, g, deps, nd, &cp), "conditional node");
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  // capture the body into the node's graph on the side stream
+  cudaStream_t main = s->st;
+  s->st = s->st_body;
+  int rc = cuda_check(cudaStreamBeginCaptureToGraph(s->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+                      "capture loop body");
+  if (!rc) {
+    rc = inner_cg_body<T>(s, x, h, 1);
+    cudaGraph_t out = nullptr;
+    const int rc2 = cuda_check(cudaStreamEndCapture(s->st, &out), "end loop body capture");
+    if (!rc) rc = rc2;
+  }
+  s->st = main;
+  if (rc) return rc;
+  return cuda_check(cudaStreamUpdateCaptureDependencies(main, &cn, 1, cudaStreamSetCaptureDependencies),
+                    "capture dependencies");
 }
 
 // block upper-triangular preconditioner: zp = S^{-1} rp ; zu = MG(ru - A12 zp)
@@ -685,6 +812,7 @@ int p3d_solver_default_opts(p3d_solver_opts *o)
   o->use_graph = 1;
   o->verbose = 0;
   o->inner_its = 0;
+  o->inner_rtol = 0.0;
   o->coarse_op = P3D_COARSE_GALERKIN;
   o->schur_eta = P3D_SCHUR_ETA_QP;
   o->coarse_eta = P3D_COARSE_ETA_GEOMEAN;
@@ -736,7 +864,8 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
     return set_error(P3D_ERR_ARG, "solver_create: the solver takes a whole mesh (no ghost layers)");
   if (o.nlevels < 1 || o.nlevels > 12 || o.restart < 1 || o.restart > P3D_MAX_RESTART || o.max_it < 1 ||
       o.cheb_its < 1 || !(o.cheb_hi > o.cheb_lo) || o.cheb_lo <= 0 || (o.mg_precision != 64 && o.mg_precision != 32) ||
-      o.inner_its < 0 || o.inner_its > 1000 || (o.coarse_op != P3D_COARSE_GALERKIN && o.coarse_op != P3D_COARSE_REDISC) ||
+      o.inner_its < 0 || o.inner_its > 1000 || !(o.inner_rtol >= 0.0 && o.inner_rtol < 1.0) ||
+      (o.inner_rtol > 0.0 && o.inner_its < 1) || (o.coarse_op != P3D_COARSE_GALERKIN && o.coarse_op != P3D_COARSE_REDISC) ||
       (o.schur_eta != P3D_SCHUR_ETA_QP && o.schur_eta != P3D_SCHUR_ETA_GEOMEAN) ||
       (o.coarse_eta != P3D_COARSE_ETA_GEOMEAN && o.coarse_eta != P3D_COARSE_ETA_Q1))
     return set_error(P3D_ERR_ARG, "solver_create: bad options");
@@ -798,12 +927,13 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
     if (!rc) rc = dev_alloc(&s->cg_p, s->nu * 8, "cg p");
     if (!rc) rc = dev_alloc(&s->cg_q, s->nu * 8, "cg q");
     if (!rc) rc = dev_alloc((void **)&s->cg_ptr, 2 * sizeof(void *), "cg ptrs");
-    if (!rc) rc = dev_alloc((void **)&s->cg_sc, 4 * 8, "cg scalars");
+    if (!rc) rc = dev_alloc((void **)&s->cg_sc, CG_NSC * 8, "cg scalars");
     if (!rc) {
       void *ptrs[2] = {s->cg_p, s->cg_r};
       rc = cuda_check(cudaMemcpy(s->cg_ptr, ptrs, sizeof ptrs, cudaMemcpyHostToDevice), "cg ptrs");
     }
-    if (!rc) rc = cuda_check(cudaMemset(s->cg_sc, 0, 4 * 8), "cg scalars");
+    if (!rc) rc = cuda_check(cudaMemset(s->cg_sc, 0, CG_NSC * 8), "cg scalars");
+    if (!rc) rc = cuda_check(cudaStreamCreateWithFlags(&s->st_body, cudaStreamNonBlocking), "body stream");
   }
   if (!rc) rc = cuda_check(cudaMemset(s->bvec, 0, N * 8), "rhs zero");
   if (rc) {
@@ -895,7 +1025,14 @@ int solver_solve_nowait(p3d_solver *s, double *u, double *p, p3d_solve_stats *st
   double *x = s->xsol;
   int rc = cuda_check(cudaMemcpyAsync(x, u, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "x u");
   if (!rc) rc = cuda_check(cudaMemcpyAsync(x + s->nu, p, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "x p");
+  if (!rc && s->cg_sc) rc = cuda_check(cudaMemsetAsync(s->cg_sc + CG_TOTAL, 0, 8, s->st), "inner count");
   if (!rc) rc = fgmres(s, x, &local);
+  if (!rc && s->cg_sc && s->o.inner_rtol > 0.0) {
+    double tot = 0.0;
+    rc = cuda_check(cudaMemcpyAsync(&tot, s->cg_sc + CG_TOTAL, 8, cudaMemcpyDeviceToHost, s->st), "inner count");
+    if (!rc) rc = cuda_check(cudaStreamSynchronize(s->st), "inner count");
+    local.inner_iterations = (int32_t)tot;
+  }
   if (!rc) rc = cuda_check(cudaMemcpyAsync(u, x, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "u out");
   if (!rc) rc = cuda_check(cudaMemcpyAsync(p, x + s->nu, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "p out");
   if (!rc) rc = cuda_check(cudaStreamSynchronize(s->st), "solve sync");
@@ -953,6 +1090,7 @@ int p3d_solver_destroy(p3d_solver *s)
                   (void *)s->cg_sc})
     if (p) cudaFree(p);
   if (s->hhost) cudaFreeHost(s->hhost);
+  if (s->st_body) cudaStreamDestroy(s->st_body);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
   return P3D_OK;

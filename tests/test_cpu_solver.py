@@ -1,6 +1,8 @@
 """The CPU restatement of the solver (oracle/cpu_solver.py, the CPU solve
 baseline of bench.py) solves the oracle's assembled Stokes system, and on the
 GPU it takes the same path as the device solver."""
+import os
+
 import numpy as np
 import pytest
 
@@ -73,3 +75,65 @@ def test_slab_partitioned_reference_apply(reference_kernels):
     assert t > 0.0
     reference_kernels.setup((m, m, m), c, eta)
     assert rel(y, reference_kernels.a11_raw(x, "avx")) <= 1e-12
+
+
+def _application_case(name):
+    import json
+
+    from cases import bump_case, sinker_markers
+    from oracle.oracle import marker_project
+    rec = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                      "application_expected.json")))[name]
+    case = bump_case(rec["mx"], rec["my"], rec["mz"])
+    wil, xi, eta_p, rho_p = sinker_markers(case, rec["eta0"], rec["eta1"], rec["rho0"], rec["rho1"])
+    eta_q, rho_q = marker_project(case["dims"], 1, wil, xi, eta_p, rho_p)
+    return rec, case, eta_q, rho_q
+
+
+def test_restatement_takes_the_reference_application_iteration_count(reference_kernels):
+    """The reference's viscous-sinker solve with its own solver options
+    (tests/application/linear/sinker_galerkin_8x8x8/opts: 3 levels, Galerkin
+    coarse operators, Chebyshev(10)/Jacobi, inner velocity solve to rtol 1e-2,
+    outer FGMRES to rtol 1e-3) converges in 17 outer iterations.  The host
+    restatement of the device solver (inner conjugate gradients instead of
+    FGMRES, exact 4x4 Schur blocks instead of their Jacobi diagonal) takes
+    that count to within 3 iterations.  PETSc is not vendored, so the count is
+    compared, not the history."""
+    from oracle.cpu_solver import CpuStokesSolver
+    rec, case, eta_q, rho_q = _application_case("sinker_galerkin_8x8x8")
+    assert rec["a11_operator_type"] == "2,2,0" and rec["outer_iterations"] == 17
+    S = CpuStokesSolver(case["dims"], case["coords"], eta_q, rho_q, case["bits"], nlevels=rec["nlevels"],
+                        cheb_its=rec["cheb_its"], schur_geomean=False, g=(0.0, 1.0, 0.0),
+                        inner_rtol=rec["inner_rtol"], inner_its=200)
+    _, _, its, rt, _ = S.solve(rtol=rec["ksp_rtol"], max_it=100)
+    assert rt <= rec["ksp_rtol"]
+    assert abs(its - rec["outer_iterations"]) <= 3, its
+    assert its <= S.inner_total <= 4 * its  # a few inner iterations per outer one, as the reference prints
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", [64, 32])
+def test_cpu_and_gpu_inner_solves_agree(cuda, reference_kernels, prec):
+    """With the velocity block solved to a relative tolerance by inner
+    conjugate gradients, the device solve (FP64, or FP32 multigrid) and the
+    host restatement take outer and total inner iteration counts within 15 %
+    of each other and reach the same solution."""
+    from oracle.cpu_solver import CpuStokesSolver
+    from ptatin3d_b200 import SCHUR_ETA_GEOMEAN
+    from ptatin3d_b200.solver import StokesSolver
+    m = 8
+    c, eta, rho = sinker(m, 1e3)
+    C = CpuStokesSolver(m, c, eta, rho, BITS, nlevels=3, inner_rtol=1e-2, inner_its=100)
+    uc, pc, itc, rtc, _ = C.solve(rtol=1e-9, max_it=500)
+    G = StokesSolver(m, m, m, BITS, nlevels=3, rtol=1e-9, max_it=500, schur_eta=SCHUR_ETA_GEOMEAN,
+                     inner_rtol=1e-2, inner_its=100, mg_precision=prec)
+    G.setup(c, eta)
+    G.set_rhs_body_force(rho)
+    ug, pg, st = G.solve()
+    assert rtc <= 1e-9 and st["converged"]
+    assert abs(st["iterations"] - itc) <= 0.15 * itc + 2
+    assert abs(st["inner_iterations"] - C.inner_total) <= 0.15 * C.inner_total + 3
+    assert st["inner_iterations"] > st["iterations"]
+    # a variable (inner-tolerance) preconditioner: both stop at rtol 1e-9 on
+    # different Krylov paths, so their solutions differ by the conditioning
+    assert rel(ug.cpu().numpy(), uc) <= 2e-5

@@ -30,15 +30,18 @@ def request(m, nsph, contrast, seed):
 
 
 def submit(S, m, arrays, tag, **kw):
-    return S.submit((m, m, m), BITS, *arrays, tag=tag, nlevels=max_levels(m), **OPTS, **kw)
+    return S.submit((m, m, m), BITS, *arrays, tag=tag, nlevels=max_levels(m), **dict(OPTS, **kw))
 
 
 def test_result_same_alone_and_in_the_mix(cuda):
+    # solved to rtol 1e-11: the rounding-order perturbation of the brick-face
+    # atomics, amplified by the FP32 preconditioner and the conditioning, then
+    # stays three orders below the 1e-7 compared here (at 1e-9 it reached 5e-7)
     A = request(16, 2, 1e2, 1)
     with StokesServer(hbm_budget=8 << 30, max_active=4) as S:
-        submit(S, 16, A, 0, mg_precision=PREC_F32)
+        submit(S, 16, A, 0, mg_precision=PREC_F32, rtol=1e-11)
         alone = S.wait_all()[0]
-        submit(S, 16, A, 100, mg_precision=PREC_F32)
+        submit(S, 16, A, 100, mg_precision=PREC_F32, rtol=1e-11)
         for t, (m, ns, cst) in enumerate([(8, 1, 1e3), (12, 3, 1e2), (24, 2, 1e2), (16, 4, 10.0), (8, 2, 1e2)]):
             submit(S, m, request(m, ns, cst, 10 + t), 200 + t, mg_precision=PREC_F32)
         res = {r["tag"]: r for r in S.wait_all()}
@@ -49,7 +52,7 @@ def test_result_same_alone_and_in_the_mix(cuda):
     assert rel(mixed["p"], alone["p"]) <= 1e-6
     assert st["completed"] == 7 and st["solvers_reused"] >= 1
     # and the same as a direct solve of the request through the solver API
-    D = StokesSolver(16, 16, 16, BITS, nlevels=max_levels(16), mg_precision=PREC_F32, **OPTS)
+    D = StokesSolver(16, 16, 16, BITS, nlevels=max_levels(16), mg_precision=PREC_F32, **dict(OPTS, rtol=1e-11))
     D.setup(A[0], A[1])
     D.set_rhs_body_force(A[2])
     u, p, _ = D.solve()

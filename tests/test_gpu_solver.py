@@ -295,3 +295,42 @@ def test_setup_waits_for_arrays_written_on_the_callers_stream(cuda, restatement)
     assert rel(p_d.cpu().numpy(), p_h.cpu().numpy()) <= 1e-5
     S.destroy()
     H.destroy()
+
+
+@pytest.mark.parametrize("prec", [PREC_F64, PREC_F32])
+def test_inner_tolerance_loop_graph_and_eager_agree(cuda, prec):
+    """The tolerance-driven inner velocity solve runs as a conditional WHILE
+    node inside the captured preconditioner graph, and as a host loop without
+    the graph: the same outer and inner iteration counts (up to the rounding
+    order of atomics) and the same solution."""
+    m = 16
+    c, eta, rho = sinker(m, nsph=4, radius=0.15, contrast=1e3)
+    out = {}
+    for graph in (1, 0):
+        S = StokesSolver(m, m, m, BITS, nlevels=3, rtol=1e-8, max_it=300, mg_precision=prec, inner_rtol=1e-2,
+                         inner_its=60, use_graph=graph, schur_eta=SCHUR_ETA_GEOMEAN)
+        S.setup(c, eta)
+        S.set_rhs_body_force(rho)
+        u, p, st = S.solve()
+        out[graph] = (u.cpu().numpy(), p.cpu().numpy(), st)
+        S.destroy()
+    (ug, pg, sg), (ue, pe, se) = out[1], out[0]
+    assert sg["converged"] and se["converged"]
+    assert abs(sg["iterations"] - se["iterations"]) <= 0.03 * se["iterations"] + 1
+    assert abs(sg["inner_iterations"] - se["inner_iterations"]) <= 0.03 * se["inner_iterations"] + 2
+    assert sg["iterations"] < sg["inner_iterations"] <= 60 * sg["iterations"]
+    assert rel(ug, ue) <= 1e-6 and rel(pg, pe) <= 1e-6
+
+
+def test_inner_tolerance_cap_ends_the_loop(cuda):
+    """An unreachable inner tolerance stops at inner_its iterations per
+    preconditioner application (the device loop's bound), and the outer
+    iteration still converges."""
+    m = 8
+    c, eta, rho = sinker(m, contrast=1e2)
+    S = StokesSolver(m, m, m, BITS, nlevels=2, rtol=1e-8, max_it=100, inner_rtol=1e-300, inner_its=3)
+    S.setup(c, eta)
+    S.set_rhs_body_force(rho)
+    _, _, st = S.solve()
+    assert st["converged"]
+    assert st["inner_iterations"] == 3 * st["iterations"]  # one preconditioner application per outer iteration

@@ -145,3 +145,36 @@ def test_device_marker_hierarchy_levels_match_oracle(cuda, restatement):
         ref = matmult_a11(lambda w: restatement.a11_raw((mm, mm, mm), cl, etas[depth], w), x, mask)
         assert np.linalg.norm(y - ref) <= 1e-12 * np.linalg.norm(ref), depth
     S.destroy()
+
+
+def test_device_solver_takes_the_reference_application_iteration_count(cuda):
+    """The viscous-sinker application solve with the reference's own solver
+    options (tests/application/linear/sinker_galerkin_8x8x8/opts: 3 levels,
+    Galerkin coarse operators, Chebyshev(10)/Jacobi, inner velocity solve to
+    rtol 1e-2, outer FGMRES to rtol 1e-3), from the device projection of the
+    markers: the reference converges in 17 outer iterations; the device solve
+    (inner conjugate gradients in a conditional graph loop, exact 4x4 Schur
+    blocks) takes that count to within 3 and starts from the printed residual."""
+    import torch
+
+    from ptatin3d_b200 import SCHUR_ETA_QP
+    from ptatin3d_b200.markers import PROJ_Q1, update_gauss_properties
+    from ptatin3d_b200.solver import StokesSolver
+    rec = APP["sinker_galerkin_8x8x8"]
+    assert rec["a11_operator_type"] == "2,2,0" and rec["outer_iterations"] == 17
+    case = bump_case(rec["mx"], rec["my"], rec["mz"])
+    wil, xi, eta_p, rho_p = sinker_markers(case, rec["eta0"], rec["eta1"], rec["rho0"], rec["rho1"])
+    eta_q, rho_q = update_gauss_properties(case["dims"], PROJ_Q1, _device(cuda, wil, torch.int32),
+                                           _device(cuda, xi, torch.float64), _device(cuda, eta_p, torch.float64),
+                                           _device(cuda, rho_p, torch.float64))
+    S = StokesSolver(*case["dims"], case["bits"], nlevels=rec["nlevels"], cheb_its=rec["cheb_its"],
+                     rtol=rec["ksp_rtol"], max_it=100, inner_rtol=rec["inner_rtol"], inner_its=200,
+                     schur_eta=SCHUR_ETA_QP)
+    S.setup(_device(cuda, case["coords"], torch.float64), eta_q)
+    S.set_rhs_body_force(rho_q, (0.0, 1.0, 0.0))
+    _, _, st = S.solve()
+    S.destroy()
+    assert st["converged"]
+    assert abs(st["r0"] - rec["outer_history"][0]) <= 5e-6 * rec["outer_history"][0]
+    assert abs(st["iterations"] - rec["outer_iterations"]) <= 3, st["iterations"]
+    assert st["iterations"] <= st["inner_iterations"] <= 4 * st["iterations"]
