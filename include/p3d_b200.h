@@ -51,6 +51,7 @@ extern "C" {
 #define P3D_ERR_NOCONV 5  /* a solve hit its iteration limit               */
 #define P3D_ERR_BREAKDOWN 6 /* a solve produced a non-finite residual      */
 #define P3D_ERR_TIMEOUT 7 /* a bounded wait ran out                        */
+#define P3D_ERR_CANCELLED 8 /* a served request was cancelled              */
 
 /* ---------------------------------------------------------- meshes ---- */
 /* Dirichlet bits: bit (3*face + component), faces in this order.  A bit is
@@ -364,8 +365,16 @@ int p3d_server_create(int device, int64_t hbm_budget_bytes, int32_t max_active, 
 /* Non-blocking.  The request's host arrays must stay valid until its result
  * has been returned by p3d_server_poll. */
 int p3d_server_submit(p3d_server *server, const p3d_request *request);
-/* Up to max_results finished solves (waits up to timeout_ms for the first). */
+/* Up to max_results finished solves.  timeout_ms > 0: waits up to that long
+ * for the first and returns P3D_ERR_TIMEOUT (with *n = 0) when none finished
+ * in time; timeout_ms <= 0 returns at once (P3D_OK, possibly *n = 0). */
 int p3d_server_poll(p3d_server *server, p3d_result *results, int32_t max_results, int32_t timeout_ms, int32_t *n);
+/* Cancel the request with this tag.  A queued request completes at once, a
+ * running one after its current outer iteration; its result has status
+ * P3D_ERR_CANCELLED (u, p hold the last iterate of a running one) and its
+ * execution slot and memory go back to the pool.  P3D_ERR_ARG when no queued
+ * or running request has the tag (for example one that already finished). */
+int p3d_server_cancel(p3d_server *server, int64_t tag);
 int p3d_server_get_stats(p3d_server *server, p3d_server_stats *stats);
 /* Finishes every submitted solve, then frees the pool. */
 int p3d_server_destroy(p3d_server *server);
@@ -375,6 +384,11 @@ int p3d_server_destroy(p3d_server *server);
 const char *p3d_last_error(void);
 /* Number of kernels this library launched since load (all devices). */
 int64_t p3d_kernel_launch_count(void);
+/* Failure injection for tests of the error paths (host side; no GPU fault):
+ * after `after` more successful device allocations by this library, every
+ * further one fails with P3D_ERR_NOMEM, as an exhausted device would.  A
+ * negative value switches the injection off (the default). */
+int p3d_debug_fail_allocations_after(int64_t after);
 /* Library version string. */
 const char *p3d_version(void);
 

@@ -66,10 +66,24 @@ def prolongation(nc, mask_f, mask_c):
     return (sp.diags((~mask_f).astype(float)) @ P @ sp.diags((~mask_c).astype(float))).tocsr()
 
 
+def _start_vector(n):
+    """The device solver's deterministic start vector of the lambda_max
+    estimate: xorshift64 (13, 7, 17) from 0x9E3779B97F4A7C15, the top 53 bits
+    scaled to [0, 1), minus 1/2."""
+    out = np.empty(n)
+    st = 0x9E3779B97F4A7C15
+    m64 = (1 << 64) - 1
+    for i in range(n):
+        st ^= (st << 13) & m64
+        st ^= st >> 7
+        st ^= (st << 17) & m64
+        out[i] = (st >> 11) * (1.0 / 9007199254740992.0) - 0.5
+    return out
+
+
 def _lmax(A, dinv, mask, its=10):
-    """lambda_max(D^-1 A) from CG-Lanczos."""
-    rng = np.random.default_rng(0)
-    r = rng.uniform(-0.5, 0.5, dinv.size)
+    """lambda_max(D^-1 A) from CG-Lanczos, from the device solver's start vector."""
+    r = _start_vector(dinv.size)
     r[mask] = 0.0
     z = dinv * r
     p = z.copy()

@@ -45,6 +45,8 @@ def build(ref_dir: str | None = None, quiet: bool = True) -> None:
     if not os.path.isdir(os.path.join(ref_dir, "src")):
         raise FileNotFoundError(f"pTatin3d source tree not found: {ref_dir}/src")
     subprocess.run(["make", "-C", HERE, "ref", f"REF_DIR={ref_dir}"], check=True, stdout=out)
+    if os.path.exists(os.path.join(os.path.dirname(HERE), "ptatin3d_b200", "libp3d_b200.so")):
+        subprocess.run(["make", "-C", HERE, "bind", f"REF_DIR={ref_dir}"], check=True, stdout=out)
 
 
 def _p(a):

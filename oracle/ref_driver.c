@@ -141,6 +141,18 @@ PetscErrorCode DMDAGetCorners(DM dm, PetscInt *x, PetscInt *y, PetscInt *z, Pets
 {
   return DMDAGetGhostCorners(dm, x, y, z, m, n, p);
 }
+/* first owned element's first node and the owned element counts (one process) */
+PetscErrorCode DMDAGetCornersElementQ2(DM dm, PetscInt *sei, PetscInt *sej, PetscInt *sek, PetscInt *mx, PetscInt *my,
+                                       PetscInt *mz)
+{
+  if (sei) *sei = 0;
+  if (sej) *sej = 0;
+  if (sek) *sek = 0;
+  if (mx) *mx = (dm->M - 1) / 2;
+  if (my) *my = (dm->N - 1) / 2;
+  if (mz) *mz = (dm->P - 1) / 2;
+  return 0;
+}
 
 PetscErrorCode DMDAGetElements_pTatinQ2P1(DM dm, PetscInt *nel, PetscInt *npe, const PetscInt **e)
 {
@@ -427,5 +439,9 @@ int ref_solcx_exact(double eta0, double eta1, double xc, int n, double *pos, dou
   if ((rc = EvaluateV_SolCx(pos, vel, (void *)&prm))) return rc;
   return EvaluateP_SolCx(pos, pressure, (void *)&prm);
 }
+/* the velocity DM and the volume quadrature of the mesh given to ref_setup
+ * (what pTatin3d hands an A11 back end through struct _p_MatA11MF) */
+DM ref_velocity_dm(void) { return &g_dau; }
+Quadrature ref_quadrature(void) { return &g_Q; }
 int ref_set_threads(int n) { omp_set_num_threads(n); return 0; }
 int ref_max_threads(void) { return omp_get_max_threads(); }

@@ -14,7 +14,8 @@ import os
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libp3d_b200.so")
 
 P3D_OK = 0
-P3D_ERR_ARG, P3D_ERR_CUDA, P3D_ERR_STATE, P3D_ERR_NOMEM, P3D_ERR_NOCONV, P3D_ERR_BREAKDOWN, P3D_ERR_TIMEOUT = range(1, 8)
+(P3D_ERR_ARG, P3D_ERR_CUDA, P3D_ERR_STATE, P3D_ERR_NOMEM, P3D_ERR_NOCONV, P3D_ERR_BREAKDOWN, P3D_ERR_TIMEOUT,
+ P3D_ERR_CANCELLED) = range(1, 9)
 PREC_F64, PREC_F32 = 64, 32
 COARSE_GALERKIN, COARSE_REDISC = 0, 1
 SCHUR_ETA_QP, SCHUR_ETA_GEOMEAN = 0, 1
@@ -118,6 +119,8 @@ _SIGS = {
     "p3d_a11_apply_host": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_a11_apply_host_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_op_set_host_register": ([C.c_void_p, C.c_int], C.c_int),
+    "p3d_server_cancel": ([C.c_void_p, C.c_int64], C.c_int),
+    "p3d_debug_fail_allocations_after": ([C.c_int64], C.c_int),
     "p3d_mg_prolong": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_mg_restrict": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_marker_project_workspace": ([C.c_int32, C.c_int32, C.c_int32, C.c_int, C.POINTER(C.c_int64)], C.c_int),

@@ -186,10 +186,17 @@ static void free_dev(void *&p)
   p = nullptr;
 }
 
+// failure injection: allocations left before every device allocation fails (< 0: off)
+static std::atomic<long long> g_alloc_budget{-1};
+
 int dev_alloc(void **p, size_t bytes, const char *what)
 {
   *p = nullptr;
   if (bytes == 0) bytes = 16;
+  for (long long b = g_alloc_budget.load(); b >= 0;) {
+    if (b == 0) return set_error(P3D_ERR_NOMEM, "cudaMalloc(%zu) for %s: failure injected", bytes, what);
+    if (g_alloc_budget.compare_exchange_weak(b, b - 1)) break;
+  }
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -326,6 +333,11 @@ extern "C" {
 const char *p3d_last_error(void) { return g_err; }
 int64_t p3d_kernel_launch_count(void) { return (int64_t)g_launches.load(); }
 const char *p3d_version(void) { return "p3d_b200 0.1 (sm_100a)"; }
+int p3d_debug_fail_allocations_after(int64_t after)
+{
+  g_alloc_budget.store(after < 0 ? -1 : (long long)after);
+  return P3D_OK;
+}
 
 int p3d_mesh_desc_whole(int32_t mx, int32_t my, int32_t mz, uint32_t dirichlet, p3d_mesh_desc *out)
 {

@@ -60,7 +60,7 @@ static bool same_opts(const p3d_solver_opts &a, const p3d_solver_opts &b)
          a.esteig_its == b.esteig_its && a.mg_precision == b.mg_precision && a.restart == b.restart &&
          a.max_it == b.max_it && a.rtol == b.rtol && a.atol == b.atol && a.use_graph == b.use_graph &&
          a.verbose == b.verbose && a.inner_its == b.inner_its && a.coarse_op == b.coarse_op &&
-         a.schur_eta == b.schur_eta && a.coarse_eta == b.coarse_eta;
+         a.schur_eta == b.schur_eta && a.coarse_eta == b.coarse_eta && a.inner_rtol == b.inner_rtol;
 }
 
 static bool same_shape(const Slot &s, const p3d_request &r)
@@ -107,8 +107,9 @@ static int create_slot(Slot *s, int device)
   return rc;
 }
 
-// one solve in slot s; returns the status recorded in the result
-static int run_request(Slot *s, const p3d_request &r, p3d_result &res)
+// one solve in slot s; returns the status recorded in the result.  cancel:
+// set by p3d_server_cancel while the solve runs.
+static int run_request(Slot *s, const p3d_request &r, p3d_result &res, const volatile int *cancel)
 {
   const size_t nn = (size_t)(2 * r.mx + 1) * (2 * r.my + 1) * (2 * r.mz + 1), nel = (size_t)r.mx * r.my * r.mz;
   cudaStream_t io = s->io;
@@ -122,8 +123,13 @@ static int run_request(Slot *s, const p3d_request &r, p3d_result &res)
   if (!rc) rc = solver_rhs_body_force_nowait(s->solver, s->rho, r.gx, r.gy, r.gz);
   p3d_solve_stats st;
   memset(&st, 0, sizeof st);
-  int srv = rc ? rc : solver_solve_nowait(s->solver, s->u, s->p, &st);
-  if (!rc && (srv == P3D_OK || srv == P3D_ERR_NOCONV)) {
+  int srv = rc;
+  if (!rc) {
+    solver_set_cancel_flag(s->solver, cancel);
+    srv = solver_solve_nowait(s->solver, s->u, s->p, &st);
+    solver_set_cancel_flag(s->solver, nullptr);
+  }
+  if (!rc && (srv == P3D_OK || srv == P3D_ERR_NOCONV || srv == P3D_ERR_CANCELLED)) {
     rc = cuda_check(cudaMemcpyAsync(r.u, s->u, 3 * nn * 8, cudaMemcpyDeviceToHost, io), "d2h u");
     if (!rc) rc = cuda_check(cudaMemcpyAsync(r.p, s->p, 4 * nel * 8, cudaMemcpyDeviceToHost, io), "d2h p");
     if (!rc) rc = cuda_check(cudaStreamSynchronize(io), "d2h sync");
@@ -148,6 +154,7 @@ struct p3d_server {
   std::deque<p3d_result> done;
   std::vector<std::thread> workers;
   bool stopping = false;
+  std::vector<std::pair<int64_t, volatile int *>> running; // tags of the solves in progress, their cancel flags
   int active = 0;
   int64_t bytes = 0, peak = 0;
   uint64_t clock = 0;
@@ -240,13 +247,19 @@ static void worker(p3d_server *S)
     S->cv_work.notify_all(); // the next request may fit as well
     lk.unlock();
     for (Slot *e : evict) { release_slot(e); delete e; }
+    volatile int cancel_flag = 0;
+    lk.lock();
+    S->running.emplace_back(job.req.tag, &cancel_flag);
+    lk.unlock();
     int rc = fresh ? create_slot(slot, S->device) : P3D_OK;
-    if (!rc) rc = run_request(slot, job.req, res);
+    if (!rc) rc = cancel_flag ? P3D_ERR_CANCELLED : run_request(slot, job.req, res, &cancel_flag);
     const double t_end = wall_ms();
     res.status = rc;
     res.run_ms = t_end - t_admit;
     res.latency_ms = t_end - job.t_submit;
     lk.lock();
+    for (auto it = S->running.begin(); it != S->running.end(); ++it)
+      if (it->second == &cancel_flag) { S->running.erase(it); break; }
     slot->busy = false;
     slot->last_used = ++S->clock;
     if (!slot->ready) { // creation failed: give the memory back
@@ -298,9 +311,11 @@ int p3d_server_submit(p3d_server *S, const p3d_request *req)
 int p3d_server_poll(p3d_server *S, p3d_result *results, int32_t max_results, int32_t timeout_ms, int32_t *n)
 {
   if (!S || !results || !n || max_results < 1) return set_error(P3D_ERR_ARG, "server_poll: bad arguments");
+  *n = 0;
   std::unique_lock<std::mutex> lk(S->mu);
-  if (S->done.empty() && timeout_ms > 0)
-    S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [S] { return !S->done.empty(); });
+  if (S->done.empty() && timeout_ms > 0 &&
+      !S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [S] { return !S->done.empty(); }))
+    return set_error(P3D_ERR_TIMEOUT, "server_poll: no result within %d ms", (int)timeout_ms);
   int k = 0;
   while (k < max_results && !S->done.empty()) {
     results[k++] = S->done.front();
@@ -308,6 +323,32 @@ int p3d_server_poll(p3d_server *S, p3d_result *results, int32_t max_results, int
   }
   *n = k;
   return P3D_OK;
+}
+
+int p3d_server_cancel(p3d_server *S, int64_t tag)
+{
+  if (!S) return set_error(P3D_ERR_ARG, "server_cancel: null server");
+  std::lock_guard<std::mutex> g(S->mu);
+  for (auto it = S->queue.begin(); it != S->queue.end(); ++it)
+    if (it->req.tag == tag) {
+      p3d_result res;
+      memset(&res, 0, sizeof res);
+      res.tag = tag;
+      res.status = P3D_ERR_CANCELLED;
+      res.wait_ms = res.latency_ms = wall_ms() - it->t_submit;
+      S->queue.erase(it);
+      S->done.push_back(res);
+      S->st.completed++;
+      S->cv_done.notify_all();
+      S->cv_work.notify_all();
+      return P3D_OK;
+    }
+  for (auto &r : S->running)
+    if (r.first == tag) {
+      *r.second = 1;
+      return P3D_OK;
+    }
+  return set_error(P3D_ERR_ARG, "server_cancel: no queued or running request has tag %lld", (long long)tag);
 }
 
 int p3d_server_get_stats(p3d_server *S, p3d_server_stats *st)

@@ -64,6 +64,9 @@ namespace p3d {
 int solver_setup_nowait(p3d_solver *s, const double *coords, const double *eta);
 int solver_rhs_body_force_nowait(p3d_solver *s, const double *rho, double gx, double gy, double gz);
 int solver_solve_nowait(p3d_solver *s, double *u, double *p, struct p3d_solve_stats *stats);
+// a flag the outer iteration reads between iterations: non-zero ends the
+// solve with P3D_ERR_CANCELLED (u, p the iterate reached); nullptr: none
+void solver_set_cancel_flag(p3d_solver *s, const volatile int *flag);
 
 // dense_inverse.cu (coarse-grid operator, in place, blocked Gauss-Jordan)
 size_t dense_inverse_scratch(int n);

@@ -68,6 +68,7 @@ struct p3d_solver {
   void **cg_ptr = nullptr; // device pointers {p, r} for the dot kernels
   double *cg_sc = nullptr; // fixed count: {rz (2 slots, alternating), pq}; tolerance: see CG_* below
   cudaStream_t st_body = nullptr; // side stream on which the inner loop's body is captured
+  const volatile int *cancel = nullptr; // set by another thread: stop after the current outer iteration
   // preconditioner buffers (fixed for graph capture)
   double *pc_in = nullptr, *pc_out = nullptr, *pc_t = nullptr;
   double *xsol = nullptr; // [u; p] iterate of a solve
@@ -379,7 +380,8 @@ static int norm2(p3d_solver *s, const double *v, size_t n, double *out)
   v_mdot<double>(n, 1, (const double *const *)(s->Vptr + slot), v, s->part, s->hdev + h, s->st);
   CU(cudaMemcpyAsync(s->hhost + h, s->hdev + h, 8, cudaMemcpyDeviceToHost, s->st), "d2h");
   CU(cudaStreamSynchronize(s->st), "sync");
-  *out = std::sqrt(std::max(0.0, s->hhost[h]));
+  const double ss = s->hhost[h];
+  *out = ss > 0.0 ? std::sqrt(ss) : (ss <= 0.0 ? 0.0 : ss); // a NaN stays NaN (std::max(0, NaN) would give 0)
   return P3D_OK;
 }
 
@@ -699,8 +701,8 @@ static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
   std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
   double r0 = -1.0, rnorm = 0.0;
   int its = 0;
-  bool conv = false;
-  while (its < s->o.max_it) {
+  bool conv = false, cancelled = false;
+  while (its < s->o.max_it && !cancelled) {
     // r = b - A x  into V_0
     CK(stokes_op(s, x, w));
     v_residual<double>(N, s->bvec, w, V, s->st);
@@ -768,6 +770,7 @@ static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
       if (s->o.verbose) fprintf(stderr, "  fgmres %3d  |r| %.6e\n", its + 1, rnorm);
       if (!std::isfinite(rnorm)) return set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual estimate");
       if (rnorm <= tol || hn == 0.0) { j++; its++; conv = rnorm <= tol; break; }
+      if (s->cancel && *s->cancel) { j++; its++; cancelled = true; break; }
     }
     // y = H^{-1} g ; x += Z y
     for (int i = j - 1; i >= 0; i--) {
@@ -787,8 +790,10 @@ static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
   stats->r0 = r0;
   stats->rfinal = rt;
   stats->converged = conv || rt <= std::max(s->o.rtol * r0, s->o.atol) * 1.0000001;
-  return P3D_OK;
+  return cancelled && !stats->converged ? P3D_ERR_CANCELLED : P3D_OK;
 }
+
+void solver_set_cancel_flag(p3d_solver *s, const volatile int *flag) { s->cancel = flag; }
 
 } // namespace p3d
 
@@ -1026,7 +1031,11 @@ int solver_solve_nowait(p3d_solver *s, double *u, double *p, p3d_solve_stats *st
   int rc = cuda_check(cudaMemcpyAsync(x, u, s->nu * 8, cudaMemcpyDeviceToDevice, s->st), "x u");
   if (!rc) rc = cuda_check(cudaMemcpyAsync(x + s->nu, p, s->np * 8, cudaMemcpyDeviceToDevice, s->st), "x p");
   if (!rc && s->cg_sc) rc = cuda_check(cudaMemsetAsync(s->cg_sc + CG_TOTAL, 0, 8, s->st), "inner count");
-  if (!rc) rc = fgmres(s, x, &local);
+  bool cancelled = false;
+  if (!rc) {
+    rc = fgmres(s, x, &local);
+    if (rc == P3D_ERR_CANCELLED) { cancelled = true; rc = P3D_OK; }
+  }
   if (!rc && s->cg_sc && s->o.inner_rtol > 0.0) {
     double tot = 0.0;
     rc = cuda_check(cudaMemcpyAsync(&tot, s->cg_sc + CG_TOTAL, 8, cudaMemcpyDeviceToHost, s->st), "inner count");
@@ -1042,6 +1051,7 @@ int solver_solve_nowait(p3d_solver *s, double *u, double *p, p3d_solve_stats *st
   local.coarse_dofs = s->nc;
   if (stats) *stats = local;
   if (rc) return rc;
+  if (cancelled) return set_error(P3D_ERR_CANCELLED, "solve cancelled after %d iterations", local.iterations);
   if (!local.converged) return set_error(P3D_ERR_NOCONV, "FGMRES: %d iterations, |r| %.3e / %.3e", local.iterations,
                                          local.rfinal, local.r0);
   return P3D_OK;

@@ -14,7 +14,7 @@ import itertools
 
 import numpy as np
 
-from ._lib import P3D_OK, Request, Result, ServerStats, check, lib
+from ._lib import P3D_ERR_TIMEOUT, P3D_OK, Request, Result, ServerStats, check, lib
 from .solver import default_opts
 
 
@@ -48,7 +48,10 @@ class StokesServer:
     def poll(self, timeout_ms: int = 0, max_results: int = 64):
         buf = (Result * max_results)()
         n = C.c_int32()
-        check(lib().p3d_server_poll(self.h, buf, max_results, int(timeout_ms), C.byref(n)))
+        rc = lib().p3d_server_poll(self.h, buf, max_results, int(timeout_ms), C.byref(n))
+        if rc == P3D_ERR_TIMEOUT:  # nothing finished within timeout_ms
+            return []
+        check(rc)
         out = []
         for r in buf[:n.value]:
             arrs = self._live.pop(r.tag)
@@ -56,6 +59,11 @@ class StokesServer:
                             rel_residual=r.rel_residual, wait_ms=r.wait_ms, run_ms=r.run_ms,
                             latency_ms=r.latency_ms, u=arrs["u"], p=arrs["p"]))
         return out
+
+    def cancel(self, tag: int) -> None:
+        """Cancel a queued or running request; its result (status
+        P3D_ERR_CANCELLED) still comes back through poll."""
+        check(lib().p3d_server_cancel(self.h, int(tag)))
 
     def wait_all(self, timeout_ms: int = 100):
         res = []

@@ -116,8 +116,9 @@ def test_restatement_takes_the_reference_application_iteration_count(reference_k
 def test_cpu_and_gpu_inner_solves_agree(cuda, reference_kernels, prec):
     """With the velocity block solved to a relative tolerance by inner
     conjugate gradients, the device solve (FP64, or FP32 multigrid) and the
-    host restatement take outer and total inner iteration counts within 15 %
-    of each other and reach the same solution."""
+    host restatement (both estimate lambda_max from the same start vector)
+    take outer and total inner iteration counts within 15 % of each other
+    and reach the same solution."""
     from oracle.cpu_solver import CpuStokesSolver
     from ptatin3d_b200 import SCHUR_ETA_GEOMEAN
     from ptatin3d_b200.solver import StokesSolver
@@ -131,6 +132,7 @@ def test_cpu_and_gpu_inner_solves_agree(cuda, reference_kernels, prec):
     G.set_rhs_body_force(rho)
     ug, pg, st = G.solve()
     assert rtc <= 1e-9 and st["converged"]
+    assert abs(st["lmax_fine"] / C.lv[-1].lmax - 1.0) <= 1e-8  # the same Lanczos start vector
     assert abs(st["iterations"] - itc) <= 0.15 * itc + 2
     assert abs(st["inner_iterations"] - C.inner_total) <= 0.15 * C.inner_total + 3
     assert st["inner_iterations"] > st["iterations"]

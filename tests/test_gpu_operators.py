@@ -444,16 +444,20 @@ def test_c3_layered_apply_matches_reference_kernel(cuda, reference_kernels):
     assert rel(host(y32), y64) <= TOL32
 
 
-@pytest.mark.parametrize("dims", [(13, 7, 5), (1, 1, 1), (9, 5, 3), (8, 4, 2)])
-def test_fp32_general_ragged(cuda, dims):
-    """The FP32 general A11 kernel on ragged meshes (bricks cut by the mesh
-    edges), in the MatMult and the raw (y +=) forms, against the FP64 operator."""
+@pytest.mark.parametrize("dims", [(13, 7, 5), (1, 1, 1), (9, 5, 3), (8, 4, 2), (6, 4, 17), (11, 3, 8)])
+@pytest.mark.parametrize("geom", [GEOM_GENERAL, GEOM_AFFINE])
+def test_fp32_ragged(cuda, dims, geom):
+    """The FP32 A11 kernels on ragged meshes (bricks cut by the mesh edges),
+    affine and general geometry, in the MatMult and the raw (y +=) forms,
+    against the FP64 operator."""
     mx, my, mz = dims
-    c = M.perturb_interior(M.uniform_coords(mx, my, mz), mx, my, mz, frac=0.15, seed=sum(dims))
+    c = M.uniform_coords(mx, my, mz, hi=(1.0, 2.0, 0.5))
+    if geom == GEOM_GENERAL:
+        c = M.perturb_interior(c, mx, my, mz, frac=0.15, seed=sum(dims))
     eta = 10 ** np.random.default_rng(1).uniform(-1, 1, size=(mx * my * mz, 27))
     case = dict(dims=dims, coords=c, eta=eta, bits=M.FREE_SLIP)
     op64, op32 = make_op(case), make_op(case, prec=PREC_F32)
-    assert op32.geometry_mode == GEOM_GENERAL
+    assert op32.geometry_mode == geom and op64.geometry_mode == geom
     x = np.random.default_rng(2).uniform(-1, 1, size=c.size)
     y64 = torch.empty(x.size, dtype=torch.float64, device="cuda")
     y32 = torch.empty(x.size, dtype=torch.float32, device="cuda")
