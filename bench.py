@@ -298,16 +298,18 @@ SOLVE_C4_WORKLOAD = ("Stokes solve, Q2-P1disc 96^3 deformed mesh (interior nodes
 
 
 SOLVE_C3_WORKLOAD = ("Stokes solve, Q2-P1disc {m}^3 unit cube, layered eta (6 layers, log10 eta in [-3,3], 16 "
-                     "inclusions), 8 sinkers of density +1%, g=-z, free slip walls/base, free surface top; FGMRES(30) "
-                     "+ Schur upper (geometric mean) + 5-level Galerkin GMG, Chebyshev(3)/Jacobi, rtol 1e-6, at most "
-                     "{max_it} iterations")
+                     "inclusions), 8 sinkers of density +1%, g=-z, free slip walls/base, free surface top; "
+                     "FGMRES({restart}) + Schur upper (geometric mean) + 5-level Galerkin GMG, Chebyshev(3)/Jacobi, "
+                     "rtol 1e-6, at most {max_it} iterations")
 
 
-def solve_c3_leg(device, m=64, seed=4, max_it=600):
+def solve_c3_leg(device, m=64, seed=4, max_it=3000, restart=120):
     """FP64 and mixed-precision solves of the layered 64^3 field (eta over six
     decades), each bounded to max_it outer iterations: this preconditioner
-    family stagnates on it (the CPU restatement too), so the leg records the
-    residual reached and the time per iteration of both precisions."""
+    family converges slowly on it (the CPU restatement too; FGMRES(120)
+    reaches about 1e-3 in 3,000 iterations where FGMRES(30) stalls near 0.9),
+    so the leg records the residual reached and the time per iteration of
+    both precisions."""
     import torch
 
     from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
@@ -322,7 +324,7 @@ def solve_c3_leg(device, m=64, seed=4, max_it=600):
     out, sols = {}, {}
     for name, prec in (("fp64", PREC_F64), ("mixed", PREC_F32)):
         S = StokesSolver(m, m, m, bits, device=device, nlevels=5, rtol=1e-6, max_it=max_it, mg_precision=prec,
-                         schur_eta=SCHUR_ETA_GEOMEAN)
+                         schur_eta=SCHUR_ETA_GEOMEAN, restart=restart)
         S.setup(c, eta)
         S.set_rhs_body_force(rho)
         torch.cuda.synchronize()
@@ -338,7 +340,7 @@ def solve_c3_leg(device, m=64, seed=4, max_it=600):
         del S, u, p
         torch.cuda.empty_cache()
     (u64, p64), (u32, p32) = sols["fp64"], sols["mixed"]
-    return {"workload": SOLVE_C3_WORKLOAD.format(m=m, max_it=max_it), "unit": "s", "fp64": out["fp64"],
+    return {"workload": SOLVE_C3_WORKLOAD.format(m=m, max_it=max_it, restart=restart), "unit": "s", "fp64": out["fp64"],
             "mixed": out["mixed"],
             "ms_per_iteration_ratio_fp64_vs_mixed": out["fp64"]["ms_per_iteration"] / out["mixed"]["ms_per_iteration"],
             "u_diff_mixed_vs_fp64": float(np.linalg.norm(u32 - u64) / np.linalg.norm(u64)),

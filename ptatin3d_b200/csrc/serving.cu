@@ -109,7 +109,7 @@ static int create_slot(Slot *s, int device)
 
 // one solve in slot s; returns the status recorded in the result.  cancel:
 // set by p3d_server_cancel while the solve runs.
-static int run_request(Slot *s, const p3d_request &r, p3d_result &res, const volatile int *cancel)
+static int run_request(Slot *s, const p3d_request &r, p3d_result &res, const std::atomic<int> *cancel)
 {
   const size_t nn = (size_t)(2 * r.mx + 1) * (2 * r.my + 1) * (2 * r.mz + 1), nel = (size_t)r.mx * r.my * r.mz;
   cudaStream_t io = s->io;
@@ -154,7 +154,7 @@ struct p3d_server {
   std::deque<p3d_result> done;
   std::vector<std::thread> workers;
   bool stopping = false;
-  std::vector<std::pair<int64_t, volatile int *>> running; // tags of the solves in progress, their cancel flags
+  std::vector<std::pair<int64_t, std::atomic<int> *>> running; // tags of the solves in progress, their cancel flags
   int active = 0;
   int64_t bytes = 0, peak = 0;
   uint64_t clock = 0;
@@ -247,12 +247,12 @@ static void worker(p3d_server *S)
     S->cv_work.notify_all(); // the next request may fit as well
     lk.unlock();
     for (Slot *e : evict) { release_slot(e); delete e; }
-    volatile int cancel_flag = 0;
+    std::atomic<int> cancel_flag{0};
     lk.lock();
     S->running.emplace_back(job.req.tag, &cancel_flag);
     lk.unlock();
     int rc = fresh ? create_slot(slot, S->device) : P3D_OK;
-    if (!rc) rc = cancel_flag ? P3D_ERR_CANCELLED : run_request(slot, job.req, res, &cancel_flag);
+    if (!rc) rc = cancel_flag.load() ? P3D_ERR_CANCELLED : run_request(slot, job.req, res, &cancel_flag);
     const double t_end = wall_ms();
     res.status = rc;
     res.run_ms = t_end - t_admit;
@@ -345,7 +345,7 @@ int p3d_server_cancel(p3d_server *S, int64_t tag)
     }
   for (auto &r : S->running)
     if (r.first == tag) {
-      *r.second = 1;
+      r.second->store(1);
       return P3D_OK;
     }
   return set_error(P3D_ERR_ARG, "server_cancel: no queued or running request has tag %lld", (long long)tag);

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
+
+#include <atomic>
 #include <stdint.h>
 
 #define P3D_MDOT_CHUNK 8    // vectors per multi-dot / multi-axpy launch (register accumulators)
@@ -66,7 +68,7 @@ int solver_rhs_body_force_nowait(p3d_solver *s, const double *rho, double gx, do
 int solver_solve_nowait(p3d_solver *s, double *u, double *p, struct p3d_solve_stats *stats);
 // a flag the outer iteration reads between iterations: non-zero ends the
 // solve with P3D_ERR_CANCELLED (u, p the iterate reached); nullptr: none
-void solver_set_cancel_flag(p3d_solver *s, const volatile int *flag);
+void solver_set_cancel_flag(p3d_solver *s, const std::atomic<int> *flag);
 
 // dense_inverse.cu (coarse-grid operator, in place, blocked Gauss-Jordan)
 size_t dense_inverse_scratch(int n);

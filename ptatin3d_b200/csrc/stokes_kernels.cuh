@@ -36,9 +36,16 @@ __device__ __forceinline__ LaneMap lane_map()
 }
 
 
-// correctly rounded reciprocal (CUDA's intrinsics)
+// reciprocal of a Jacobian determinant: FP64 correctly rounded (CUDA's
+// intrinsic); FP32 the hardware approximation rcp.approx (within an ulp, one
+// instruction and no slow-path branch; the FP32 operators feed the smoother)
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
-__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float rcp_rn(float x)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // 3x3 inverse: M[3d+l] = dx_l/dxi_d  ->  Mi[3k+d] = dxi_d/dx_k, returns det
 template <typename T> __device__ __forceinline__ T inv3(const T M[9], T Mi[9])
@@ -53,7 +60,7 @@ template <typename T> __device__ __forceinline__ T inv3(const T M[9], T Mi[9])
   T c21 = -(M[0] * M[5] - M[2] * M[3]);
   T c22 = M[0] * M[4] - M[1] * M[3];
   T det = M[0] * c00 + M[1] * c01 + M[2] * c02;
-  T r = rcp_rn(det); // = 1 / det, correctly rounded
+  T r = rcp_rn(det); // = 1 / det
   // Mi[k][d] = cof[d][k] / det
   Mi[0] = c00 * r; Mi[1] = c10 * r; Mi[2] = c20 * r;
   Mi[3] = c01 * r; Mi[4] = c11 * r; Mi[5] = c21 * r;
@@ -540,12 +547,12 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
           T d1 = dcol(j, xp[i + 9 * k], xp[i + 3 + 9 * k], xp[i + 6 + 9 * k]);
           T d2 = dcol(k, xp[i + 3 * j], xp[i + 3 * j + 9], xp[i + 3 * j + 18]);
           if (!valid) { d0 = (T)(L.f == 0); d1 = (T)(L.f == 1); d2 = (T)(L.f == 2); }
-          if (L.active) {
-            g[q9 * GQ + 0 + L.f] = d0;
-            g[q9 * GQ + 3 + L.f] = d1;
-            g[q9 * GQ + 6 + L.f] = d2;
-            if (PB) g[q9 * GQ + 11 + L.f] = (xp[q9 + 9 * k] - avg) * rL;
-          }
+          // lanes 30 and 31 repeat lanes 27 and 28 (slot 9): their stores write
+          // the same values to the same places, so no lane guard is needed
+          g[q9 * GQ + 0 + L.f] = d0;
+          g[q9 * GQ + 3 + L.f] = d1;
+          g[q9 * GQ + 6 + L.f] = d2;
+          if (PB) g[q9 * GQ + 11 + L.f] = (xp[q9 + 9 * k] - avg) * rL;
         }
     }
     __syncwarp();
@@ -559,12 +566,10 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
       T det = inv3(M, Mi);
       T w = (T)(w1d(L.f) * w1d(t) * w1d(k)) * det;
       T eta = valid ? eta_e[q9 + 9 * k] : (T)0;
-      if (L.active) {
 #pragma unroll
-        for (int rr = 0; rr < 9; rr++) G[rr] = Mi[rr];
-        G[9] = eta * w;
-        if (GQ > 10) G[10] = valid ? w : (T)0;
-      }
+      for (int rr = 0; rr < 9; rr++) G[rr] = Mi[rr];
+      G[9] = eta * w;
+      if (GQ > 10) G[10] = valid ? w : (T)0;
     }
     __syncwarp();
     // ---- the plane's 9 Gauss points

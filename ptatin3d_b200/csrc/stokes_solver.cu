@@ -68,7 +68,7 @@ struct p3d_solver {
   void **cg_ptr = nullptr; // device pointers {p, r} for the dot kernels
   double *cg_sc = nullptr; // fixed count: {rz (2 slots, alternating), pq}; tolerance: see CG_* below
   cudaStream_t st_body = nullptr; // side stream on which the inner loop's body is captured
-  const volatile int *cancel = nullptr; // set by another thread: stop after the current outer iteration
+  const std::atomic<int> *cancel = nullptr; // set by another thread: stop after the current outer iteration
   // preconditioner buffers (fixed for graph capture)
   double *pc_in = nullptr, *pc_out = nullptr, *pc_t = nullptr;
   double *xsol = nullptr; // [u; p] iterate of a solve
@@ -770,7 +770,7 @@ static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
       if (s->o.verbose) fprintf(stderr, "  fgmres %3d  |r| %.6e\n", its + 1, rnorm);
       if (!std::isfinite(rnorm)) return set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual estimate");
       if (rnorm <= tol || hn == 0.0) { j++; its++; conv = rnorm <= tol; break; }
-      if (s->cancel && *s->cancel) { j++; its++; cancelled = true; break; }
+      if (s->cancel && s->cancel->load(std::memory_order_relaxed)) { j++; its++; cancelled = true; break; }
     }
     // y = H^{-1} g ; x += Z y
     for (int i = j - 1; i >= 0; i--) {
@@ -793,7 +793,7 @@ static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
   return cancelled && !stats->converged ? P3D_ERR_CANCELLED : P3D_OK;
 }
 
-void solver_set_cancel_flag(p3d_solver *s, const volatile int *flag) { s->cancel = flag; }
+void solver_set_cancel_flag(p3d_solver *s, const std::atomic<int> *flag) { s->cancel = flag; }
 
 } // namespace p3d
 
