@@ -862,25 +862,34 @@ def run_slabs(args, rank, world, local):
 
 
 def profile_solve(spec):
-    """One short C2-construction solve for profiling its kernel mix:
-    spec = "m,iterations,precision" (precision 64 or 32).  Unit cube, 8
-    sinkers of radius 0.1, viscosity contrast 1e4, density +1 %, free slip
-    walls and base, free surface top, 4 Galerkin levels, Chebyshev(3)/Jacobi,
-    geometric-mean Schur weighting; stops after `iterations` FGMRES
-    iterations.  Prints one line, no JSON (not a benchmark number)."""
+    """One short solve for profiling its kernel mix: spec =
+    "m,iterations,precision[,deformed]" (precision 64 or 32).  Default: the C2
+    construction (unit cube, 8 sinkers of radius 0.1, viscosity contrast 1e4,
+    density +1 %, free slip walls and base, free surface top, 4 Galerkin
+    levels); "deformed": the deformed-mesh solve of the apply benchmark
+    (interior nodes +-0.2h, log-normal eta of sigma 1 decade, 5 levels).
+    Chebyshev(3)/Jacobi, geometric-mean Schur weighting; stops after
+    `iterations` FGMRES iterations.  Prints one line, no JSON (not a
+    benchmark number)."""
     import torch
 
     from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
     from ptatin3d_b200 import mesh as M
     from ptatin3d_b200.solver import StokesSolver, max_levels
-    m, its, prec = (int(v) for v in spec.split(","))
+    parts = spec.split(",")
+    m, its, prec = (int(v) for v in parts[:3])
+    deformed = len(parts) > 3 and parts[3] == "deformed"
     bits = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
     c = M.uniform_coords(m, m, m)
+    if deformed:
+        c = M.perturb_interior(c, m, m, m, frac=0.2, seed=4)
     qp = M.qp_coords(c, m, m, m)
     cen, r = M.random_sinkers(8, 1, 0.1)
-    S = StokesSolver(m, m, m, bits, nlevels=min(4, max_levels(m)), rtol=1e-12, max_it=its,
+    eta = (M.lognormal_grf_eta(m, m, m, seed=4, sigma_decades=1.0, corr_len=0.1) if deformed
+           else M.sinker_eta(qp, cen, r, 1.0, 1e4))
+    S = StokesSolver(m, m, m, bits, nlevels=min(5 if deformed else 4, max_levels(m)), rtol=1e-12, max_it=its,
                      mg_precision=PREC_F32 if prec == 32 else PREC_F64, schur_eta=SCHUR_ETA_GEOMEAN)
-    S.setup(c, M.sinker_eta(qp, cen, r, 1.0, 1e4))
+    S.setup(c, eta)
     S.set_rhs_body_force(M.sinker_density(qp, cen, r, 1.0, 1.01))
     u, p, st = S.solve(raise_on_noconv=False)
     torch.cuda.synchronize()

@@ -175,6 +175,16 @@ int p3d_a11_apply_host_noalloc(p3d_op *op, const double *x_host, double *y_host)
 int p3d_mg_prolong(int prec, int cnx, int cny, int cnz, int ndof, const void *xc, void *xf, void *stream);
 int p3d_mg_restrict(int prec, int cnx, int cny, int cnz, int ndof, const void *xf, void *xc, void *stream);
 
+/* ------------------------------------------------ z-slab exchange ---- */
+/* One node plane of a z-slab partitioned velocity vector (3 components per
+ * node of the (2mx+1) x (2my+1) plane): y_plane += recv, then the plane's
+ * Dirichlet rows (x/y face bits of `dirichlet`) reset to x_plane.  The
+ * receiving half of DMLocalToGlobal(ADD) on a shared slab plane followed by
+ * the MatMult row convention (src/stokes_operators.c:1192-1201).  Device
+ * arrays of `prec`; asynchronous on `stream`. */
+int p3d_slab_add_plane(int prec, int32_t mx, int32_t my, uint32_t dirichlet, const void *recv, const void *x_plane,
+                       void *y_plane, void *stream);
+
 /* ------------------------------- material points -> Gauss points ---- */
 /* Viscosity and density of material points (markers) onto the 27 Gauss
  * points of every element of one whole mx*my*mz mesh, by the projection types

@@ -172,9 +172,48 @@ template int mg_restrict<float>(int, int, int, int, const float *, float *, cuda
 
 } // namespace p3d
 
+namespace p3d {
+
+// y += recv on one node plane (3 components per node), then the plane's
+// Dirichlet rows reset to x: the second half of DMLocalToGlobal(ADD) on a
+// z-slab boundary plane followed by the MatMult row convention
+template <typename T>
+__global__ void slab_plane_kernel(int nx, int ny, uint32_t dir, const T *__restrict__ recv, const T *__restrict__ x,
+                                  T *__restrict__ y)
+{
+  const int n = 3 * nx * ny;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int c = i % 3, node = i / 3, ix = node % nx, iy = node / nx;
+    bool d = (ix == 0 && (dir >> (0 + c) & 1u)) || (ix == nx - 1 && (dir >> (3 + c) & 1u)) ||
+             (iy == 0 && (dir >> (6 + c) & 1u)) || (iy == ny - 1 && (dir >> (9 + c) & 1u));
+    y[i] = d ? x[i] : y[i] + recv[i];
+  }
+}
+
+} // namespace p3d
+
 using namespace p3d;
 
 extern "C" {
+int p3d_slab_add_plane(int prec, int32_t mx, int32_t my, uint32_t dirichlet, const void *recv, const void *x_plane,
+                       void *y_plane, void *stream)
+{
+  if (mx < 1 || my < 1 || !recv || !x_plane || !y_plane) return set_error(P3D_ERR_ARG, "slab_add_plane: bad args");
+  const int nx = 2 * mx + 1, ny = 2 * my + 1, n = 3 * nx * ny;
+  const int grid = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (prec == P3D_PREC_F64)
+    slab_plane_kernel<double><<<grid, 256, 0, st>>>(nx, ny, dirichlet, (const double *)recv, (const double *)x_plane,
+                                                   (double *)y_plane);
+  else if (prec == P3D_PREC_F32)
+    slab_plane_kernel<float><<<grid, 256, 0, st>>>(nx, ny, dirichlet, (const float *)recv, (const float *)x_plane,
+                                                  (float *)y_plane);
+  else
+    return set_error(P3D_ERR_ARG, "slab_add_plane: precision must be 64 or 32");
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "slab_add_plane");
+}
+
 int p3d_mg_prolong(int prec, int cnx, int cny, int cnz, int ndof, const void *xc, void *xf, void *stream)
 {
   if (cnx < 1 || cny < 1 || cnz < 1 || ndof < 1 || !xc || !xf) return set_error(P3D_ERR_ARG, "mg_prolong: bad args");

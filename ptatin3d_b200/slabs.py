@@ -19,6 +19,8 @@ exchange runs with the sm_100a operator on GPUs and with any CPU operator.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import torch
 import torch.distributed as dist
@@ -68,6 +70,7 @@ class SlabExchange:
         self.plane = 3 * (2 * mx + 1) * (2 * my + 1)
         self.nz_local = 2 * (self.z1 - self.z0) + 1
         self.n_local = self.plane * self.nz_local
+        self.bits = bits
         m = plane_dirichlet(mx, my, bits).astype(bool)
         dev = device if device is not None else torch.device("cpu")
         self.plane_mask = torch.tensor(m, device=dev)
@@ -90,10 +93,17 @@ class SlabExchange:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
         for off, buf in recv:
-            seg = y[off:off + P]
-            seg += buf
-            xs = x[off:off + P]
-            seg[self.plane_mask] = xs[self.plane_mask]
+            if y.is_cuda:  # one library kernel: add the partials, reset the Dirichlet rows
+                from ._lib import PREC_F32, PREC_F64, check, lib
+                prec = PREC_F64 if y.dtype == torch.float64 else PREC_F32
+                check(lib().p3d_slab_add_plane(prec, self.mx, self.my, self.bits, C.c_void_p(buf.data_ptr()),
+                                               C.c_void_p(x[off:].data_ptr()), C.c_void_p(y[off:].data_ptr()),
+                                               C.c_void_p(torch.cuda.current_stream(y.device).cuda_stream)))
+            else:  # host ranks (gloo): the same arithmetic on CPU tensors
+                seg = y[off:off + P]
+                seg += buf
+                xs = x[off:off + P]
+                seg[self.plane_mask] = xs[self.plane_mask]
 
 
 class SlabA11:

@@ -128,3 +128,30 @@ def test_slab_coords_agree_on_shared_planes():
     h = (1 / (2 * mx), 1 / (2 * my), 1 / (2 * mzg))
     for l in range(3):
         assert 0 < d[..., l].max() <= 0.2 * h[l] + 1e-15
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_slab_plane_kernel_matches_host_arithmetic(cuda, dtype):
+    """The library's receiving step of the shared-plane exchange
+    (p3d_slab_add_plane: y += partials, Dirichlet rows reset to x) equals the
+    host arithmetic the gloo ranks run."""
+    import ctypes as C
+
+    from ptatin3d_b200 import _lib
+    from ptatin3d_b200.slabs import plane_dirichlet
+    mx, my = 5, 3
+    bits = M.FREE_SLIP
+    P = 3 * (2 * mx + 1) * (2 * my + 1)
+    g = torch.Generator().manual_seed(3)
+    x, y, r = (torch.rand(P, generator=g, dtype=torch.float64) for _ in range(3))
+    mask = torch.tensor(plane_dirichlet(mx, my, bits).astype(bool))
+    ref = y + r
+    ref[mask] = x[mask]
+    xd, yd, rd = (t.to(device=cuda, dtype=dtype) for t in (x, y, r))
+    prec = _lib.PREC_F64 if dtype == torch.float64 else _lib.PREC_F32
+    _lib.check(_lib.lib().p3d_slab_add_plane(prec, mx, my, bits, C.c_void_p(rd.data_ptr()), C.c_void_p(xd.data_ptr()),
+                                             C.c_void_p(yd.data_ptr()), C.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    tol = 0.0 if dtype == torch.float64 else 1e-6
+    assert float((yd.double().cpu() - ref).abs().max()) <= tol
