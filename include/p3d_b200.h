@@ -114,6 +114,13 @@ int p3d_a11_apply(p3d_op *op, const void *x, void *y, void *stream);
  * which zeroes Yu and then adds): y is overwritten and never read, which
  * saves the read of y that the "+=" form needs. */
 int p3d_a11_mult(p3d_op *op, const void *x, void *y, void *stream);
+/* The MatMult of k operators at once (no counterpart in the reference,
+ * which applies one operator per process): y[i] = A11_i x[i] for k <= 32
+ * operators of the same mesh shape, precision, geometry path and boundary
+ * mode (the solves of a served batch), in one zeroing launch and one
+ * element-kernel launch whose grid covers the bricks of every member. */
+#define P3D_GROUP_MAX 32
+int p3d_a11_mult_grouped(p3d_op *const ops[], const void *const x[], void *const y[], int32_t k, void *stream);
 int p3d_a11_diagonal(p3d_op *op, void *d, void *stream);           /* d += diag(A11); Dirichlet slots = 1 with MATMULT */
 int p3d_a12_apply(p3d_op *op, const void *p, void *yu, void *stream);  /* yu += A12 p; Dirichlet rows 0 with MATMULT */
 int p3d_a21_apply(p3d_op *op, const void *u, void *yp, void *stream);  /* yp += A21 u; Dirichlet columns zeroed with MATMULT */

@@ -120,6 +120,8 @@ _SIGS = {
     "p3d_a11_apply_host_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_op_set_host_register": ([C.c_void_p, C.c_int], C.c_int),
     "p3d_server_cancel": ([C.c_void_p, C.c_int64], C.c_int),
+    "p3d_a11_mult_grouped": ([C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32,
+                              C.c_void_p], C.c_int),
     "p3d_slab_add_plane": ([C.c_int, C.c_int32, C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                             C.c_void_p], C.c_int),
     "p3d_debug_fail_allocations_after": ([C.c_int64], C.c_int),

@@ -55,6 +55,13 @@ int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_
                    int tzb = 0, int tze = -1);
 // brick layer height along z of the A11 path the operator uses
 int a11_brick_height(const p3d_op *op);
+// K operators of one mesh shape, precision, path and mode in one launch
+// (u, p, yu, yp: per-member pointers or nullptr); y overwritten when overwrite
+template <typename T, bool DA11, bool DA12, bool DA21>
+int launch_group(p3d_op *const *ops, int K, const T *const *u, const T *const *p, T *const *yu, T *const *yp,
+                 cudaStream_t st, bool overwrite);
+// zero K buffers of `bytes` bytes (a multiple of 4) in one launch
+int zero_group(void *const *v, int K, size_t bytes, cudaStream_t st);
 // coefficient setup from device FP64 arrays on op->stream (no ordering against
 // other streams: the caller orders the arrays' producers first)
 int op_setup_device(p3d_op *op, const double *coords, const double *eta, int geom_mode);

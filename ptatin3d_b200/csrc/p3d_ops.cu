@@ -154,6 +154,99 @@ int launch_general(p3d_op *op, const T *u, const T *p, T *yu, T *yp, cudaStream_
   return cuda_check(cudaGetLastError(), "stokes launch");
 }
 
+// ----------------------------------------------------- grouped launches ---
+// The operators of K resident problems of one mesh shape (and precision,
+// geometry path and boundary mode) in ONE launch: grid (bricks, K), the
+// member's tile arguments passed in the launch parameters (TileGroup).
+static bool same_shape_ops(p3d_op *const *ops, int K)
+{
+  const p3d_mesh_desc &m = ops[0]->m;
+  for (int k = 1; k < K; k++) {
+    const p3d_op *o = ops[k];
+    if (!o || !o->have_coef || o->prec != ops[0]->prec || o->geom != ops[0]->geom || o->bc != ops[0]->bc ||
+        o->aff_exact != ops[0]->aff_exact || o->device != ops[0]->device || o->m.mx != m.mx || o->m.my != m.my ||
+        o->m.mz != m.mz || o->m.gx != m.gx || o->m.gy != m.gy || o->m.gz != m.gz || o->m.ox != m.ox ||
+        o->m.oy != m.oy || o->m.oz != m.oz || o->m.dirichlet != m.dirichlet || o->m.global_faces != m.global_faces)
+      return false;
+  }
+  return true;
+}
+
+template <typename T, bool DA11, bool DA12, bool DA21>
+int launch_group(p3d_op *const *ops, int K, const T *const *u, const T *const *p, T *const *yu, T *const *yp,
+                 cudaStream_t st, bool overwrite)
+{
+  if (K < 1 || K > P3D_GROUP_MAX) return set_error(P3D_ERR_ARG, "grouped launch: %d members (1..%d)", K, P3D_GROUP_MAX);
+  if (!ops[0] || !ops[0]->have_coef) return set_error(P3D_ERR_STATE, "grouped launch: operator not set up");
+  if (!same_shape_ops(ops, K)) return set_error(P3D_ERR_ARG, "grouped launch: members differ in shape, path or mode");
+  p3d_op *op0 = ops[0];
+  const bool affine = op0->geom == P3D_GEOM_AFFINE && (op0->aff_exact || !(DA12 || DA21));
+  const int nw = affine ? NW_AFF : NW_GEN;
+  TileGroup<T> G;
+  memset(&G, 0, sizeof G);
+  for (int k = 0; k < K; k++) {
+    TileArgs<T> a = tile_args<T>(ops[k], nw);
+    a.x = u ? u[k] : nullptr; a.y = yu ? yu[k] : nullptr; a.p = p ? p[k] : nullptr; a.yp = yp ? yp[k] : nullptr;
+    a.kdat = reinterpret_cast<const T *>(affine ? ops[k]->kaff : ops[k]->kgen);
+    a.kgq = reinterpret_cast<const T *>(affine ? ops[k]->kpre : ops[k]->kgq);
+    a.overwrite = overwrite ? 1 : 0;
+    a.brick0 = 0;
+    G.a[k] = a;
+  }
+  const int nb = G.a[0].ntx * G.a[0].nty * G.a[0].ntz;
+  if (nb == 0) return P3D_OK;
+  void (*kern)(const TileGroup<T>) = nullptr;
+  size_t smem = 0;
+  if (affine) {
+    kern = stokes_affine_kernel_group<T, NW_AFF, DA11, DA12, DA21>;
+    smem = AffineSmem<T, NW_AFF, DA11, DA12, DA21>::BYTES;
+  } else if (sizeof(T) == 8) {
+    kern = stokes_general_kernel_group<T, NW_GEN, DA11, DA12, DA21>;
+    smem = GeneralSmem<T, NW_GEN, DA11, DA12, DA21>::BYTES;
+  } else {
+    kern = stokes_general_tab_kernel_group<T, NW_GEN, DA11, DA12, DA21>;
+    smem = GeneralTabSmem<T, NW_GEN, DA11, DA12, DA21>::BYTES;
+  }
+  int rc = prep_kernel(kern, smem);
+  if (rc) return rc;
+  kern<<<dim3(nb, K), 32 * nw, smem, st>>>(G);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "grouped launch");
+}
+
+// zero K vectors of n elements in one launch (blockIdx.y = member)
+struct PtrGroup {
+  void *p[P3D_GROUP_MAX];
+};
+__global__ void zero_group_kernel(const __grid_constant__ PtrGroup P, size_t n_words)
+{
+  uint32_t *v = reinterpret_cast<uint32_t *>(P.p[blockIdx.y]);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n_words; i += (size_t)gridDim.x * blockDim.x) v[i] = 0u;
+}
+int zero_group(void *const *v, int K, size_t bytes, cudaStream_t st)
+{
+  if (K < 1 || K > P3D_GROUP_MAX || bytes % 4) return set_error(P3D_ERR_ARG, "zero_group: bad arguments");
+  PtrGroup P;
+  memset(&P, 0, sizeof P);
+  for (int k = 0; k < K; k++) P.p[k] = v[k];
+  const size_t words = bytes / 4;
+  size_t g = (words + 255) / 256;
+  if (g > 148 * 4) g = 148 * 4;
+  if (g < 1) g = 1;
+  zero_group_kernel<<<dim3((unsigned)g, K), 256, 0, st>>>(P, words);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "zero_group");
+}
+
+template int launch_group<double, true, false, false>(p3d_op *const *, int, const double *const *, const double *const *,
+                                                     double *const *, double *const *, cudaStream_t, bool);
+template int launch_group<float, true, false, false>(p3d_op *const *, int, const float *const *, const float *const *,
+                                                    float *const *, float *const *, cudaStream_t, bool);
+template int launch_group<double, true, true, true>(p3d_op *const *, int, const double *const *, const double *const *,
+                                                   double *const *, double *const *, cudaStream_t, bool);
+template int launch_group<double, false, true, false>(p3d_op *const *, int, const double *const *, const double *const *,
+                                                     double *const *, double *const *, cudaStream_t, bool);
+
 template <typename T> int launch_diag(p3d_op *op, T *d, cudaStream_t st)
 {
   TileArgs<T> a = tile_args<T>(op, NW_GEN);
@@ -510,6 +603,25 @@ int p3d_a11_mult(p3d_op *op, const void *x, void *y, void *stream)
   if (rc) return rc;
   if (op->prec == P3D_PREC_F64) return launch_a11<double>(op, (const double *)x, (double *)y, st, true);
   return launch_a11<float>(op, (const float *)x, (float *)y, st, true);
+}
+
+int p3d_a11_mult_grouped(p3d_op *const ops[], const void *const x[], void *const y[], int32_t k, void *stream)
+{
+  if (!ops || !x || !y || k < 1 || k > P3D_GROUP_MAX) return set_error(P3D_ERR_ARG, "a11_mult_grouped: bad arguments");
+  for (int i = 0; i < k; i++)
+    if (!ops[i] || !x[i] || !y[i]) return set_error(P3D_ERR_ARG, "a11_mult_grouped: null member %d", i);
+  P3D_REQUIRE_SETUP(ops[0]);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = 3ull * ops[0]->m.gx * ops[0]->m.gy * ops[0]->m.gz, es = ops[0]->prec == P3D_PREC_F64 ? 8 : 4;
+  if (!same_shape_ops(ops, k)) return set_error(P3D_ERR_ARG, "a11_mult_grouped: members differ in shape, path or mode");
+  // y zeroed (brick-face nodes are accumulated atomically) and never read, as p3d_a11_mult
+  int rc = zero_group(y, k, n * es, st);
+  if (rc) return rc;
+  if (ops[0]->prec == P3D_PREC_F64)
+    return launch_group<double, true, false, false>(ops, k, (const double *const *)x, nullptr, (double *const *)y,
+                                                    nullptr, st, true);
+  return launch_group<float, true, false, false>(ops, k, (const float *const *)x, nullptr, (float *const *)y, nullptr,
+                                                 st, true);
 }
 
 int p3d_a11_diagonal(p3d_op *op, void *d, void *stream)

@@ -132,6 +132,15 @@ template <typename T> struct TileArgs {
   int brick0;                 // first brick of the launch (z-chunked launches)
 };
 
+// The tile arguments of up to P3D_GROUP_MAX operators of one mesh shape,
+// passed by value to a grouped launch (kernel parameters, no device table).
+#ifndef P3D_GROUP_MAX
+#define P3D_GROUP_MAX 32
+#endif
+template <typename T> struct TileGroup {
+  TileArgs<T> a[P3D_GROUP_MAX];
+};
+
 __device__ __forceinline__ bool is_dirichlet(uint32_t m, int ix, int iy, int iz, int ox, int oy, int oz, int ex,
                                              int ey, int ez, int comp)
 {

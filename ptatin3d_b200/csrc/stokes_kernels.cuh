@@ -214,7 +214,7 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct AffineSmem
 };
 
 template <typename T, int NW, bool DA11, bool DA12, bool DA21>
-__global__ void __launch_bounds__(32 * NW, (DA12 || DA21) ? (DA11 ? 2 : 3) : 4) stokes_affine_kernel(TileArgs<T> A)
+__device__ __forceinline__ void stokes_affine_kernel_body(const TileArgs<T> &A)
 {
   using BK = Brick<NW>;
   using SM = AffineSmem<T, NW, DA11, DA12, DA21>;
@@ -310,6 +310,14 @@ __global__ void __launch_bounds__(32 * NW, (DA12 || DA21) ? (DA11 ? 2 : 3) : 4) 
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
   }
 }
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW, (DA12 || DA21) ? (DA11 ? 2 : 3) : 4) stokes_affine_kernel(TileArgs<T> A) { stokes_affine_kernel_body<T, NW, DA11, DA12, DA21>(A); }
+// the same over the K operators of a group (blockIdx.y = member), one launch
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW, (DA12 || DA21) ? (DA11 ? 2 : 3) : 4) stokes_affine_kernel_group(const __grid_constant__ TileGroup<T> G)
+{
+  stokes_affine_kernel_body<T, NW, DA11, DA12, DA21>(G.a[blockIdx.y]);
+}
 
 // Gauss-point coordinate table (general path), packed at setup, GQC values per
 // element in blocks of one brick.  A brick's block holds
@@ -356,7 +364,7 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralSme
 };
 
 template <typename T, int NW, bool DA11, bool DA12, bool DA21>
-__global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> A)
+__device__ __forceinline__ void stokes_general_kernel_body(const TileArgs<T> &A)
 {
   using BK = Brick<NW>;
   using SM = GeneralSmem<T, NW, DA11, DA12, DA21>;
@@ -466,6 +474,14 @@ __global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> 
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
   }
 }
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel(TileArgs<T> A) { stokes_general_kernel_body<T, NW, DA11, DA12, DA21>(A); }
+// the same over the K operators of a group (blockIdx.y = member), one launch
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW, 6) stokes_general_kernel_group(const __grid_constant__ TileGroup<T> G)
+{
+  stokes_general_kernel_body<T, NW, DA11, DA12, DA21>(G.a[blockIdx.y]);
+}
 
 // ---------------------------------------- general geometry, table variant
 // Used for FP32, where the table costs less than the shuffle exchange.
@@ -494,7 +510,7 @@ template <typename T, int NW, bool DA11, bool DA12, bool DA21> struct GeneralTab
 };
 
 template <typename T, int NW, bool DA11, bool DA12, bool DA21>
-__global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T> A)
+__device__ __forceinline__ void stokes_general_tab_kernel_body(const TileArgs<T> &A)
 {
   using BK = Brick<NW>;
   using SM = GeneralTabSmem<T, NW, DA11, DA12, DA21>;
@@ -624,6 +640,14 @@ __global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T>
     accumulate_tile<T, NW>(s_acc, r, L.a, L.b, L.c, L.f, L.active && valid);
     write_tile<T, NW>(A, b, s_acc, s_y, DA11 ? 0 : 1);
   }
+}
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel(TileArgs<T> A) { stokes_general_tab_kernel_body<T, NW, DA11, DA12, DA21>(A); }
+// the same over the K operators of a group (blockIdx.y = member), one launch
+template <typename T, int NW, bool DA11, bool DA12, bool DA21>
+__global__ void __launch_bounds__(32 * NW) stokes_general_tab_kernel_group(const __grid_constant__ TileGroup<T> G)
+{
+  stokes_general_tab_kernel_body<T, NW, DA11, DA12, DA21>(G.a[blockIdx.y]);
 }
 
 // --------------------------------------------------------------- diagonal

@@ -469,3 +469,42 @@ def test_fp32_ragged(cuda, dims, geom):
     op64.spmv(T(x), z64)
     op32.spmv(T(x, torch.float32), z32)
     assert rel(host(z32), host(z64)) <= TOL32
+
+
+@pytest.mark.parametrize("geom,prec", [(GEOM_AFFINE, PREC_F64), (GEOM_GENERAL, PREC_F64), (GEOM_AFFINE, PREC_F32),
+                                       (GEOM_GENERAL, PREC_F32)])
+def test_grouped_mult_equals_member_mults(cuda, geom, prec):
+    """p3d_a11_mult_grouped: five operators of one mesh shape with different
+    coefficients applied in one launch give each member's own MatMult, and a
+    member of another shape is refused."""
+    import ctypes as C
+
+    from ptatin3d_b200 import _lib
+    dims = (9, 6, 7)
+    dt = torch.float64 if prec == PREC_F64 else torch.float32
+    ops, xs, ys, refs = [], [], [], []
+    for k in range(5):
+        c = M.uniform_coords(*dims)
+        if geom == GEOM_GENERAL:
+            c = M.perturb_interior(c, *dims, frac=0.15, seed=k)
+        eta = 10 ** np.random.default_rng(k).uniform(-1, 1, size=(int(np.prod(dims)), 27))
+        op = make_op(dict(dims=dims, coords=c, eta=eta, bits=M.FREE_SLIP), prec=prec)
+        assert op.geometry_mode == geom
+        x = T(np.random.default_rng(10 + k).uniform(-1, 1, size=c.size), dt)
+        r = torch.empty_like(x)
+        op.mult(x, r)
+        ops.append(op); xs.append(x); ys.append(torch.full_like(x, float("nan"))); refs.append(r)
+    P = C.c_void_p * 5
+    rc = _lib.lib().p3d_a11_mult_grouped(P(*[o.h.value for o in ops]), P(*[x.data_ptr() for x in xs]),
+                                         P(*[y.data_ptr() for y in ys]), 5, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    _lib.check(rc)
+    torch.cuda.synchronize()
+    for y, r in zip(ys, refs):
+        assert rel(host(y), host(r)) <= (1e-14 if prec == PREC_F64 else 1e-6)
+    other = make_op(dict(dims=(9, 6, 8), coords=M.uniform_coords(9, 6, 8), eta=np.ones((9 * 6 * 8, 27)), bits=M.FREE_SLIP),
+                    prec=prec)
+    P2 = C.c_void_p * 2
+    x2 = T(np.zeros(other.n_velocity), dt)
+    rc = _lib.lib().p3d_a11_mult_grouped(P2(ops[0].h.value, other.h.value), P2(xs[0].data_ptr(), x2.data_ptr()),
+                                         P2(ys[0].data_ptr(), x2.data_ptr()), 2, None)
+    assert rc == _lib.P3D_ERR_ARG
