@@ -332,6 +332,21 @@ int p3d_solver_set_rhs(p3d_solver *s, const double *bu_dev, const double *bp_dev
 /* Solve; u (3*nn) and p (4*nel) are device FP64 arrays holding the initial
  * guess on entry and the solution on return. */
 int p3d_solver_solve(p3d_solver *s, double *u_dev, double *p_dev, p3d_solve_stats *stats);
+/* Solve k <= 32 solvers of one mesh shape and option set (each set up, with
+ * its right-hand side) together: the FGMRES iterations of all members run in
+ * lock-step, and every kernel of an iteration -- operators, smoothers,
+ * transfers, stencils, coarse solves, Gram-Schmidt -- is one launch over all
+ * members, the block preconditioner of all members one captured graph (no
+ * counterpart in the reference, which solves one system per process).  Each
+ * member keeps its own Krylov basis, step lengths and stopping test; a member
+ * that converges or breaks down leaves the group and the others go on.
+ * Members need one V-cycle per outer iteration (inner_its = 0, inner_rtol =
+ * 0) and at least 2 levels.  u[i], p[i]: device initial guesses in, solutions
+ * out; stats[i] per member; status[i] (may be NULL): P3D_OK, P3D_ERR_NOCONV
+ * or P3D_ERR_BREAKDOWN per member.  Returns P3D_OK when every member
+ * converged, else a member's failure status. */
+int p3d_solver_solve_grouped(p3d_solver *const solvers[], int32_t k, double *const u[], double *const p[],
+                             p3d_solve_stats stats[], int32_t status[]);
 /* One application of the block preconditioner (testing / external Krylov). */
 int p3d_solver_apply_pc(p3d_solver *s, const double *ru, const double *rp, double *zu, double *zp);
 /* y = A_l x with the FP64 velocity operator of multigrid level `level`
@@ -343,10 +358,12 @@ int p3d_solver_destroy(p3d_solver *s);
 /* A persistent request loop for independent Stokes solves of uneven mesh
  * sizes (no counterpart in the reference, which runs one solve per process).
  * Requests are admitted first-in first-out as soon as one of `max_active`
- * execution slots and the device memory they need (p3d_solver_estimate_bytes)
- * are free; admitted solves run concurrently, each on its own stream with its
- * state resident in HBM.  Solvers are pooled by mesh and options and reused
- * by later requests of the same shape. */
+ * workers and the device memory they need (p3d_solver_estimate_bytes) are
+ * free; a worker also takes the queued requests of the head's shape that fit
+ * and solves them as one group (shared launches, p3d_server_set_group_max).
+ * Groups of different shapes run concurrently, each on its own stream, with
+ * their state resident in HBM.  Solvers are pooled by mesh and options and
+ * reused by later requests of the same shape. */
 typedef struct p3d_server p3d_server;
 
 typedef struct p3d_request {
@@ -376,9 +393,17 @@ typedef struct p3d_server_stats {
   int32_t active, queued;
   int64_t device_bytes, peak_device_bytes; /* estimated bytes held by pooled solvers */
   int32_t solvers_created, solvers_reused;
+  int64_t grouped;        /* requests solved in groups of two or more          */
+  int64_t groups;         /* such groups                                        */
 } p3d_server_stats;
 
 int p3d_server_create(int device, int64_t hbm_budget_bytes, int32_t max_active, p3d_server **server);
+/* Up to group_max (1..32, default 8) queued requests of one mesh shape and
+ * option set are admitted together and solved as one group
+ * (p3d_solver_solve_grouped: one launch per kernel for all of them); 1 solves
+ * every request on its own.  Requests with an inner velocity solve or one
+ * level are always solved alone. */
+int p3d_server_set_group_max(p3d_server *server, int32_t group_max);
 /* Non-blocking.  The request's host arrays must stay valid until its result
  * has been returned by p3d_server_poll. */
 int p3d_server_submit(p3d_server *server, const p3d_request *request);

@@ -69,7 +69,8 @@ class Result(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64), ("active", C.c_int32),
                 ("queued", C.c_int32), ("device_bytes", C.c_int64), ("peak_device_bytes", C.c_int64),
-                ("solvers_created", C.c_int32), ("solvers_reused", C.c_int32)]
+                ("solvers_created", C.c_int32), ("solvers_reused", C.c_int32), ("grouped", C.c_int64),
+                ("groups", C.c_int64)]
 
 
 class SolveStats(C.Structure):
@@ -120,6 +121,9 @@ _SIGS = {
     "p3d_a11_apply_host_noalloc": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_op_set_host_register": ([C.c_void_p, C.c_int], C.c_int),
     "p3d_server_cancel": ([C.c_void_p, C.c_int64], C.c_int),
+    "p3d_server_set_group_max": ([C.c_void_p, C.c_int32], C.c_int),
+    "p3d_solver_solve_grouped": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                  C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
     "p3d_a11_mult_grouped": ([C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32,
                               C.c_void_p], C.c_int),
     "p3d_slab_add_plane": ([C.c_int, C.c_int32, C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -43,8 +43,8 @@ static int ggrid(size_t n)
 // in flight to stream the coefficients even on the small coarse levels.
 constexpr int STENCIL_NODES = 32;
 template <typename T>
-__global__ void __launch_bounds__(9 * STENCIL_NODES) k_stencil_apply(int nx, int ny, int nz, const T *__restrict__ G,
-                                                                    const T *__restrict__ x, T *__restrict__ y)
+__device__ __forceinline__ void stencil_apply_body(int nx, int ny, int nz, const T *__restrict__ G, const T *__restrict__ x,
+                                                   T *__restrict__ y)
 {
   __shared__ T part[9][STENCIL_NODES];
   const size_t nn = (size_t)nx * ny * nz;
@@ -68,6 +68,19 @@ __global__ void __launch_bounds__(9 * STENCIL_NODES) k_stencil_apply(int nx, int
   part[w][lane] = a;
   __syncthreads();
   if (dk == -1 && i < nn) y[3 * i + r] = part[w][lane] + part[w + 1][lane] + part[w + 2][lane];
+}
+template <typename T>
+__global__ void __launch_bounds__(9 * STENCIL_NODES) k_stencil_apply(int nx, int ny, int nz, const T *__restrict__ G,
+                                                                    const T *__restrict__ x, T *__restrict__ y)
+{
+  stencil_apply_body<T>(nx, ny, nz, G, x, y);
+}
+// over the members of a group (blockIdx.y = member): a = G, b = x, out = y
+template <typename T>
+__global__ void __launch_bounds__(9 * STENCIL_NODES) k_stencil_apply_group(const __grid_constant__ TGroup<T> P, int nx, int ny,
+                                                                          int nz)
+{
+  stencil_apply_body<T>(nx, ny, nz, P.a[blockIdx.y], P.b[blockIdx.y], P.out[blockIdx.y]);
 }
 
 // probe vector: component d of every node of colour (ci,cj,ck), zero on Dirichlet dofs
@@ -149,6 +162,15 @@ template <typename T> void g_apply(int nx, int ny, int nz, const T *G, const T *
   k_stencil_apply<T><<<(unsigned)((nn + STENCIL_NODES - 1) / STENCIL_NODES), 9 * STENCIL_NODES, 0, s>>>(nx, ny, nz, G, x, y);
   count_launch(1);
 }
+template <typename T> void g_apply_group(const TGroup<T> &P, int K, int nx, int ny, int nz, cudaStream_t s)
+{
+  const size_t nn = (size_t)nx * ny * nz;
+  k_stencil_apply_group<T><<<dim3((unsigned)((nn + STENCIL_NODES - 1) / STENCIL_NODES), K), 9 * STENCIL_NODES, 0, s>>>(P, nx,
+                                                                                                                     ny, nz);
+  count_launch(1);
+}
+template void g_apply_group<double>(const TGroup<double> &, int, int, int, int, cudaStream_t);
+template void g_apply_group<float>(const TGroup<float> &, int, int, int, int, cudaStream_t);
 void g_probe_vec(int nx, int ny, int nz, int ci, int cj, int ck, int d, uint32_t dir, double *x, cudaStream_t s)
 {
   k_probe_vec<<<ggrid((size_t)nx * ny * nz), 256, 0, s>>>(nx, ny, nz, ci, cj, ck, d, dir, x);

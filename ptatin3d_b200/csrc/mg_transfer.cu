@@ -71,8 +71,8 @@ __global__ void restrict_kernel(int cnx, int cny, int cnz, int ndof, const T *__
 // dofs count as zero, the coarse Dirichlet dofs are zeroed; one pass instead
 // of residual, mask, restriction and mask.
 template <typename T>
-__global__ void restrict_residual_kernel(int cnx, int cny, int cnz, uint32_t dir, const T *__restrict__ b,
-                                         const T *__restrict__ Ax, T *__restrict__ xc)
+__device__ __forceinline__ void restrict_residual_body(int cnx, int cny, int cnz, uint32_t dir, const T *__restrict__ b,
+                                                       const T *__restrict__ Ax, T *__restrict__ xc)
 {
   const int fnx = 2 * cnx - 1, fny = 2 * cny - 1, fnz = 2 * cnz - 1;
   const size_t total = (size_t)cnx * cny * cnz * 3;
@@ -108,7 +108,21 @@ __global__ void restrict_residual_kernel(int cnx, int cny, int cnz, uint32_t dir
 }
 
 template <typename T>
-__global__ void prolong_add_kernel(int cnx, int cny, int cnz, uint32_t dir, const T *__restrict__ xc, T *__restrict__ xf)
+__global__ void restrict_residual_kernel(int cnx, int cny, int cnz, uint32_t dir, const T *__restrict__ b,
+                                         const T *__restrict__ Ax, T *__restrict__ xc)
+{
+  restrict_residual_body<T>(cnx, cny, cnz, dir, b, Ax, xc);
+}
+// over the members of a group (blockIdx.y = member): a = b, b = Ax, out = xc
+template <typename T>
+__global__ void restrict_residual_group(const __grid_constant__ TGroup<T> G, int cnx, int cny, int cnz, uint32_t dir)
+{
+  restrict_residual_body<T>(cnx, cny, cnz, dir, G.a[blockIdx.y], G.b[blockIdx.y], G.out[blockIdx.y]);
+}
+
+template <typename T>
+__device__ __forceinline__ void prolong_add_body(int cnx, int cny, int cnz, uint32_t dir, const T *__restrict__ xc,
+                                                 T *__restrict__ xf)
 {
   const int fnx = 2 * cnx - 1, fny = 2 * cny - 1, fnz = 2 * cnz - 1;
   const size_t total = (size_t)fnx * fny * fnz * 3;
@@ -123,6 +137,18 @@ __global__ void prolong_add_kernel(int cnx, int cny, int cnz, uint32_t dir, cons
     const T s01 = C(i0, j0, k1) + C(i1, j0, k1), s11 = C(i0, j1, k1) + C(i1, j1, k1);
     xf[idx] += (T)0.125 * ((s00 + s10) + (s01 + s11));
   }
+}
+
+template <typename T>
+__global__ void prolong_add_kernel(int cnx, int cny, int cnz, uint32_t dir, const T *__restrict__ xc, T *__restrict__ xf)
+{
+  prolong_add_body<T>(cnx, cny, cnz, dir, xc, xf);
+}
+// over the members of a group: a = xc, out = xf
+template <typename T>
+__global__ void prolong_add_group(const __grid_constant__ TGroup<T> G, int cnx, int cny, int cnz, uint32_t dir)
+{
+  prolong_add_body<T>(cnx, cny, cnz, dir, G.a[blockIdx.y], G.out[blockIdx.y]);
 }
 
 static int tgrid(size_t n)
@@ -161,6 +187,26 @@ template <typename T> int mg_prolong_add(int cnx, int cny, int cnz, uint32_t dir
   count_launch(1);
   return cuda_check(cudaGetLastError(), "prolong launch");
 }
+template <typename T>
+int mg_restrict_residual_group(const TGroup<T> &G, int K, int cnx, int cny, int cnz, uint32_t dir, cudaStream_t st)
+{
+  size_t n = (size_t)cnx * cny * cnz * 3;
+  restrict_residual_group<T><<<dim3(tgrid(n), K), 256, 0, st>>>(G, cnx, cny, cnz, dir);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "grouped restrict launch");
+}
+template <typename T>
+int mg_prolong_add_group(const TGroup<T> &G, int K, int cnx, int cny, int cnz, uint32_t dir, cudaStream_t st)
+{
+  size_t n = (size_t)(2 * cnx - 1) * (2 * cny - 1) * (2 * cnz - 1) * 3;
+  prolong_add_group<T><<<dim3(tgrid(n), K), 256, 0, st>>>(G, cnx, cny, cnz, dir);
+  count_launch(1);
+  return cuda_check(cudaGetLastError(), "grouped prolong launch");
+}
+template int mg_restrict_residual_group<double>(const TGroup<double> &, int, int, int, int, uint32_t, cudaStream_t);
+template int mg_restrict_residual_group<float>(const TGroup<float> &, int, int, int, int, uint32_t, cudaStream_t);
+template int mg_prolong_add_group<double>(const TGroup<double> &, int, int, int, int, uint32_t, cudaStream_t);
+template int mg_prolong_add_group<float>(const TGroup<float> &, int, int, int, int, uint32_t, cudaStream_t);
 template int mg_restrict_residual<double>(int, int, int, uint32_t, const double *, const double *, double *, cudaStream_t);
 template int mg_restrict_residual<float>(int, int, int, uint32_t, const float *, const float *, float *, cudaStream_t);
 template int mg_prolong_add<double>(int, int, int, uint32_t, const double *, double *, cudaStream_t);

@@ -2,11 +2,13 @@
 //
 // Requests (a whole mesh, coefficients, density, gravity, solver options)
 // arrive with p3d_server_submit and are admitted first-in first-out as soon
-// as an execution slot and the HBM they need are free.  Each admitted solve
-// runs on one of `max_active` worker threads, on its own CUDA stream, with
-// all of its state (hierarchy, Krylov basis, captured preconditioner graph)
-// resident in device memory; solves that are admitted together overlap on the
-// device.  Finished solvers go back to a pool keyed by mesh and options, so a
+// as a worker and the HBM they need are free.  The worker also takes the
+// queued requests of the head's shape and options that fit (up to
+// group_max) and solves them as one group: lock-step FGMRES with every kernel
+// launched once for all members (p3d_solver_solve_grouped).  Each of the
+// `max_active` workers runs on its own CUDA streams, with all of its solves'
+// state (hierarchy, Krylov bases, captured preconditioner graph) resident in
+// device memory; groups admitted together overlap on the device.  Finished solvers go back to a pool keyed by mesh and options, so a
 // later request of the same shape reuses the device memory and only uploads
 // new coefficients (no cudaMalloc/cudaFree on the hot path).  Idle pooled
 // solvers are released, least recently used first, when a request needs
@@ -107,9 +109,9 @@ static int create_slot(Slot *s, int device)
   return rc;
 }
 
-// one solve in slot s; returns the status recorded in the result.  cancel:
-// set by p3d_server_cancel while the solve runs.
-static int run_request(Slot *s, const p3d_request &r, p3d_result &res, const std::atomic<int> *cancel)
+// the request's inputs onto the slot's device buffers, solver set-up and
+// right-hand side
+static int prepare_request(Slot *s, const p3d_request &r)
 {
   const size_t nn = (size_t)(2 * r.mx + 1) * (2 * r.my + 1) * (2 * r.mz + 1), nel = (size_t)r.mx * r.my * r.mz;
   cudaStream_t io = s->io;
@@ -121,22 +123,64 @@ static int run_request(Slot *s, const p3d_request &r, p3d_result &res, const std
   if (!rc) rc = cuda_check(cudaStreamSynchronize(io), "h2d sync");
   if (!rc) rc = solver_setup_nowait(s->solver, s->coords, s->eta); // ordered by the io sync above
   if (!rc) rc = solver_rhs_body_force_nowait(s->solver, s->rho, r.gx, r.gy, r.gz);
-  p3d_solve_stats st;
-  memset(&st, 0, sizeof st);
-  int srv = rc;
-  if (!rc) {
-    solver_set_cancel_flag(s->solver, cancel);
-    srv = solver_solve_nowait(s->solver, s->u, s->p, &st);
-    solver_set_cancel_flag(s->solver, nullptr);
+  return rc;
+}
+
+// the solution back to the request's host arrays
+static int finish_request(Slot *s, const p3d_request &r)
+{
+  const size_t nn = (size_t)(2 * r.mx + 1) * (2 * r.my + 1) * (2 * r.mz + 1), nel = (size_t)r.mx * r.my * r.mz;
+  int rc = cuda_check(cudaMemcpyAsync(r.u, s->u, 3 * nn * 8, cudaMemcpyDeviceToHost, s->io), "d2h u");
+  if (!rc) rc = cuda_check(cudaMemcpyAsync(r.p, s->p, 4 * nel * 8, cudaMemcpyDeviceToHost, s->io), "d2h p");
+  if (!rc) rc = cuda_check(cudaStreamSynchronize(s->io), "d2h sync");
+  return rc;
+}
+
+// requests that can share grouped launches: one V-cycle per outer iteration
+static bool groupable(const p3d_request &r)
+{
+  return r.opts.inner_its == 0 && r.opts.inner_rtol == 0.0 && r.opts.nlevels >= 2 && r.opts.use_graph;
+}
+
+// the solves of several requests of one shape in slots s[0..K): set-up of
+// each, then one grouped solve (p3d_solver_solve_grouped); status per member
+static void run_group(Slot *const *s, const p3d_request *const *r, int K, p3d_result *res,
+                      const std::atomic<int> *const *cancel, int *status)
+{
+  p3d_solver *sol[P3D_GROUP_MAX];
+  double *u[P3D_GROUP_MAX], *p[P3D_GROUP_MAX];
+  int idx[P3D_GROUP_MAX], n = 0;
+  for (int k = 0; k < K; k++) {
+    status[k] = prepare_request(s[k], *r[k]);
+    res[k].iterations = 0;
+    res[k].rel_residual = 0.0;
+    if (!status[k] && cancel[k]->load()) status[k] = P3D_ERR_CANCELLED;
+    if (status[k]) continue;
+    sol[n] = s[k]->solver; u[n] = s[k]->u; p[n] = s[k]->p; idx[n] = k;
+    solver_set_cancel_flag(s[k]->solver, cancel[k]);
+    n++;
   }
-  if (!rc && (srv == P3D_OK || srv == P3D_ERR_NOCONV || srv == P3D_ERR_CANCELLED)) {
-    rc = cuda_check(cudaMemcpyAsync(r.u, s->u, 3 * nn * 8, cudaMemcpyDeviceToHost, io), "d2h u");
-    if (!rc) rc = cuda_check(cudaMemcpyAsync(r.p, s->p, 4 * nel * 8, cudaMemcpyDeviceToHost, io), "d2h p");
-    if (!rc) rc = cuda_check(cudaStreamSynchronize(io), "d2h sync");
+  if (!n) return;
+  p3d_solve_stats st[P3D_GROUP_MAX];
+  int ms[P3D_GROUP_MAX];
+  memset(st, 0, sizeof st);
+  const int rc = n == 1 ? solver_solve_nowait(sol[0], u[0], p[0], &st[0])
+                        : solver_group_solve(sol, n, u, p, st, ms);
+  if (n == 1) ms[0] = rc;
+  for (int q = 0; q < n; q++) {
+    const int k = idx[q];
+    solver_set_cancel_flag(s[k]->solver, nullptr);
+    int sk = (n > 1 && rc != P3D_OK && rc != P3D_ERR_NOCONV && rc != P3D_ERR_BREAKDOWN && rc != P3D_ERR_CANCELLED)
+                 ? rc
+                 : ms[q];
+    if (sk == P3D_OK || sk == P3D_ERR_NOCONV || sk == P3D_ERR_CANCELLED) {
+      const int fr = finish_request(s[k], *r[k]);
+      if (fr) sk = fr;
+    }
+    status[k] = sk;
+    res[k].iterations = st[q].iterations;
+    res[k].rel_residual = st[q].r0 > 0 ? st[q].rfinal / st[q].r0 : 0.0;
   }
-  res.iterations = st.iterations;
-  res.rel_residual = st.r0 > 0 ? st.rfinal / st.r0 : 0.0;
-  return rc ? rc : srv;
 }
 
 } // namespace p3d
@@ -147,6 +191,7 @@ struct p3d_server {
   int device = 0;
   int64_t budget = 0;
   int max_active = 1;
+  int group_max = 8; // requests of one shape solved together by one worker
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Pending> queue;
@@ -166,9 +211,8 @@ namespace p3d {
 // Under the lock: pick (or reserve memory for) a slot for the queue head.
 // Returns the slot, or nullptr when the head must wait.  `evict` collects idle
 // slots to release outside the lock.
-static Slot *admit_head(p3d_server *S, std::vector<Slot *> &evict, bool &fresh, bool &too_big)
+static Slot *admit_request(p3d_server *S, const p3d_request &r, std::vector<Slot *> &evict, bool &fresh, bool &too_big)
 {
-  const p3d_request &r = S->queue.front().req;
   fresh = false;
   too_big = false;
   for (Slot *s : S->slots)
@@ -213,7 +257,7 @@ static void worker(p3d_server *S)
     }
     std::vector<Slot *> evict;
     bool fresh = false, too_big = false;
-    Slot *slot = admit_head(S, evict, fresh, too_big);
+    Slot *slot = admit_request(S, S->queue.front().req, evict, fresh, too_big);
     if (!slot && !too_big) {
       if (!evict.empty()) { // memory was given back: release it and look again
         lk.unlock();
@@ -239,37 +283,91 @@ static void worker(p3d_server *S)
       S->cv_done.notify_all();
       continue;
     }
+    // the head, and queued requests of its shape that fit, form a group
+    Slot *gs[P3D_GROUP_MAX];
+    Pending gj[P3D_GROUP_MAX];
+    bool gfresh[P3D_GROUP_MAX];
+    int K = 0;
+    gs[K] = slot; gj[K] = job; gfresh[K] = fresh; K++;
     slot->busy = true;
-    S->active++;
-    S->st.admitted++;
-    if (fresh) S->st.solvers_created++;
-    else S->st.solvers_reused++;
+    if (groupable(job.req))
+      for (auto it = S->queue.begin(); it != S->queue.end() && K < std::min(S->group_max, P3D_GROUP_MAX);) {
+        if (!(groupable(it->req) && it->req.mx == job.req.mx && it->req.my == job.req.my && it->req.mz == job.req.mz &&
+              it->req.dirichlet == job.req.dirichlet && same_opts(it->req.opts, job.req.opts))) {
+          ++it;
+          continue;
+        }
+        bool f2 = false, big2 = false;
+        Slot *s2 = admit_request(S, it->req, evict, f2, big2);
+        if (!s2) break; // no slot or memory for more now
+        s2->busy = true;
+        gs[K] = s2; gj[K] = *it; gfresh[K] = f2; K++;
+        it = S->queue.erase(it);
+      }
+    std::atomic<int> cflag[P3D_GROUP_MAX];
+    for (int k = 0; k < K; k++) {
+      cflag[k].store(0);
+      S->active++;
+      S->st.admitted++;
+      if (gfresh[k]) S->st.solvers_created++;
+      else S->st.solvers_reused++;
+      S->running.emplace_back(gj[k].req.tag, &cflag[k]);
+    }
     S->cv_work.notify_all(); // the next request may fit as well
     lk.unlock();
     for (Slot *e : evict) { release_slot(e); delete e; }
-    std::atomic<int> cancel_flag{0};
-    lk.lock();
-    S->running.emplace_back(job.req.tag, &cancel_flag);
-    lk.unlock();
-    int rc = fresh ? create_slot(slot, S->device) : P3D_OK;
-    if (!rc) rc = cancel_flag.load() ? P3D_ERR_CANCELLED : run_request(slot, job.req, res, &cancel_flag);
-    const double t_end = wall_ms();
-    res.status = rc;
-    res.run_ms = t_end - t_admit;
-    res.latency_ms = t_end - job.t_submit;
-    lk.lock();
-    for (auto it = S->running.begin(); it != S->running.end(); ++it)
-      if (it->second == &cancel_flag) { S->running.erase(it); break; }
-    slot->busy = false;
-    slot->last_used = ++S->clock;
-    if (!slot->ready) { // creation failed: give the memory back
-      S->bytes -= slot->bytes;
-      S->slots.erase(std::find(S->slots.begin(), S->slots.end(), slot));
-      delete slot;
+    p3d_result gres[P3D_GROUP_MAX];
+    int gst[P3D_GROUP_MAX];
+    const p3d_request *greq[P3D_GROUP_MAX];
+    const std::atomic<int> *gcan[P3D_GROUP_MAX];
+    Slot *run_s[P3D_GROUP_MAX];
+    const p3d_request *run_r[P3D_GROUP_MAX];
+    const std::atomic<int> *run_c[P3D_GROUP_MAX];
+    int run_i[P3D_GROUP_MAX], nrun = 0;
+    for (int k = 0; k < K; k++) {
+      memset(&gres[k], 0, sizeof gres[k]);
+      gres[k].tag = gj[k].req.tag;
+      gres[k].wait_ms = (k == 0 ? t_admit : wall_ms()) - gj[k].t_submit;
+      greq[k] = &gj[k].req;
+      gcan[k] = &cflag[k];
+      gst[k] = gfresh[k] ? create_slot(gs[k], S->device) : P3D_OK;
+      if (!gst[k]) { run_s[nrun] = gs[k]; run_r[nrun] = greq[k]; run_c[nrun] = gcan[k]; run_i[nrun] = k; nrun++; }
     }
-    S->active--;
-    S->done.push_back(res);
-    S->st.completed++;
+    if (nrun > 1) {
+      std::lock_guard<std::mutex> g2(S->mu);
+      S->st.grouped += nrun;
+      S->st.groups++;
+    }
+    if (nrun) {
+      p3d_result rr[P3D_GROUP_MAX];
+      int rs[P3D_GROUP_MAX];
+      run_group(run_s, run_r, nrun, rr, run_c, rs);
+      for (int q = 0; q < nrun; q++) {
+        gst[run_i[q]] = rs[q];
+        gres[run_i[q]].iterations = rr[q].iterations;
+        gres[run_i[q]].rel_residual = rr[q].rel_residual;
+      }
+    }
+    const double t_end = wall_ms();
+    lk.lock();
+    for (int k = 0; k < K; k++) {
+      gres[k].status = gst[k];
+      gres[k].run_ms = t_end - t_admit;
+      gres[k].latency_ms = t_end - gj[k].t_submit;
+      for (auto it = S->running.begin(); it != S->running.end(); ++it)
+        if (it->second == &cflag[k]) { S->running.erase(it); break; }
+      Slot *sl = gs[k];
+      sl->busy = false;
+      sl->last_used = ++S->clock;
+      if (!sl->ready) { // creation failed: give the memory back
+        S->bytes -= sl->bytes;
+        S->slots.erase(std::find(S->slots.begin(), S->slots.end(), sl));
+        delete sl;
+      }
+      S->active--;
+      S->done.push_back(gres[k]);
+      S->st.completed++;
+    }
     S->cv_done.notify_all();
     S->cv_work.notify_all();
   }
@@ -292,6 +390,15 @@ int p3d_server_create(int device, int64_t hbm_budget_bytes, int32_t max_active, 
   S->max_active = max_active;
   for (int i = 0; i < max_active; i++) S->workers.emplace_back(worker, S);
   *out = S;
+  return P3D_OK;
+}
+
+int p3d_server_set_group_max(p3d_server *S, int32_t group_max)
+{
+  if (!S || group_max < 1 || group_max > P3D_GROUP_MAX)
+    return set_error(P3D_ERR_ARG, "server_set_group_max: 1..%d", P3D_GROUP_MAX);
+  std::lock_guard<std::mutex> g(S->mu);
+  S->group_max = group_max;
   return P3D_OK;
 }
 

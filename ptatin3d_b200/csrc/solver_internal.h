@@ -6,6 +6,9 @@
 #include <atomic>
 #include <stdint.h>
 
+#ifndef P3D_GROUP_MAX
+#define P3D_GROUP_MAX 32
+#endif
 #define P3D_MDOT_CHUNK 8    // vectors per multi-dot / multi-axpy launch (register accumulators)
 #define P3D_MDOT_BLOCKS 592 // 4 x 148 SMs
 
@@ -34,6 +37,54 @@ template <typename T> void v_cg_p(size_t n, const double *num, const double *den
 void v_block4(size_t nel, const double *B, const double *x, double *y, double alpha, cudaStream_t s);
 void v_invert_diag(size_t n, const double *d, double *dinv, unsigned int *bad, cudaStream_t s);
 void v_dense_mv(int n, const double *M, const double *x, double *y, cudaStream_t s);
+
+// vec_kernels.cu, grouped forms: one launch over the K members of a group of
+// same-shape solves (blockIdx.y = member); roles of v[] per kernel:
+//   cheb_init0   v0 b, v1 x, v2 r, v3 d; s0 1/theta
+//   cheb_init_res v0 b, v1 Ax, v2 r, v3 d; s0 1/theta
+//   cheb_step    v0 x, v1 r, v2 Ad, v3 d; s0 c1, s1 c2
+//   axpby        v0 x, v1 y; s0 a, s1 b (y = a x + b y; y not read when b = 0)
+//   residual     v0 b, v1 Ax, v2 r
+//   convert      v0 in, v1 out (raw pointers)
+//   block4       v0 B, v1 x, v2 y;  dense_mv v0 M, v1 x, v2 y
+template <typename T> struct VGroup {
+  T *v[4][P3D_GROUP_MAX];
+  const double *dinv[P3D_GROUP_MAX];
+  double s[2][P3D_GROUP_MAX];
+};
+// Gram-Schmidt per member: V[m] its basis (device array of vector pointers),
+// w[m] the vector, out[m] the coefficients (device), self_out[m] |w|^2 or
+// nullptr, part[m] its partials buffer and ticket
+struct MGroup {
+  double *const *V[P3D_GROUP_MAX];
+  double *w[P3D_GROUP_MAX];
+  double *out[P3D_GROUP_MAX];
+  double *self_out[P3D_GROUP_MAX];
+  double *part[P3D_GROUP_MAX];
+};
+template <typename T> void vg_cheb_init0(const VGroup<T> &G, int K, size_t n, cudaStream_t s);
+template <typename T> void vg_cheb_init_res(const VGroup<T> &G, int K, size_t n, cudaStream_t s);
+template <typename T> void vg_cheb_step(const VGroup<T> &G, int K, size_t n, bool last, cudaStream_t s);
+template <typename T> void vg_axpby(const VGroup<T> &G, int K, size_t n, cudaStream_t s);
+template <typename T> void vg_residual(const VGroup<T> &G, int K, size_t n, cudaStream_t s);
+template <typename A, typename B> void vg_convert(const VGroup<double> &G, int K, size_t n, cudaStream_t s);
+void vg_block4(const VGroup<double> &G, int K, size_t nel, cudaStream_t s);
+void vg_dense_mv(const VGroup<double> &G, int K, int n, cudaStream_t s);
+void vg_mdot(const MGroup &G, int K, size_t n, int k, cudaStream_t s);
+void vg_maxpy(const MGroup &G, int K, size_t n, int k, double sign, cudaStream_t s);
+// per-member operands of the grouped transfers and stencil applies
+template <typename T> struct TGroup {
+  const T *a[P3D_GROUP_MAX];
+  const T *b[P3D_GROUP_MAX];
+  T *out[P3D_GROUP_MAX];
+};
+// mg_transfer.cu: restrict_residual (a = b, b = Ax, out = xc), prolong_add (a = xc, out = xf)
+template <typename T>
+int mg_restrict_residual_group(const TGroup<T> &G, int K, int cnx, int cny, int cnz, uint32_t dir, cudaStream_t st);
+template <typename T>
+int mg_prolong_add_group(const TGroup<T> &G, int K, int cnx, int cny, int cnz, uint32_t dir, cudaStream_t st);
+// galerkin.cu: y = G x per member (a = G, b = x, out = y)
+template <typename T> void g_apply_group(const TGroup<T> &P, int K, int nx, int ny, int nz, cudaStream_t s);
 
 // setup_kernels.cu (whole-mesh lattices, FP64)
 void s_schur_blocks(int mx, int my, int mz, const double *coords, const double *eta, int geomean, double *Binv,
@@ -69,6 +120,12 @@ int solver_solve_nowait(p3d_solver *s, double *u, double *p, struct p3d_solve_st
 // a flag the outer iteration reads between iterations: non-zero ends the
 // solve with P3D_ERR_CANCELLED (u, p the iterate reached); nullptr: none
 void solver_set_cancel_flag(p3d_solver *s, const std::atomic<int> *flag);
+// lock-step solve of K same-shape solvers (set up, right-hand sides set);
+// u, p: device initial guesses in, solutions out; stats per member.  Returns
+// P3D_OK when all converged, else a failure's status; status[k] (may be
+// nullptr) per member: P3D_OK, P3D_ERR_NOCONV, _BREAKDOWN or _CANCELLED.
+int solver_group_solve(p3d_solver *const *solvers, int K, double *const *u, double *const *p,
+                       struct p3d_solve_stats *stats, int *status);
 
 // dense_inverse.cu (coarse-grid operator, in place, blocked Gauss-Jordan)
 size_t dense_inverse_scratch(int n);

@@ -60,6 +60,7 @@ struct p3d_solver {
   // FGMRES
   double *V = nullptr, *Z = nullptr, *w = nullptr;
   double **Vptr = nullptr; // device array of pointers: V_0..V_m, then one scratch slot
+  double **Zptr = nullptr; // device array of pointers: Z_0..Z_{m-1} (grouped solves)
   double *part = nullptr, *hdev = nullptr;
   double *hhost = nullptr; // pinned; [0,hs) and [hs,2hs) Gram-Schmidt passes, 2hs norm
   int hs = 0;              // restart + 1
@@ -795,6 +796,586 @@ static int fgmres(p3d_solver *s, double *x, p3d_solve_stats *stats)
 
 void solver_set_cancel_flag(p3d_solver *s, const std::atomic<int> *flag) { s->cancel = flag; }
 
+
+// ============================================================ grouped solve
+// The solves of K solvers of one mesh shape and option set, in lock-step:
+// every kernel of an iteration -- operators, smoothers, transfers, stencils,
+// coarse solves, Gram-Schmidt -- is one launch over all members (grid
+// dimension y = member, per-member pointers and scalars in the launch
+// parameters), and the block preconditioner of all members is one captured
+// graph.  Each member keeps its own Krylov basis, Hessenberg matrix, step
+// lengths and stopping test, so its iterates are those of its own solve; a
+// member that converges (or breaks down) leaves the group, and the others go
+// on (the graph is captured again for the smaller group).
+struct Group {
+  int K = 0;
+  p3d_solver *m[P3D_GROUP_MAX] = {};
+  cudaStream_t st = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+};
+
+template <typename T> static T *lvec(void *p) { return reinterpret_cast<T *>(p); }
+
+// y = A_l x on level l for every member (y overwritten)
+template <typename T> static int g_a11(Group &g, int l, T *const *x, T *const *y)
+{
+  Level &L0 = g.m[0]->lv[l];
+  if (L0.gal) {
+    TGroup<T> P;
+    memset(&P, 0, sizeof P);
+    for (int k = 0; k < g.K; k++) {
+      Level &L = g.m[k]->lv[l];
+      P.a[k] = sizeof(T) == 8 ? (const T *)L.G64 : (const T *)L.G32;
+      P.b[k] = x[k];
+      P.out[k] = y[k];
+    }
+    g_apply_group<T>(P, g.K, L0.n[0], L0.n[1], L0.n[2], g.st);
+    return P3D_OK;
+  }
+  p3d_op *ops[P3D_GROUP_MAX];
+  for (int k = 0; k < g.K; k++) ops[k] = sizeof(T) == 8 ? g.m[k]->lv[l].op64 : g.m[k]->lv[l].op32;
+  CK(zero_group((void *const *)y, g.K, L0.nv * sizeof(T), g.st));
+  return launch_group<T, true, false, false>(ops, g.K, (const T *const *)x, nullptr, y, nullptr, g.st, true);
+}
+
+template <typename T> static int g_smooth(Group &g, int l, T *const *b, T *const *x, bool zero_guess)
+{
+  const int K = g.K;
+  const size_t n = g.m[0]->lv[l].nv;
+  double theta[P3D_GROUP_MAX], delta[P3D_GROUP_MAX], sigma[P3D_GROUP_MAX], rho[P3D_GROUP_MAX];
+  T *r[P3D_GROUP_MAX], *d[P3D_GROUP_MAX], *t[P3D_GROUP_MAX];
+  VGroup<T> V;
+  memset(&V, 0, sizeof V);
+  for (int k = 0; k < K; k++) {
+    Level &L = g.m[k]->lv[l];
+    const double lo = g.m[k]->o.cheb_lo * L.lmax, hi = g.m[k]->o.cheb_hi * L.lmax;
+    theta[k] = 0.5 * (hi + lo); delta[k] = 0.5 * (hi - lo); sigma[k] = theta[k] / delta[k]; rho[k] = 1.0 / sigma[k];
+    r[k] = lvec<T>(L.r); d[k] = lvec<T>(L.d); t[k] = lvec<T>(L.t);
+    V.dinv[k] = L.dinv;
+    V.s[0][k] = 1.0 / theta[k];
+  }
+  if (zero_guess) {
+    for (int k = 0; k < K; k++) { V.v[0][k] = b[k]; V.v[1][k] = x[k]; V.v[2][k] = r[k]; V.v[3][k] = d[k]; }
+    vg_cheb_init0<T>(V, K, n, g.st);
+  } else {
+    CK(g_a11<T>(g, l, x, t));
+    for (int k = 0; k < K; k++) { V.v[0][k] = b[k]; V.v[1][k] = t[k]; V.v[2][k] = r[k]; V.v[3][k] = d[k]; }
+    vg_cheb_init_res<T>(V, K, n, g.st);
+  }
+  const int its = std::max(1, g.m[0]->o.cheb_its);
+  if (its == 1) {
+    for (int k = 0; k < K; k++) { V.v[0][k] = d[k]; V.v[1][k] = x[k]; V.s[0][k] = 1.0; V.s[1][k] = 1.0; }
+    vg_axpby<T>(V, K, n, g.st); // x += d
+    return P3D_OK;
+  }
+  for (int step = 0; step < its - 1; step++) {
+    CK(g_a11<T>(g, l, d, t));
+    for (int k = 0; k < K; k++) {
+      const double rn = 1.0 / (2.0 * sigma[k] - rho[k]);
+      V.v[0][k] = x[k]; V.v[1][k] = r[k]; V.v[2][k] = t[k]; V.v[3][k] = d[k];
+      V.s[0][k] = rn * rho[k];
+      V.s[1][k] = 2.0 * rn / delta[k];
+      rho[k] = rn;
+    }
+    vg_cheb_step<T>(V, K, n, step == its - 2, g.st);
+  }
+  return P3D_OK;
+}
+
+template <typename T> static int g_coarse(Group &g, T *const *b, T *const *x)
+{
+  const int K = g.K, nc = g.m[0]->nc;
+  VGroup<double> V;
+  memset(&V, 0, sizeof V);
+  if (sizeof(T) == 8) {
+    for (int k = 0; k < K; k++) { V.v[0][k] = g.m[k]->cinv; V.v[1][k] = (double *)b[k]; V.v[2][k] = (double *)x[k]; }
+    vg_dense_mv(V, K, nc, g.st);
+    return P3D_OK;
+  }
+  for (int k = 0; k < K; k++) { V.v[0][k] = (double *)b[k]; V.v[1][k] = g.m[k]->cb64; }
+  vg_convert<float, double>(V, K, nc, g.st);
+  for (int k = 0; k < K; k++) { V.v[0][k] = g.m[k]->cinv; V.v[1][k] = g.m[k]->cb64; V.v[2][k] = g.m[k]->cx64; }
+  vg_dense_mv(V, K, nc, g.st);
+  for (int k = 0; k < K; k++) { V.v[0][k] = g.m[k]->cx64; V.v[1][k] = (double *)x[k]; }
+  vg_convert<double, float>(V, K, nc, g.st);
+  return P3D_OK;
+}
+
+template <typename T> static int g_vcycle(Group &g, int l, T *const *b, T *const *x)
+{
+  if (l == 0) return g_coarse<T>(g, b, x);
+  const int K = g.K;
+  Level &C0 = g.m[0]->lv[l - 1];
+  const uint32_t dir = level_dir(g.m[0]);
+  T *t[P3D_GROUP_MAX], *cb[P3D_GROUP_MAX], *cx[P3D_GROUP_MAX];
+  for (int k = 0; k < K; k++) {
+    t[k] = lvec<T>(g.m[k]->lv[l].t);
+    cb[k] = lvec<T>(g.m[k]->lv[l - 1].b);
+    cx[k] = lvec<T>(g.m[k]->lv[l - 1].x);
+  }
+  CK(g_smooth<T>(g, l, b, x, true));
+  CK(g_a11<T>(g, l, x, t));
+  TGroup<T> P;
+  memset(&P, 0, sizeof P);
+  for (int k = 0; k < K; k++) { P.a[k] = b[k]; P.b[k] = t[k]; P.out[k] = cb[k]; }
+  CK(mg_restrict_residual_group<T>(P, K, C0.n[0], C0.n[1], C0.n[2], dir, g.st));
+  CK(g_vcycle<T>(g, l - 1, cb, cx));
+  memset(&P, 0, sizeof P);
+  for (int k = 0; k < K; k++) { P.a[k] = cx[k]; P.out[k] = x[k]; }
+  CK(mg_prolong_add_group<T>(P, K, C0.n[0], C0.n[1], C0.n[2], dir, g.st));
+  return g_smooth<T>(g, l, b, x, false);
+}
+
+// the block preconditioner of every member on its pc_in -> pc_out
+static int g_apply_pc(Group &g)
+{
+  const int K = g.K;
+  const size_t nu = g.m[0]->nu, np = g.m[0]->np;
+  VGroup<double> V;
+  memset(&V, 0, sizeof V);
+  p3d_op *ops[P3D_GROUP_MAX];
+  double *t[P3D_GROUP_MAX], *zp[P3D_GROUP_MAX];
+  for (int k = 0; k < K; k++) {
+    p3d_solver *s = g.m[k];
+    V.v[0][k] = s->Binv; V.v[1][k] = s->pc_in + nu; V.v[2][k] = s->pc_out + nu;
+    t[k] = s->pc_t;
+    zp[k] = s->pc_out + nu;
+    ops[k] = s->lv.back().op64;
+  }
+  vg_block4(V, K, np / 4, g.st); // zp = S^{-1} rp
+  CK(zero_group((void *const *)t, K, nu * 8, g.st));
+  CK((launch_group<double, false, true, false>(ops, K, nullptr, (const double *const *)zp, t, nullptr, g.st, false)));
+  for (int k = 0; k < K; k++) { V.v[0][k] = g.m[k]->pc_in; V.v[1][k] = t[k]; V.s[0][k] = 1.0; V.s[1][k] = -1.0; }
+  vg_axpby<double>(V, K, nu, g.st); // t = ru - A12 zp
+  const int top = (int)g.m[0]->lv.size() - 1;
+  if (g.m[0]->o.mg_precision == P3D_PREC_F64) {
+    double *zu[P3D_GROUP_MAX];
+    for (int k = 0; k < K; k++) zu[k] = g.m[k]->pc_out;
+    return g_vcycle<double>(g, top, t, zu);
+  }
+  float *tf[P3D_GROUP_MAX], *xf[P3D_GROUP_MAX];
+  for (int k = 0; k < K; k++) {
+    tf[k] = lvec<float>(g.m[k]->cg_r);
+    xf[k] = lvec<float>(g.m[k]->lv.back().x);
+    V.v[0][k] = t[k]; V.v[1][k] = (double *)tf[k];
+  }
+  vg_convert<double, float>(V, K, nu, g.st);
+  CK(g_vcycle<float>(g, top, tf, xf));
+  for (int k = 0; k < K; k++) { V.v[0][k] = (double *)xf[k]; V.v[1][k] = g.m[k]->pc_out; }
+  vg_convert<float, double>(V, K, nu, g.st);
+  return P3D_OK;
+}
+
+static void g_release_graph(Group &g)
+{
+  if (g.gexec) cudaGraphExecDestroy(g.gexec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  g.gexec = nullptr;
+  g.graph = nullptr;
+}
+
+// capture the grouped preconditioner of the current members (after one eager run)
+static int g_capture(Group &g)
+{
+  g_release_graph(g);
+  CK(g_apply_pc(g));
+  CU(cudaStreamSynchronize(g.st), "grouped pc warm");
+  CU(cudaStreamBeginCapture(g.st, cudaStreamCaptureModeThreadLocal), "begin capture");
+  int rc = g_apply_pc(g);
+  cudaGraph_t gr = nullptr;
+  cudaError_t e = cudaStreamEndCapture(g.st, &gr);
+  if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+  CU(e, "end capture");
+  g.graph = gr;
+  return cuda_check(cudaGraphInstantiate(&g.gexec, gr, 0), "graph instantiate");
+}
+
+// y = [A11 A12; A21 0] x for every member
+static int g_stokes_op(Group &g, double *const *x, double *const *y)
+{
+  const int K = g.K;
+  const size_t nu = g.m[0]->nu;
+  p3d_op *ops[P3D_GROUP_MAX];
+  const double *u[P3D_GROUP_MAX], *p[P3D_GROUP_MAX];
+  double *yu[P3D_GROUP_MAX], *yp[P3D_GROUP_MAX];
+  for (int k = 0; k < K; k++) {
+    ops[k] = g.m[k]->lv.back().op64;
+    u[k] = x[k]; p[k] = x[k] + nu; yu[k] = y[k]; yp[k] = y[k] + nu;
+  }
+  CK(zero_group((void *const *)y, K, g.m[0]->N * 8, g.st));
+  return launch_group<double, true, true, true>(ops, K, u, p, yu, yp, g.st, true);
+}
+
+// |v_k|^2 of every member into hhost[2hs] (one synchronisation); v given by
+// the member's Vptr slot `slot`
+static int g_norms2(Group &g, int slot, double *const *v, double *out)
+{
+  MGroup M;
+  memset(&M, 0, sizeof M);
+  for (int k = 0; k < g.K; k++) {
+    p3d_solver *s = g.m[k];
+    M.V[k] = s->Vptr + slot;
+    M.w[k] = v[k];
+    M.out[k] = s->hdev + 2 * s->hs;
+    M.part[k] = s->part;
+  }
+  vg_mdot(M, g.K, g.m[0]->N, 1, g.st);
+  for (int k = 0; k < g.K; k++)
+    CU(cudaMemcpyAsync(g.m[k]->hhost + 2 * g.m[k]->hs, g.m[k]->hdev + 2 * g.m[k]->hs, 8, cudaMemcpyDeviceToHost, g.st), "d2h");
+  CU(cudaStreamSynchronize(g.st), "sync");
+  for (int k = 0; k < g.K; k++) {
+    const double ss = g.m[k]->hhost[2 * g.m[k]->hs];
+    out[k] = ss > 0.0 ? std::sqrt(ss) : (ss <= 0.0 ? 0.0 : ss);
+  }
+  return P3D_OK;
+}
+
+struct MemberState {
+  std::vector<double> H, cs, sn, gv, y;
+  double r0 = -1.0, tol = 0.0, rnorm = 0.0;
+  int its = 0;
+  bool conv = false, done = false;
+  int status = P3D_OK;
+};
+
+// x += sum_{i<j} y_i Z_i for the members listed (coefficients uploaded to hdev)
+static int g_update_x(Group &g, const std::vector<int> &idx, std::vector<MemberState> &ms, int j, int msize)
+{
+  if (idx.empty() || j == 0) return P3D_OK;
+  MGroup M;
+  memset(&M, 0, sizeof M);
+  int K = 0;
+  for (int k : idx) {
+    p3d_solver *s = g.m[k];
+    MemberState &st = ms[k];
+    for (int i = j - 1; i >= 0; i--) {
+      double acc = st.gv[i];
+      for (int c = i + 1; c < j; c++) acc -= st.H[(size_t)i * msize + c] * st.y[c];
+      st.y[i] = acc / st.H[(size_t)i * msize + i];
+    }
+    CU(cudaMemcpyAsync(s->hdev, st.y.data(), j * 8, cudaMemcpyHostToDevice, g.st), "h2d y");
+    M.V[K] = s->Zptr;
+    M.w[K] = s->xsol;
+    M.out[K] = s->hdev;
+    K++;
+  }
+  vg_maxpy(M, K, g.m[0]->N, j, 1.0, g.st);
+  return cuda_check(cudaStreamSynchronize(g.st), "x update"); // y (host) must outlive the copy
+}
+
+// lock-step FGMRES(m) of the members; their xsol hold the initial guesses
+static int group_fgmres(Group &all, std::vector<MemberState> &ms)
+{
+  const int msize = all.m[0]->o.restart, max_it = all.m[0]->o.max_it;
+  const size_t N = all.m[0]->N;
+  for (int k = 0; k < all.K; k++) {
+    ms[k].H.assign((size_t)(msize + 1) * msize, 0.0);
+    ms[k].cs.assign(msize, 0.0); ms[k].sn.assign(msize, 0.0);
+    ms[k].gv.assign(msize + 1, 0.0); ms[k].y.assign(msize, 0.0);
+    // the scratch slot of the basis pointers names the member's w (norms)
+    double *w = all.m[k]->w;
+    CU(cudaMemcpyAsync(all.m[k]->Vptr + all.m[k]->hs, &w, sizeof(double *), cudaMemcpyHostToDevice, all.st), "ptr");
+  }
+  CU(cudaStreamSynchronize(all.st), "sync");
+  std::vector<int> act; // indices into all.m of the members still solving
+  for (int k = 0; k < all.K; k++) act.push_back(k);
+  int rc = P3D_OK;
+  Group g;
+  g.st = all.st;
+  auto rebuild = [&]() -> int {
+    g_release_graph(g);
+    g.K = (int)act.size();
+    for (int i = 0; i < g.K; i++) g.m[i] = all.m[act[i]];
+    if (!g.K) return P3D_OK;
+    return g_capture(g);
+  };
+  int its = 0;
+  if ((rc = rebuild())) return rc;
+  while (!act.empty() && its < max_it) {
+    // r = b - A x into V_0 of every member, |r|
+    double *x[P3D_GROUP_MAX], *w[P3D_GROUP_MAX], *v0[P3D_GROUP_MAX];
+    for (int i = 0; i < g.K; i++) { x[i] = g.m[i]->xsol; w[i] = g.m[i]->w; v0[i] = g.m[i]->V; }
+    if ((rc = g_stokes_op(g, x, w))) break;
+    VGroup<double> V;
+    memset(&V, 0, sizeof V);
+    for (int i = 0; i < g.K; i++) { V.v[0][i] = g.m[i]->bvec; V.v[1][i] = w[i]; V.v[2][i] = v0[i]; }
+    vg_residual<double>(V, g.K, N, g.st);
+    double beta[P3D_GROUP_MAX];
+    if ((rc = g_norms2(g, 0, v0, beta))) break;
+    std::vector<int> leave;
+    for (int i = 0; i < g.K; i++) {
+      MemberState &st = ms[act[i]];
+      if (st.r0 < 0) st.r0 = beta[i];
+      st.rnorm = beta[i];
+      st.tol = std::max(g.m[i]->o.rtol * st.r0, g.m[i]->o.atol);
+      if (!std::isfinite(beta[i])) { st.status = set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual"); leave.push_back(i); }
+      else if (beta[i] <= st.tol) { st.conv = true; leave.push_back(i); }
+    }
+    if (!leave.empty()) {
+      std::vector<int> keep;
+      for (int i = 0; i < g.K; i++)
+        if (std::find(leave.begin(), leave.end(), i) == leave.end()) keep.push_back(act[i]);
+      act = keep;
+      if ((rc = rebuild())) break;
+      continue; // recompute the residual pointers for the smaller group
+    }
+    for (int i = 0; i < g.K; i++) {
+      V.v[0][i] = v0[i]; V.v[1][i] = v0[i]; V.s[0][i] = 1.0 / beta[i]; V.s[1][i] = 0.0;
+      MemberState &st = ms[act[i]];
+      std::fill(st.gv.begin(), st.gv.end(), 0.0);
+      st.gv[0] = beta[i];
+    }
+    vg_axpby<double>(V, g.K, N, g.st); // V_0 /= beta
+    int j = 0;
+    bool cycle_end = false;
+    for (; j < msize && its < max_it && !cycle_end; j++, its++) {
+      // z_j = PC v_j (grouped graph), w = A z_j
+      for (int i = 0; i < g.K; i++) {
+        V.v[0][i] = g.m[i]->V + (size_t)j * N; V.v[1][i] = g.m[i]->pc_in; V.s[0][i] = 1.0; V.s[1][i] = 0.0;
+      }
+      vg_axpby<double>(V, g.K, N, g.st);
+      if ((rc = cuda_check(cudaGraphLaunch(g.gexec, g.st), "grouped pc graph"))) break;
+      count_launch(1);
+      double *zj[P3D_GROUP_MAX];
+      for (int i = 0; i < g.K; i++) {
+        zj[i] = g.m[i]->Z + (size_t)j * N;
+        V.v[0][i] = g.m[i]->pc_out; V.v[1][i] = zj[i];
+      }
+      vg_axpby<double>(V, g.K, N, g.st);
+      if ((rc = g_stokes_op(g, zj, w))) break;
+      // classical Gram-Schmidt, first pass with |w|^2; second pass where needed
+      MGroup M;
+      memset(&M, 0, sizeof M);
+      for (int i = 0; i < g.K; i++) {
+        p3d_solver *s = g.m[i];
+        M.V[i] = s->Vptr; M.w[i] = w[i]; M.out[i] = s->hdev; M.self_out[i] = s->hdev + j + 1; M.part[i] = s->part;
+      }
+      vg_mdot(M, g.K, N, j + 1, g.st);
+      vg_maxpy(M, g.K, N, j + 1, -1.0, g.st);
+      for (int i = 0; i < g.K; i++)
+        if ((rc = cuda_check(cudaMemcpyAsync(g.m[i]->hhost, g.m[i]->hdev, (j + 2) * 8, cudaMemcpyDeviceToHost, g.st), "d2h")))
+          break;
+      if (rc) break;
+      if ((rc = cuda_check(cudaStreamSynchronize(g.st), "sync"))) break;
+      double hn[P3D_GROUP_MAX];
+      bool second[P3D_GROUP_MAX];
+      int nsecond = 0;
+      for (int i = 0; i < g.K; i++) {
+        MemberState &st = ms[act[i]];
+        double hh = 0.0;
+        for (int c = 0; c <= j; c++) {
+          st.H[(size_t)c * msize + j] = g.m[i]->hhost[c];
+          hh += g.m[i]->hhost[c] * g.m[i]->hhost[c];
+        }
+        const double wb2 = g.m[i]->hhost[j + 1];
+        second[i] = !(wb2 - hh > 0.5 * wb2);
+        if (!second[i]) hn[i] = std::sqrt(wb2 - hh);
+        nsecond += second[i];
+      }
+      if (nsecond) {
+        MGroup M2;
+        memset(&M2, 0, sizeof M2);
+        int K2 = 0;
+        double *w2[P3D_GROUP_MAX];
+        Group g2; // the members that need the second pass
+        g2.st = g.st;
+        for (int i = 0; i < g.K; i++)
+          if (second[i]) {
+            p3d_solver *s = g.m[i];
+            M2.V[K2] = s->Vptr; M2.w[K2] = w[i]; M2.out[K2] = s->hdev + s->hs; M2.part[K2] = s->part;
+            g2.m[K2] = s; w2[K2] = w[i];
+            K2++;
+          }
+        g2.K = K2;
+        vg_mdot(M2, K2, N, j + 1, g.st);
+        vg_maxpy(M2, K2, N, j + 1, -1.0, g.st);
+        for (int q = 0; q < K2; q++)
+          if ((rc = cuda_check(cudaMemcpyAsync(g2.m[q]->hhost + g2.m[q]->hs, g2.m[q]->hdev + g2.m[q]->hs, (j + 1) * 8,
+                                               cudaMemcpyDeviceToHost, g.st), "d2h")))
+            break;
+        if (rc) break;
+        double n2[P3D_GROUP_MAX];
+        if ((rc = g_norms2(g2, g2.m[0]->hs, w2, n2))) break; // synchronizes
+        for (int i = 0, q = 0; i < g.K; i++)
+          if (second[i]) {
+            MemberState &st = ms[act[i]];
+            for (int c = 0; c <= j; c++) st.H[(size_t)c * msize + j] += g.m[i]->hhost[g.m[i]->hs + c];
+            hn[i] = n2[q++];
+          }
+      }
+      // v_{j+1} = w / hn, Givens rotations, residual estimates
+      std::vector<int> fin; // members whose cycle ends here
+      for (int i = 0; i < g.K; i++) {
+        MemberState &st = ms[act[i]];
+        std::vector<double> &H = st.H;
+        H[(size_t)(j + 1) * msize + j] = hn[i];
+        V.v[0][i] = w[i]; V.v[1][i] = g.m[i]->V + (size_t)(j + 1) * N; V.s[0][i] = hn[i] > 0 ? 1.0 / hn[i] : 0.0;
+        V.s[1][i] = 0.0;
+        for (int c = 0; c < j; c++) {
+          const double a = H[(size_t)c * msize + j], b = H[(size_t)(c + 1) * msize + j];
+          H[(size_t)c * msize + j] = st.cs[c] * a + st.sn[c] * b;
+          H[(size_t)(c + 1) * msize + j] = -st.sn[c] * a + st.cs[c] * b;
+        }
+        const double a = H[(size_t)j * msize + j], b = H[(size_t)(j + 1) * msize + j];
+        const double rr = std::hypot(a, b);
+        st.cs[j] = rr > 0 ? a / rr : 1.0;
+        st.sn[j] = rr > 0 ? b / rr : 0.0;
+        H[(size_t)j * msize + j] = rr;
+        H[(size_t)(j + 1) * msize + j] = 0.0;
+        st.gv[j + 1] = -st.sn[j] * st.gv[j];
+        st.gv[j] = st.cs[j] * st.gv[j];
+        st.rnorm = std::fabs(st.gv[j + 1]);
+        st.its++;
+        if (!std::isfinite(st.rnorm)) {
+          st.status = set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual estimate");
+          fin.push_back(i);
+        } else if (st.rnorm <= st.tol || hn[i] == 0.0) {
+          st.conv = st.rnorm <= st.tol;
+          fin.push_back(i);
+        } else if (g.m[i]->cancel && g.m[i]->cancel->load(std::memory_order_relaxed)) {
+          st.status = P3D_ERR_CANCELLED; // keeps the iterate reached
+          fin.push_back(i);
+        }
+      }
+      vg_axpby<double>(V, g.K, N, g.st);
+      if (!fin.empty()) {
+        // finished members: x += Z y over their j + 1 directions, then they leave
+        // (a member that broke down keeps its iterate)
+        Group gf;
+        gf.st = g.st;
+        std::vector<MemberState> fs;
+        std::vector<int> upd;
+        for (int i : fin) {
+          if (ms[act[i]].status == P3D_OK || ms[act[i]].status == P3D_ERR_CANCELLED) upd.push_back(gf.K);
+          gf.m[gf.K++] = g.m[i];
+          fs.push_back(ms[act[i]]);
+        }
+        if ((rc = g_update_x(gf, upd, fs, j + 1, msize))) break;
+        for (int q = 0; q < (int)fin.size(); q++) {
+          ms[act[fin[q]]] = fs[q];
+          ms[act[fin[q]]].done = true;
+        }
+        std::vector<int> keep;
+        for (int i = 0; i < g.K; i++)
+          if (std::find(fin.begin(), fin.end(), i) == fin.end()) keep.push_back(act[i]);
+        act = keep;
+        if (act.empty()) { j++; its++; break; }
+        if ((rc = rebuild())) break;
+        for (int i = 0; i < g.K; i++) w[i] = g.m[i]->w;
+      }
+    }
+    if (rc) break;
+    if (act.empty()) break; // every member left during the cycle (its update is done)
+    // end of the cycle (restart or iteration limit): x += Z y for the rest
+    std::vector<int> idx;
+    for (int i = 0; i < g.K; i++) idx.push_back(i);
+    std::vector<MemberState> cur;
+    for (int i = 0; i < g.K; i++) cur.push_back(ms[act[i]]);
+    if ((rc = g_update_x(g, idx, cur, j, msize))) break;
+    for (int i = 0; i < g.K; i++) ms[act[i]] = cur[i];
+  }
+  g_release_graph(g);
+  return rc;
+}
+
+int solver_group_solve(p3d_solver *const *solvers, int K, double *const *u, double *const *p, p3d_solve_stats *stats,
+                       int *status)
+{
+  if (!solvers || !u || !p || K < 1 || K > P3D_GROUP_MAX) return set_error(P3D_ERR_ARG, "group solve: bad arguments");
+  p3d_solver *s0 = solvers[0];
+  for (int k = 0; k < K; k++) {
+    p3d_solver *s = solvers[k];
+    if (!s || !u[k] || !p[k]) return set_error(P3D_ERR_ARG, "group solve: null member %d", k);
+    if (!s->setup_done || !s->rhs_set) return set_error(P3D_ERR_STATE, "group solve: member %d before setup / rhs", k);
+    if (s->device != s0->device || s->mesh.mx != s0->mesh.mx || s->mesh.my != s0->mesh.my || s->mesh.mz != s0->mesh.mz ||
+        s->mesh.dirichlet != s0->mesh.dirichlet || s->o.nlevels != s0->o.nlevels || s->o.cheb_its != s0->o.cheb_its ||
+        s->o.mg_precision != s0->o.mg_precision || s->o.restart != s0->o.restart || s->o.max_it != s0->o.max_it ||
+        s->o.coarse_op != s0->o.coarse_op)
+      return set_error(P3D_ERR_ARG, "group solve: member %d differs in mesh or options", k);
+    if (s->o.inner_its > 0 || s->o.inner_rtol > 0.0 || s->lv.size() < 2)
+      return set_error(P3D_ERR_ARG, "group solve: members need one V-cycle per outer iteration and >= 2 levels");
+    for (int q = 0; q < k; q++)
+      if (solvers[q] == s) return set_error(P3D_ERR_ARG, "group solve: solver %d given twice", k);
+  }
+  cudaSetDevice(s0->device);
+  const double t0 = now_ms();
+  Group all;
+  all.K = K;
+  all.st = s0->st;
+  for (int k = 0; k < K; k++) all.m[k] = solvers[k];
+  // order the members' own streams before the group's
+  for (int k = 1; k < K; k++) CU(cudaStreamSynchronize(solvers[k]->st), "member sync");
+  for (int k = 0; k < K; k++) {
+    p3d_solver *s = solvers[k];
+    CU(cudaMemcpyAsync(s->xsol, u[k], s->nu * 8, cudaMemcpyDeviceToDevice, all.st), "x u");
+    CU(cudaMemcpyAsync(s->xsol + s->nu, p[k], s->np * 8, cudaMemcpyDeviceToDevice, all.st), "x p");
+  }
+  std::vector<MemberState> ms(K);
+  int rc = group_fgmres(all, ms);
+  // true residuals and the solutions out
+  if (!rc) {
+    double *x[P3D_GROUP_MAX], *w[P3D_GROUP_MAX];
+    for (int k = 0; k < K; k++) { x[k] = solvers[k]->xsol; w[k] = solvers[k]->w; }
+    rc = g_stokes_op(all, x, w);
+    if (!rc) {
+      VGroup<double> V;
+      memset(&V, 0, sizeof V);
+      for (int k = 0; k < K; k++) { V.v[0][k] = solvers[k]->bvec; V.v[1][k] = w[k]; V.v[2][k] = w[k]; }
+      vg_residual<double>(V, K, s0->N, all.st);
+      double rt[P3D_GROUP_MAX];
+      rc = g_norms2(all, s0->hs, w, rt);
+      for (int k = 0; !rc && k < K; k++) {
+        p3d_solver *s = solvers[k];
+        p3d_solve_stats &st = stats[k];
+        memset(&st, 0, sizeof st);
+        st.iterations = ms[k].its;
+        st.r0 = ms[k].r0;
+        st.rfinal = rt[k];
+        st.converged = ms[k].status == P3D_OK &&
+                       (ms[k].conv || rt[k] <= std::max(s->o.rtol * ms[k].r0, s->o.atol) * 1.0000001);
+        st.setup_ms = s->setup_ms;
+        st.lmax_fine = s->lv.back().lmax;
+        st.coarse_dofs = s->nc;
+        rc = cuda_check(cudaMemcpyAsync(u[k], s->xsol, s->nu * 8, cudaMemcpyDeviceToDevice, all.st), "u out");
+        if (!rc) rc = cuda_check(cudaMemcpyAsync(p[k], s->xsol + s->nu, s->np * 8, cudaMemcpyDeviceToDevice, all.st), "p out");
+      }
+      if (!rc) rc = cuda_check(cudaStreamSynchronize(all.st), "group solve sync");
+    }
+  }
+  const double dt = now_ms() - t0;
+  for (int k = 0; k < K; k++) stats[k].solve_ms = dt;
+  if (rc) return rc;
+  int worst = P3D_OK;
+  for (int k = 0; k < K; k++) {
+    const int sk = ms[k].status != P3D_OK ? ms[k].status : (stats[k].converged ? P3D_OK : P3D_ERR_NOCONV);
+    if (status) status[k] = sk;
+    if (sk != P3D_OK && (worst == P3D_OK || worst == P3D_ERR_NOCONV)) worst = sk;
+  }
+  return worst;
+}
+
+} // namespace p3d
+
+using namespace p3d;
+
+extern "C" {
+
+int p3d_solver_solve_grouped(p3d_solver *const solvers[], int32_t k, double *const u[], double *const p[],
+                             p3d_solve_stats stats[], int32_t status[])
+{
+  if (!solvers || !u || !p || !stats || k < 1 || k > P3D_GROUP_MAX)
+    return set_error(P3D_ERR_ARG, "solve_grouped: bad arguments");
+  for (int i = 0; i < k; i++)
+    if (!solvers[i]) return set_error(P3D_ERR_ARG, "solve_grouped: null solver %d", i);
+  cudaSetDevice(solvers[0]->device);
+  CK(order_after_caller());
+  return solver_group_solve(solvers, k, u, p, stats, status);
+}
+
+} // extern "C"
+
+namespace p3d {
 } // namespace p3d
 
 using namespace p3d;
@@ -914,6 +1495,7 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
   if (!rc) rc = dev_alloc((void **)&s->xsol, N * 8, "solution");
   s->hs = m + 1;
   if (!rc) rc = dev_alloc((void **)&s->Vptr, (size_t)(m + 2) * sizeof(double *), "V ptrs");
+  if (!rc) rc = dev_alloc((void **)&s->Zptr, (size_t)m * sizeof(double *), "Z ptrs");
   // partials of the multi-dot kernels, then their ticket counter (zero between launches)
   const size_t npart = (size_t)P3D_MDOT_BLOCKS * (P3D_MDOT_CHUNK + 1) + 2;
   if (!rc) rc = dev_alloc((void **)&s->part, npart * 8, "partials");
@@ -924,6 +1506,8 @@ int p3d_solver_create(const p3d_mesh_desc *mesh, const p3d_solver_opts *opts, in
     std::vector<double *> ptrs(m + 2, nullptr);
     for (int j = 0; j <= m; j++) ptrs[j] = s->V + (size_t)j * N;
     rc = cuda_check(cudaMemcpy(s->Vptr, ptrs.data(), (m + 2) * sizeof(double *), cudaMemcpyHostToDevice), "ptrs");
+    for (int j = 0; j < m; j++) ptrs[j] = s->Z + (size_t)j * N;
+    if (!rc) rc = cuda_check(cudaMemcpy(s->Zptr, ptrs.data(), m * sizeof(double *), cudaMemcpyHostToDevice), "ptrs");
   }
   // velocity-solve vectors (sized for FP64; the mixed path uses them as FP32)
   if (!rc) rc = dev_alloc(&s->cg_r, s->nu * 8, "cg r");
@@ -1095,7 +1679,7 @@ int p3d_solver_destroy(p3d_solver *s)
   if (s->graph) cudaGraphDestroy(s->graph);
   for (auto &L : s->lv) free_level(L);
   for (void *p : {(void *)s->cinv, (void *)s->cb64, (void *)s->cx64, (void *)s->gj, (void *)s->Binv, (void *)s->bvec, (void *)s->V,
-                  (void *)s->Z, (void *)s->w, (void *)s->Vptr, (void *)s->part, (void *)s->hdev, (void *)s->pc_in,
+                  (void *)s->Z, (void *)s->w, (void *)s->Vptr, (void *)s->Zptr, (void *)s->part, (void *)s->hdev, (void *)s->pc_in,
                   (void *)s->pc_out, (void *)s->pc_t, (void *)s->xsol, s->cg_r, s->cg_z, s->cg_p, s->cg_q, (void *)s->cg_ptr,
                   (void *)s->cg_sc})
     if (p) cudaFree(p);

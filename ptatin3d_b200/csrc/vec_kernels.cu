@@ -245,6 +245,293 @@ __global__ void k_dense_mv(int n, const double *__restrict__ M, const double *__
   if (lane == 0) y[row] = s;
 }
 
+// ------------------------------------------------------ grouped kernels ---
+// The same recurrences over the K members of a group of same-shape solves in
+// one launch (blockIdx.y = member).  Per-member pointers and scalars travel in
+// the launch parameters (VGroup), so a captured graph replays them as they are.
+
+template <typename T>
+__global__ void kg_cheb_init0(const __grid_constant__ VGroup<T> G, size_t n)
+{
+  const int m = blockIdx.y;
+  const double *dinv = G.dinv[m];
+  const T *b = G.v[0][m];
+  T *x = G.v[1][m], *r = G.v[2][m], *d = G.v[3][m];
+  const T inv_theta = (T)G.s[0][m];
+  GS_LOOP(i, n)
+  {
+    const T bi = b[i];
+    x[i] = (T)0;
+    r[i] = bi;
+    d[i] = (T)(dinv[i] * (double)bi) * inv_theta;
+  }
+}
+template <typename T>
+__global__ void kg_cheb_init_res(const __grid_constant__ VGroup<T> G, size_t n)
+{
+  const int m = blockIdx.y;
+  const double *dinv = G.dinv[m];
+  const T *b = G.v[0][m], *Ax = G.v[1][m];
+  T *r = G.v[2][m], *d = G.v[3][m];
+  const T inv_theta = (T)G.s[0][m];
+  GS_LOOP(i, n)
+  {
+    const T ri = b[i] - Ax[i];
+    r[i] = ri;
+    d[i] = (T)(dinv[i] * (double)ri) * inv_theta;
+  }
+}
+template <typename T>
+__global__ void kg_cheb_step(const __grid_constant__ VGroup<T> G, size_t n, int last)
+{
+  const int m = blockIdx.y;
+  const double *dinv = G.dinv[m];
+  T *x = G.v[0][m], *r = G.v[1][m], *d = G.v[3][m];
+  const T *Ad = G.v[2][m];
+  const T c1 = (T)G.s[0][m], c2 = (T)G.s[1][m];
+  GS_LOOP(i, n)
+  {
+    T di = d[i];
+    T ri = r[i] - Ad[i];
+    T dn = c1 * di + c2 * (T)(dinv[i] * (double)ri);
+    if (last) {
+      x[i] += di + dn;
+    } else {
+      x[i] += di;
+      r[i] = ri;
+      d[i] = dn;
+    }
+  }
+}
+// y = a x + b y (y is not read when b == 0, so it may hold anything)
+template <typename T>
+__global__ void kg_axpby(const __grid_constant__ VGroup<T> G, size_t n)
+{
+  const int m = blockIdx.y;
+  const T *x = G.v[0][m];
+  T *y = G.v[1][m];
+  const T a = (T)G.s[0][m], b = (T)G.s[1][m];
+  if (b == (T)0) {
+    GS_LOOP(i, n) y[i] = a * x[i];
+  } else {
+    GS_LOOP(i, n) y[i] = a * x[i] + b * y[i];
+  }
+}
+// r = b - Ax
+template <typename T>
+__global__ void kg_residual(const __grid_constant__ VGroup<T> G, size_t n)
+{
+  const int m = blockIdx.y;
+  const T *b = G.v[0][m], *Ax = G.v[1][m];
+  T *r = G.v[2][m];
+  GS_LOOP(i, n) r[i] = b[i] - Ax[i];
+}
+// precision conversion: v[1] = (B) v[0] (the roles hold raw pointers)
+template <typename A, typename B>
+__global__ void kg_convert(const __grid_constant__ VGroup<double> G, size_t n)
+{
+  const int m = blockIdx.y;
+  const A *x = reinterpret_cast<const A *>(G.v[0][m]);
+  B *y = reinterpret_cast<B *>(G.v[1][m]);
+  GS_LOOP(i, n) y[i] = (B)x[i];
+}
+// y = blockdiag(B_e) x with 4x4 blocks (v[0] = B, v[1] = x, v[2] = y)
+__global__ void kg_block4(const __grid_constant__ VGroup<double> G, size_t nel)
+{
+  const int m = blockIdx.y;
+  const double *B = G.v[0][m], *x = G.v[1][m];
+  double *y = G.v[2][m];
+  GS_LOOP(e, nel)
+  {
+    const double *b = B + 16 * e;
+    double x0 = x[4 * e], x1 = x[4 * e + 1], x2 = x[4 * e + 2], x3 = x[4 * e + 3];
+    for (int r = 0; r < 4; r++) y[4 * e + r] = b[4 * r] * x0 + b[4 * r + 1] * x1 + b[4 * r + 2] * x2 + b[4 * r + 3] * x3;
+  }
+}
+// y = M x, M dense n x n (v[0] = M, v[1] = x, v[2] = y); one warp per row
+__global__ void kg_dense_mv(const __grid_constant__ VGroup<double> G, int n)
+{
+  const int m = blockIdx.y;
+  const double *M = G.v[0][m], *x = G.v[1][m];
+  double *y = G.v[2][m];
+  int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int c = lane; c < n; c += 32) s += M[(size_t)row * n + c] * x[c];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) y[row] = s;
+}
+// partial dot products of KC basis vectors with w, per member (its own
+// partials buffer and ticket); the last block of a member finishes its sums
+template <int KC>
+__global__ void kg_mdot_partial(const __grid_constant__ MGroup G, size_t n, int j0)
+{
+  constexpr int KS = KC + 1;
+  __shared__ double red[32][KS];
+  __shared__ bool last;
+  const int mem = blockIdx.y;
+  const double *w = G.w[mem];
+  double *part = G.part[mem];
+  unsigned int *ticket = reinterpret_cast<unsigned int *>(part + (size_t)P3D_MDOT_BLOCKS * (P3D_MDOT_CHUNK + 1));
+  double *out = G.out[mem] + j0, *self_out = j0 == 0 ? G.self_out[mem] : nullptr;
+  const bool self = self_out != nullptr;
+  const int nout = KC + (self ? 1 : 0);
+  const double *v[KC];
+  double acc[KC], accs = 0.0;
+#pragma unroll
+  for (int j = 0; j < KC; j++) {
+    v[j] = G.V[mem][j0 + j];
+    acc[j] = 0.0;
+  }
+  GS_LOOP(i, n)
+  {
+    double wi = w[i];
+#pragma unroll
+    for (int j = 0; j < KC; j++) acc[j] += v[j][i] * wi;
+    if (self) accs += wi * wi;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < KS; j++) {
+    if (j == KC && !self) break;
+    double x = j < KC ? acc[j] : accs;
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[warp][j] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < nout) {
+    double x = 0.0;
+    for (int q = 0; q < nw; q++) x += red[q][threadIdx.x];
+    part[(size_t)blockIdx.x * KS + threadIdx.x] = x;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (warp < nout) {
+    double x = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(part + (size_t)b * KS + warp);
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) {
+      if (warp < KC) out[warp] = x;
+      else *self_out = x;
+    }
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+// w += sign * sum_j h_j V_j per member (h on the device)
+template <int KC>
+__global__ void kg_maxpy(const __grid_constant__ MGroup G, size_t n, int j0, double sign)
+{
+  const int mem = blockIdx.y;
+  double *w = G.w[mem];
+  const double *v[KC];
+  double c[KC];
+#pragma unroll
+  for (int j = 0; j < KC; j++) {
+    v[j] = G.V[mem][j0 + j];
+    c[j] = sign * G.out[mem][j0 + j];
+  }
+  GS_LOOP(i, n)
+  {
+    double s = w[i];
+#pragma unroll
+    for (int j = 0; j < KC; j++) s += c[j] * v[j][i];
+    w[i] = s;
+  }
+}
+
+template <typename T> void vg_cheb_init0(const VGroup<T> &G, int K, size_t n, cudaStream_t s)
+{
+  kg_cheb_init0<T><<<dim3(vgrid(n), K), 256, 0, s>>>(G, n);
+  count_launch(1);
+}
+template <typename T> void vg_cheb_init_res(const VGroup<T> &G, int K, size_t n, cudaStream_t s)
+{
+  kg_cheb_init_res<T><<<dim3(vgrid(n), K), 256, 0, s>>>(G, n);
+  count_launch(1);
+}
+template <typename T> void vg_cheb_step(const VGroup<T> &G, int K, size_t n, bool last, cudaStream_t s)
+{
+  kg_cheb_step<T><<<dim3(vgrid(n), K), 256, 0, s>>>(G, n, last ? 1 : 0);
+  count_launch(1);
+}
+template <typename T> void vg_axpby(const VGroup<T> &G, int K, size_t n, cudaStream_t s)
+{
+  kg_axpby<T><<<dim3(vgrid(n), K), 256, 0, s>>>(G, n);
+  count_launch(1);
+}
+template <typename T> void vg_residual(const VGroup<T> &G, int K, size_t n, cudaStream_t s)
+{
+  kg_residual<T><<<dim3(vgrid(n), K), 256, 0, s>>>(G, n);
+  count_launch(1);
+}
+template <typename A, typename B> void vg_convert(const VGroup<double> &G, int K, size_t n, cudaStream_t s)
+{
+  kg_convert<A, B><<<dim3(vgrid(n), K), 256, 0, s>>>(G, n);
+  count_launch(1);
+}
+void vg_block4(const VGroup<double> &G, int K, size_t nel, cudaStream_t s)
+{
+  kg_block4<<<dim3(vgrid(nel), K), 256, 0, s>>>(G, nel);
+  count_launch(1);
+}
+void vg_dense_mv(const VGroup<double> &G, int K, int n, cudaStream_t s)
+{
+  kg_dense_mv<<<dim3((n + 7) / 8, K), 256, 0, s>>>(G, n);
+  count_launch(1);
+}
+void vg_mdot(const MGroup &G, int K, size_t n, int k, cudaStream_t s)
+{
+  for (int j0 = 0; j0 < k; j0 += P3D_MDOT_CHUNK) {
+    const int kc = k - j0 < P3D_MDOT_CHUNK ? k - j0 : P3D_MDOT_CHUNK;
+    const dim3 grid(P3D_MDOT_BLOCKS, K);
+    switch (kc) {
+    case 1: kg_mdot_partial<1><<<grid, 256, 0, s>>>(G, n, j0); break;
+    case 2: kg_mdot_partial<2><<<grid, 256, 0, s>>>(G, n, j0); break;
+    case 3: kg_mdot_partial<3><<<grid, 256, 0, s>>>(G, n, j0); break;
+    case 4: kg_mdot_partial<4><<<grid, 256, 0, s>>>(G, n, j0); break;
+    case 5: kg_mdot_partial<5><<<grid, 256, 0, s>>>(G, n, j0); break;
+    case 6: kg_mdot_partial<6><<<grid, 256, 0, s>>>(G, n, j0); break;
+    case 7: kg_mdot_partial<7><<<grid, 256, 0, s>>>(G, n, j0); break;
+    default: kg_mdot_partial<8><<<grid, 256, 0, s>>>(G, n, j0); break;
+    }
+    count_launch(1);
+  }
+}
+void vg_maxpy(const MGroup &G, int K, size_t n, int k, double sign, cudaStream_t s)
+{
+  for (int j0 = 0; j0 < k; j0 += P3D_MDOT_CHUNK) {
+    const int kc = k - j0 < P3D_MDOT_CHUNK ? k - j0 : P3D_MDOT_CHUNK;
+    const dim3 grid(vgrid(n), K);
+    switch (kc) {
+    case 1: kg_maxpy<1><<<grid, 256, 0, s>>>(G, n, j0, sign); break;
+    case 2: kg_maxpy<2><<<grid, 256, 0, s>>>(G, n, j0, sign); break;
+    case 3: kg_maxpy<3><<<grid, 256, 0, s>>>(G, n, j0, sign); break;
+    case 4: kg_maxpy<4><<<grid, 256, 0, s>>>(G, n, j0, sign); break;
+    case 5: kg_maxpy<5><<<grid, 256, 0, s>>>(G, n, j0, sign); break;
+    case 6: kg_maxpy<6><<<grid, 256, 0, s>>>(G, n, j0, sign); break;
+    case 7: kg_maxpy<7><<<grid, 256, 0, s>>>(G, n, j0, sign); break;
+    default: kg_maxpy<8><<<grid, 256, 0, s>>>(G, n, j0, sign); break;
+    }
+    count_launch(1);
+  }
+}
+template void vg_cheb_init0<double>(const VGroup<double> &, int, size_t, cudaStream_t);
+template void vg_cheb_init0<float>(const VGroup<float> &, int, size_t, cudaStream_t);
+template void vg_cheb_init_res<double>(const VGroup<double> &, int, size_t, cudaStream_t);
+template void vg_cheb_init_res<float>(const VGroup<float> &, int, size_t, cudaStream_t);
+template void vg_cheb_step<double>(const VGroup<double> &, int, size_t, bool, cudaStream_t);
+template void vg_cheb_step<float>(const VGroup<float> &, int, size_t, bool, cudaStream_t);
+template void vg_axpby<double>(const VGroup<double> &, int, size_t, cudaStream_t);
+template void vg_axpby<float>(const VGroup<float> &, int, size_t, cudaStream_t);
+template void vg_residual<double>(const VGroup<double> &, int, size_t, cudaStream_t);
+template void vg_convert<double, float>(const VGroup<double> &, int, size_t, cudaStream_t);
+template void vg_convert<float, double>(const VGroup<double> &, int, size_t, cudaStream_t);
+
 // ------------------------------------------------------------ host API ---
 template <typename A, typename B> void v_convert(size_t n, const A *x, B *y, cudaStream_t s)
 {

@@ -113,3 +113,29 @@ class StokesSolver:
             self.destroy()
         except Exception:
             pass
+
+
+def solve_grouped(solvers, us=None, ps=None):
+    """Solve several StokesSolver objects of one mesh shape and option set
+    together (p3d_solver_solve_grouped): one launch per kernel for all of
+    them, each keeping its own Krylov iteration.  Returns [(u, p, stats,
+    status), ...] in the order given."""
+    k = len(solvers)
+    us = [None] * k if us is None else us
+    ps = [None] * k if ps is None else ps
+    U = [torch.zeros(S.nu, dtype=torch.float64, device=S.device) if u is None else S._dev(u, S.nu, "u")
+         for S, u in zip(solvers, us)]
+    P = [torch.zeros(S.np, dtype=torch.float64, device=S.device) if p is None else S._dev(p, S.np, "p")
+         for S, p in zip(solvers, ps)]
+    VP = C.c_void_p * k
+    stats = (SolveStats * k)()
+    status = (C.c_int32 * k)()
+    rc = lib().p3d_solver_solve_grouped(VP(*[S.h.value for S in solvers]), k, VP(*[u.data_ptr() for u in U]),
+                                        VP(*[p.data_ptr() for p in P]), C.cast(stats, C.c_void_p), status)
+    if rc not in (0, _lib.P3D_ERR_NOCONV, _lib.P3D_ERR_BREAKDOWN, _lib.P3D_ERR_CANCELLED):
+        check(rc)
+    out = []
+    for i in range(k):
+        st = {f: getattr(stats[i], f) for f, _ in SolveStats._fields_}
+        out.append((U[i], P[i], st, int(status[i])))
+    return out

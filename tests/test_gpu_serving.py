@@ -95,3 +95,29 @@ def test_bad_requests_raise(cuda):
             S.submit((4, 4, 4), BITS, np.zeros(3), np.zeros(27 * 64), np.zeros(27 * 64))
     with pytest.raises(P3DError):
         StokesServer(hbm_budget=0)
+
+
+def test_grouped_requests_match_their_solo_solves(cuda):
+    """Requests of one shape that queue together are admitted as one group and
+    solved with shared launches (lock-step FGMRES, p3d_solver_solve_grouped);
+    each result equals the same request solved on its own."""
+    reqs = [request(12, ns, 1e2, 30 + t) for t, ns in enumerate([1, 2, 3, 2, 1])]
+    alone = {}
+    with StokesServer(hbm_budget=8 << 30, max_active=1, group_max=1) as S:
+        for t, arr in enumerate(reqs):
+            submit(S, 12, arr, t, rtol=1e-11)
+            alone[t] = S.wait_all()[0]
+        assert S.stats()["grouped"] == 0
+    with StokesServer(hbm_budget=8 << 30, max_active=1, group_max=8) as S:
+        submit(S, 24, request(24, 2, 1e2, 9), 99)  # keeps the worker busy while the others queue
+        for t, arr in enumerate(reqs):
+            submit(S, 12, arr, 10 + t, rtol=1e-11)
+        res = {r["tag"]: r for r in S.wait_all()}
+        st = S.stats()
+    assert st["groups"] >= 1 and st["grouped"] >= 4, st
+    for t in range(len(reqs)):
+        r = res[10 + t]
+        assert r["ok"], r["status"]
+        assert abs(r["iterations"] - alone[t]["iterations"]) <= max(2, 0.05 * alone[t]["iterations"])
+        assert rel(r["u"], alone[t]["u"]) <= 1e-7
+        assert rel(r["p"], alone[t]["p"]) <= 1e-6

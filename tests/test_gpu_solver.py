@@ -370,3 +370,47 @@ def test_inner_tolerance_cap_ends_the_loop(cuda):
     _, _, st = S.solve()
     assert st["converged"]
     assert st["inner_iterations"] == 3 * st["iterations"]  # one preconditioner application per outer iteration
+
+
+@pytest.mark.parametrize("prec", [PREC_F64, PREC_F32])
+def test_grouped_solve_equals_member_solves(cuda, prec):
+    """Four solvers of one mesh shape with different sinkers solved together
+    (one launch per kernel for all four, lock-step FGMRES): each member takes
+    its own solve's iteration count and reaches its solution; a member whose
+    density holds a NaN breaks down alone, and an easy member leaves the group
+    early while the others go on."""
+    from ptatin3d_b200 import _lib
+    from ptatin3d_b200.solver import solve_grouped
+    m = 16
+    cases = [sinker(m, nsph=2, radius=0.15, contrast=1e2, seed=s) for s in (1, 2, 3)]
+    cases.append(sinker(m, nsph=1, radius=0.1, contrast=2.0, seed=4))  # converges much sooner
+    kw = dict(nlevels=3, rtol=1e-9, max_it=600, mg_precision=prec, schur_eta=SCHUR_ETA_GEOMEAN)
+    alone = []
+    for c, eta, rho in cases:
+        S = StokesSolver(m, m, m, BITS, **kw)
+        S.setup(c, eta)
+        S.set_rhs_body_force(rho)
+        u, p, st = S.solve()
+        alone.append((u.cpu().numpy(), p.cpu().numpy(), st))
+        S.destroy()
+    group = []
+    for c, eta, rho in cases:
+        S = StokesSolver(m, m, m, BITS, **kw)
+        S.setup(c, eta)
+        S.set_rhs_body_force(rho)
+        group.append(S)
+    c, eta, rho = cases[0]
+    bad = StokesSolver(m, m, m, BITS, **kw)
+    bad.setup(c, eta)
+    rho_nan = rho.copy()
+    rho_nan[40, 5] = np.nan
+    bad.set_rhs_body_force(rho_nan)
+    res = solve_grouped(group + [bad])
+    for (u, p, st, status), (ua, pa, sa) in zip(res[:4], alone):
+        assert status == 0 and st["converged"]
+        assert abs(st["iterations"] - sa["iterations"]) <= max(2, 0.05 * sa["iterations"])
+        assert rel(u.cpu().numpy(), ua) <= 1e-6 and rel(p.cpu().numpy(), pa) <= 1e-5
+    assert res[3][2]["iterations"] < res[0][2]["iterations"]
+    assert res[4][3] == _lib.P3D_ERR_BREAKDOWN
+    for S in group + [bad]:
+        S.destroy()
