@@ -431,6 +431,13 @@ int64_t p3d_kernel_launch_count(void);
  * further one fails with P3D_ERR_NOMEM, as an exhausted device would.  A
  * negative value switches the injection off (the default). */
 int p3d_debug_fail_allocations_after(int64_t after);
+/* Test aid for reads of memory nothing wrote: with fill in [0, 255] every
+ * device allocation of this library is filled with that byte before it is
+ * handed out (0xFF: every double and float reads as a NaN; 0x3F: as a
+ * finite value near 5e-4 / 0.75), so a result that depends on the former
+ * contents of reused memory shows up.  fill < 0 switches it off (the
+ * default). */
+int p3d_debug_poison_allocations(int32_t fill);
 /* Library version string. */
 const char *p3d_version(void);
 

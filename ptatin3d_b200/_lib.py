@@ -129,6 +129,7 @@ _SIGS = {
     "p3d_slab_add_plane": ([C.c_int, C.c_int32, C.c_int32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
                             C.c_void_p], C.c_int),
     "p3d_debug_fail_allocations_after": ([C.c_int64], C.c_int),
+    "p3d_debug_poison_allocations": ([C.c_int32], C.c_int),
     "p3d_mg_prolong": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_mg_restrict": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "p3d_marker_project_workspace": ([C.c_int32, C.c_int32, C.c_int32, C.c_int, C.POINTER(C.c_int64)], C.c_int),

@@ -281,6 +281,7 @@ static void free_dev(void *&p)
 
 // failure injection: allocations left before every device allocation fails (< 0: off)
 static std::atomic<long long> g_alloc_budget{-1};
+static std::atomic<int> g_alloc_poison{-1}; // fill byte of new allocations, -1: none
 
 int dev_alloc(void **p, size_t bytes, const char *what)
 {
@@ -295,6 +296,15 @@ int dev_alloc(void **p, size_t bytes, const char *what)
     *p = nullptr;
     cudaGetLastError();
     return set_error(P3D_ERR_NOMEM, "cudaMalloc(%zu) for %s: %s", bytes, what, cudaGetErrorString(e));
+  }
+  const int fill = g_alloc_poison.load();
+  if (fill >= 0) {
+    e = cudaMemset(*p, fill, bytes);
+    if (e != cudaSuccess) {
+      cudaFree(*p);
+      *p = nullptr;
+      return set_error(P3D_ERR_CUDA, "poisoning %s: %s", what, cudaGetErrorString(e));
+    }
   }
   return P3D_OK;
 }
@@ -429,6 +439,13 @@ const char *p3d_version(void) { return "p3d_b200 0.1 (sm_100a)"; }
 int p3d_debug_fail_allocations_after(int64_t after)
 {
   g_alloc_budget.store(after < 0 ? -1 : (long long)after);
+  return P3D_OK;
+}
+
+int p3d_debug_poison_allocations(int32_t fill)
+{
+  if (fill > 255) return set_error(P3D_ERR_ARG, "poison_allocations: fill byte %d out of range", fill);
+  g_alloc_poison.store(fill < 0 ? -1 : fill);
   return P3D_OK;
 }
 

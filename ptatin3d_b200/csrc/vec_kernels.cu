@@ -152,12 +152,14 @@ __global__ void k_mdot_partial(size_t n, const T *const *__restrict__ V, const T
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (warp < nout) {
+  // one warp per output; with KC = 8 and the self product there are nine
+  // outputs and only eight warps, so a warp may take a second one
+  for (int t = warp; t < nout; t += nw) {
     double x = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(part + (size_t)b * KS + warp);
+    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(part + (size_t)b * KS + t);
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
     if (lane == 0) {
-      if (warp < KC) out[warp] = x;
+      if (t < KC) out[t] = x;
       else *self_out = x;
     }
   }
@@ -411,12 +413,14 @@ __global__ void kg_mdot_partial(const __grid_constant__ MGroup G, size_t n, int 
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (warp < nout) {
+  // one warp per output; with KC = 8 and the self product there are nine
+  // outputs and only eight warps, so a warp may take a second one
+  for (int t = warp; t < nout; t += nw) {
     double x = 0.0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(part + (size_t)b * KS + warp);
+    for (int b = lane; b < (int)gridDim.x; b += 32) x += __ldcg(part + (size_t)b * KS + t);
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
     if (lane == 0) {
-      if (warp < KC) out[warp] = x;
+      if (t < KC) out[t] = x;
       else *self_out = x;
     }
   }

@@ -176,5 +176,5 @@ def test_device_solver_takes_the_reference_application_iteration_count(cuda):
     S.destroy()
     assert st["converged"]
     assert abs(st["r0"] - rec["outer_history"][0]) <= 5e-6 * rec["outer_history"][0]
-    assert abs(st["iterations"] - rec["outer_iterations"]) <= 3, st["iterations"]
+    assert abs(st["iterations"] - rec["outer_iterations"]) <= 3, st
     assert st["iterations"] <= st["inner_iterations"] <= 4 * st["iterations"]
