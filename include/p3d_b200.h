@@ -306,6 +306,8 @@ typedef struct p3d_solve_stats {
   int32_t coarse_dofs;
   int32_t inner_iterations; /* inner conjugate-gradient iterations of the solve
                                (tolerance-driven inner solves; 0 otherwise)      */
+  int32_t group_members;    /* most solves this one shared its launches with,
+                               itself included (1: solved alone)                 */
 } p3d_solve_stats;
 
 int p3d_solver_default_opts(p3d_solver_opts *opts);
@@ -393,16 +395,19 @@ typedef struct p3d_server_stats {
   int32_t active, queued;
   int64_t device_bytes, peak_device_bytes; /* estimated bytes held by pooled solvers */
   int32_t solvers_created, solvers_reused;
-  int64_t grouped;        /* requests solved in groups of two or more          */
-  int64_t groups;         /* such groups                                        */
+  int64_t grouped;        /* requests that shared launches with another one     */
+  int64_t groups;         /* rolling groups that had two or more members        */
 } p3d_server_stats;
 
 int p3d_server_create(int device, int64_t hbm_budget_bytes, int32_t max_active, p3d_server **server);
-/* Up to group_max (1..32, default 8) queued requests of one mesh shape and
- * option set are admitted together and solved as one group
- * (p3d_solver_solve_grouped: one launch per kernel for all of them); 1 solves
- * every request on its own.  Requests with an inner velocity solve or one
- * level are always solved alone. */
+/* Up to group_max (1..32, default 8) requests of one mesh shape and option
+ * set are solved as one rolling group (the lock-step solve of
+ * p3d_solver_solve_grouped: one launch per kernel for all of them).  Queued
+ * requests of the group's shape join it at the start of a restart cycle; a
+ * member leaves, and its result is posted, as soon as it converges, fails,
+ * is cancelled or reaches max_it, while the others go on.  1 solves every
+ * request on its own.  Requests with an inner velocity solve or one level are
+ * always solved alone. */
 int p3d_server_set_group_max(p3d_server *server, int32_t group_max);
 /* Non-blocking.  The request's host arrays must stay valid until its result
  * has been returned by p3d_server_poll. */

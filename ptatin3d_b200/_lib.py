@@ -76,7 +76,7 @@ class ServerStats(C.Structure):
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("converged", C.c_int32), ("r0", C.c_double), ("rfinal", C.c_double),
                 ("setup_ms", C.c_double), ("solve_ms", C.c_double), ("lmax_fine", C.c_double),
-                ("coarse_dofs", C.c_int32), ("inner_iterations", C.c_int32)]
+                ("coarse_dofs", C.c_int32), ("inner_iterations", C.c_int32), ("group_members", C.c_int32)]
 
 
 _lib = None

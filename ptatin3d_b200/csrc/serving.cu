@@ -2,13 +2,17 @@
 //
 // Requests (a whole mesh, coefficients, density, gravity, solver options)
 // arrive with p3d_server_submit and are admitted first-in first-out as soon
-// as a worker and the HBM they need are free.  The worker also takes the
-// queued requests of the head's shape and options that fit (up to
-// group_max) and solves them as one group: lock-step FGMRES with every kernel
-// launched once for all members (p3d_solver_solve_grouped).  Each of the
-// `max_active` workers runs on its own CUDA streams, with all of its solves'
-// state (hierarchy, Krylov bases, captured preconditioner graph) resident in
-// device memory; groups admitted together overlap on the device.  Finished solvers go back to a pool keyed by mesh and options, so a
+// as a worker and the HBM they need are free.  A worker solves its request in
+// a rolling group (solver_group_run): lock-step FGMRES with every kernel
+// launched once for all members.  The group starts with the queued requests
+// of the head's shape and options that fit (up to group_max); at the start of
+// every restart cycle queued requests of that shape join it, and a member
+// leaves -- its solution copied out and its result posted -- as soon as it
+// converges, fails, is cancelled or reaches max_it, while the others go on.
+// Each of the `max_active` workers runs on its own CUDA streams, with all of
+// its solves' state (hierarchy, Krylov bases, captured preconditioner graph)
+// resident in device memory; the groups of different workers overlap on the
+// device.  Finished solvers go back to a pool keyed by mesh and options, so a
 // later request of the same shape reuses the device memory and only uploads
 // new coefficients (no cudaMalloc/cudaFree on the hot path).  Idle pooled
 // solvers are released, least recently used first, when a request needs
@@ -19,10 +23,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -142,46 +148,20 @@ static bool groupable(const p3d_request &r)
   return r.opts.inner_its == 0 && r.opts.inner_rtol == 0.0 && r.opts.nlevels >= 2 && r.opts.use_graph;
 }
 
-// the solves of several requests of one shape in slots s[0..K): set-up of
-// each, then one grouped solve (p3d_solver_solve_grouped); status per member
-static void run_group(Slot *const *s, const p3d_request *const *r, int K, p3d_result *res,
-                      const std::atomic<int> *const *cancel, int *status)
+static bool same_group(const p3d_request &a, const p3d_request &b)
 {
-  p3d_solver *sol[P3D_GROUP_MAX];
-  double *u[P3D_GROUP_MAX], *p[P3D_GROUP_MAX];
-  int idx[P3D_GROUP_MAX], n = 0;
-  for (int k = 0; k < K; k++) {
-    status[k] = prepare_request(s[k], *r[k]);
-    res[k].iterations = 0;
-    res[k].rel_residual = 0.0;
-    if (!status[k] && cancel[k]->load()) status[k] = P3D_ERR_CANCELLED;
-    if (status[k]) continue;
-    sol[n] = s[k]->solver; u[n] = s[k]->u; p[n] = s[k]->p; idx[n] = k;
-    solver_set_cancel_flag(s[k]->solver, cancel[k]);
-    n++;
-  }
-  if (!n) return;
-  p3d_solve_stats st[P3D_GROUP_MAX];
-  int ms[P3D_GROUP_MAX];
-  memset(st, 0, sizeof st);
-  const int rc = n == 1 ? solver_solve_nowait(sol[0], u[0], p[0], &st[0])
-                        : solver_group_solve(sol, n, u, p, st, ms);
-  if (n == 1) ms[0] = rc;
-  for (int q = 0; q < n; q++) {
-    const int k = idx[q];
-    solver_set_cancel_flag(s[k]->solver, nullptr);
-    int sk = (n > 1 && rc != P3D_OK && rc != P3D_ERR_NOCONV && rc != P3D_ERR_BREAKDOWN && rc != P3D_ERR_CANCELLED)
-                 ? rc
-                 : ms[q];
-    if (sk == P3D_OK || sk == P3D_ERR_NOCONV || sk == P3D_ERR_CANCELLED) {
-      const int fr = finish_request(s[k], *r[k]);
-      if (fr) sk = fr;
-    }
-    status[k] = sk;
-    res[k].iterations = st[q].iterations;
-    res[k].rel_residual = st[q].r0 > 0 ? st[q].rfinal / st[q].r0 : 0.0;
-  }
+  return groupable(a) && groupable(b) && a.mx == b.mx && a.my == b.my && a.mz == b.mz && a.dirichlet == b.dirichlet &&
+         same_opts(a.opts, b.opts);
 }
+
+// an admitted request in the hands of a worker
+struct Job {
+  Pending pend;
+  Slot *slot = nullptr;
+  bool fresh = false;
+  double t_admit = 0.0;
+  std::atomic<int> cancel{0};
+};
 
 } // namespace p3d
 
@@ -245,11 +225,97 @@ static Slot *admit_request(p3d_server *S, const p3d_request &r, std::vector<Slot
   return s;
 }
 
+// Under the lock: the request leaves the queue for a worker (slot chosen)
+static Job *take_job(p3d_server *S, std::deque<std::unique_ptr<Job>> &jobs, const Pending &pend, Slot *slot, bool fresh)
+{
+  jobs.push_back(std::make_unique<Job>());
+  Job *jb = jobs.back().get();
+  jb->pend = pend;
+  jb->slot = slot;
+  jb->fresh = fresh;
+  jb->t_admit = wall_ms();
+  slot->busy = true;
+  S->active++;
+  S->st.admitted++;
+  if (fresh) S->st.solvers_created++;
+  else S->st.solvers_reused++;
+  S->running.emplace_back(pend.req.tag, &jb->cancel);
+  return jb;
+}
+
+// Under the lock: the job's result is posted and its slot goes back to the pool
+static void post_job(p3d_server *S, Job *jb, int status, int iterations, double rel_residual)
+{
+  p3d_result res;
+  memset(&res, 0, sizeof res);
+  const double t = wall_ms();
+  res.tag = jb->pend.req.tag;
+  res.status = status;
+  res.iterations = iterations;
+  res.rel_residual = rel_residual;
+  res.wait_ms = jb->t_admit - jb->pend.t_submit;
+  res.run_ms = t - jb->t_admit;
+  res.latency_ms = t - jb->pend.t_submit;
+  for (auto it = S->running.begin(); it != S->running.end(); ++it)
+    if (it->second == &jb->cancel) { S->running.erase(it); break; }
+  Slot *sl = jb->slot;
+  sl->busy = false;
+  sl->last_used = ++S->clock;
+  if (!sl->ready) { // creation failed: give the memory back
+    S->bytes -= sl->bytes;
+    S->slots.erase(std::find(S->slots.begin(), S->slots.end(), sl));
+    delete sl;
+  }
+  jb->slot = nullptr;
+  S->active--;
+  S->done.push_back(res);
+  S->st.completed++;
+  S->cv_done.notify_all();
+  S->cv_work.notify_all();
+}
+
+// Outside the lock: the job's slot created (if new) and its request set up;
+// a cancelled job is not set up
+static int start_job(p3d_server *S, Job *jb)
+{
+  int rc = jb->fresh ? create_slot(jb->slot, S->device) : P3D_OK;
+  if (!rc) rc = prepare_request(jb->slot, jb->pend.req);
+  if (!rc && jb->cancel.load()) rc = P3D_ERR_CANCELLED;
+  return rc;
+}
+
+// Under the lock: queued requests that can join a group of `ref`'s shape
+// (slots and memory permitting), up to `room`
+static int gather(p3d_server *S, const p3d_request &ref, int room, std::deque<std::unique_ptr<Job>> &jobs,
+                  std::vector<Job *> &got, std::vector<Slot *> &evict)
+{
+  int n = 0;
+  for (auto it = S->queue.begin(); it != S->queue.end() && n < room;) {
+    if (!same_group(it->req, ref)) {
+      ++it;
+      continue;
+    }
+    bool f = false, big = false;
+    Slot *sl = admit_request(S, it->req, evict, f, big);
+    if (!sl) break; // no slot or memory for more now
+    got.push_back(take_job(S, jobs, *it, sl, f));
+    it = S->queue.erase(it);
+    n++;
+  }
+  return n;
+}
+
 static void worker(p3d_server *S)
 {
   cudaSetDevice(S->device);
   std::unique_lock<std::mutex> lk(S->mu);
+  std::deque<std::unique_ptr<Job>> jobs; // this worker's jobs (stable addresses for the cancel flags)
+  auto release = [&](std::vector<Slot *> &evict) {
+    for (Slot *e : evict) { release_slot(e); delete e; }
+    evict.clear();
+  };
   for (;;) {
+    jobs.clear();
     if (S->queue.empty()) {
       if (S->stopping) return;
       S->cv_work.wait(lk);
@@ -261,115 +327,103 @@ static void worker(p3d_server *S)
     if (!slot && !too_big) {
       if (!evict.empty()) { // memory was given back: release it and look again
         lk.unlock();
-        for (Slot *e : evict) { release_slot(e); delete e; }
+        release(evict);
         lk.lock();
         continue;
       }
       S->cv_work.wait(lk);
       continue;
     }
-    Pending job = S->queue.front();
+    Pending head = S->queue.front();
     S->queue.pop_front();
-    p3d_result res;
-    memset(&res, 0, sizeof res);
-    res.tag = job.req.tag;
-    const double t_admit = wall_ms();
-    res.wait_ms = t_admit - job.t_submit;
     if (too_big) {
+      p3d_result res;
+      memset(&res, 0, sizeof res);
+      res.tag = head.req.tag;
       res.status = P3D_ERR_NOMEM;
-      res.latency_ms = res.wait_ms;
+      res.wait_ms = res.latency_ms = wall_ms() - head.t_submit;
       S->done.push_back(res);
       S->st.completed++;
       S->cv_done.notify_all();
       continue;
     }
-    // the head, and queued requests of its shape that fit, form a group
-    Slot *gs[P3D_GROUP_MAX];
-    Pending gj[P3D_GROUP_MAX];
-    bool gfresh[P3D_GROUP_MAX];
-    int K = 0;
-    gs[K] = slot; gj[K] = job; gfresh[K] = fresh; K++;
-    slot->busy = true;
-    if (groupable(job.req))
-      for (auto it = S->queue.begin(); it != S->queue.end() && K < std::min(S->group_max, P3D_GROUP_MAX);) {
-        if (!(groupable(it->req) && it->req.mx == job.req.mx && it->req.my == job.req.my && it->req.mz == job.req.mz &&
-              it->req.dirichlet == job.req.dirichlet && same_opts(it->req.opts, job.req.opts))) {
-          ++it;
-          continue;
-        }
-        bool f2 = false, big2 = false;
-        Slot *s2 = admit_request(S, it->req, evict, f2, big2);
-        if (!s2) break; // no slot or memory for more now
-        s2->busy = true;
-        gs[K] = s2; gj[K] = *it; gfresh[K] = f2; K++;
-        it = S->queue.erase(it);
-      }
-    std::atomic<int> cflag[P3D_GROUP_MAX];
-    for (int k = 0; k < K; k++) {
-      cflag[k].store(0);
-      S->active++;
-      S->st.admitted++;
-      if (gfresh[k]) S->st.solvers_created++;
-      else S->st.solvers_reused++;
-      S->running.emplace_back(gj[k].req.tag, &cflag[k]);
-    }
+    Job *first = take_job(S, jobs, head, slot, fresh);
+    const int gmax = std::min(S->group_max, P3D_GROUP_MAX);
+    std::vector<Job *> batch{first};
+    if (gmax > 1 && groupable(head.req)) gather(S, head.req, gmax - 1, jobs, batch, evict);
     S->cv_work.notify_all(); // the next request may fit as well
     lk.unlock();
-    for (Slot *e : evict) { release_slot(e); delete e; }
-    p3d_result gres[P3D_GROUP_MAX];
-    int gst[P3D_GROUP_MAX];
-    const p3d_request *greq[P3D_GROUP_MAX];
-    const std::atomic<int> *gcan[P3D_GROUP_MAX];
-    Slot *run_s[P3D_GROUP_MAX];
-    const p3d_request *run_r[P3D_GROUP_MAX];
-    const std::atomic<int> *run_c[P3D_GROUP_MAX];
-    int run_i[P3D_GROUP_MAX], nrun = 0;
-    for (int k = 0; k < K; k++) {
-      memset(&gres[k], 0, sizeof gres[k]);
-      gres[k].tag = gj[k].req.tag;
-      gres[k].wait_ms = (k == 0 ? t_admit : wall_ms()) - gj[k].t_submit;
-      greq[k] = &gj[k].req;
-      gcan[k] = &cflag[k];
-      gst[k] = gfresh[k] ? create_slot(gs[k], S->device) : P3D_OK;
-      if (!gst[k]) { run_s[nrun] = gs[k]; run_r[nrun] = greq[k]; run_c[nrun] = gcan[k]; run_i[nrun] = k; nrun++; }
-    }
-    if (nrun > 1) {
-      std::lock_guard<std::mutex> g2(S->mu);
-      S->st.grouped += nrun;
-      S->st.groups++;
-    }
-    if (nrun) {
-      p3d_result rr[P3D_GROUP_MAX];
-      int rs[P3D_GROUP_MAX];
-      run_group(run_s, run_r, nrun, rr, run_c, rs);
-      for (int q = 0; q < nrun; q++) {
-        gst[run_i[q]] = rs[q];
-        gres[run_i[q]].iterations = rr[q].iterations;
-        gres[run_i[q]].rel_residual = rr[q].rel_residual;
+    release(evict);
+    if (gmax == 1 || !groupable(head.req)) {
+      // solved alone
+      p3d_solve_stats st;
+      memset(&st, 0, sizeof st);
+      int rc = start_job(S, first);
+      if (!rc) {
+        solver_set_cancel_flag(first->slot->solver, &first->cancel);
+        rc = solver_solve_nowait(first->slot->solver, first->slot->u, first->slot->p, &st);
+        solver_set_cancel_flag(first->slot->solver, nullptr);
+        if (rc == P3D_OK || rc == P3D_ERR_NOCONV || rc == P3D_ERR_CANCELLED) {
+          const int fr = finish_request(first->slot, first->pend.req);
+          if (fr) rc = fr;
+        }
       }
+      lk.lock();
+      post_job(S, first, rc, st.iterations, st.r0 > 0 ? st.rfinal / st.r0 : 0.0);
+      continue;
     }
-    const double t_end = wall_ms();
+    // a rolling group: members set up here; later arrivals of the shape join
+    // at restart boundaries; each member is posted when it leaves
+    bool shared = false;
+    auto ready_members = [&](const std::vector<Job *> &js, GroupMember *out) -> int {
+      int n = 0;
+      for (Job *jb : js) {
+        const int rc = start_job(S, jb);
+        if (rc) {
+          std::lock_guard<std::mutex> g(S->mu);
+          post_job(S, jb, rc, 0, 0.0);
+          continue;
+        }
+        solver_set_cancel_flag(jb->slot->solver, &jb->cancel);
+        out[n].solver = jb->slot->solver;
+        out[n].u = jb->slot->u;
+        out[n].p = jb->slot->p;
+        out[n].tag = jb;
+        n++;
+      }
+      return n;
+    };
+    GroupHooks hooks;
+    hooks.admit = [&](int room, GroupMember *add) -> int {
+      std::vector<Job *> got;
+      std::vector<Slot *> ev;
+      {
+        std::lock_guard<std::mutex> g(S->mu);
+        gather(S, head.req, room, jobs, got, ev);
+      }
+      release(ev);
+      return got.empty() ? 0 : ready_members(got, add);
+    };
+    hooks.leave = [&](const GroupMember &m, int status, const p3d_solve_stats &st) {
+      Job *jb = static_cast<Job *>(m.tag);
+      solver_set_cancel_flag(jb->slot->solver, nullptr);
+      int sk = status;
+      if (sk == P3D_OK || sk == P3D_ERR_NOCONV || sk == P3D_ERR_CANCELLED) {
+        const int fr = finish_request(jb->slot, jb->pend.req);
+        if (fr) sk = fr;
+      }
+      std::lock_guard<std::mutex> g(S->mu);
+      if (st.group_members > 1) {
+        S->st.grouped++;
+        if (!shared) S->st.groups++; // counted before the first shared result is posted
+        shared = true;
+      }
+      post_job(S, jb, sk, st.iterations, st.r0 > 0 ? st.rfinal / st.r0 : 0.0);
+    };
+    GroupMember mem[P3D_GROUP_MAX];
+    const int n = ready_members(batch, mem);
+    if (n) solver_group_run(mem, n, gmax, hooks);
     lk.lock();
-    for (int k = 0; k < K; k++) {
-      gres[k].status = gst[k];
-      gres[k].run_ms = t_end - t_admit;
-      gres[k].latency_ms = t_end - gj[k].t_submit;
-      for (auto it = S->running.begin(); it != S->running.end(); ++it)
-        if (it->second == &cflag[k]) { S->running.erase(it); break; }
-      Slot *sl = gs[k];
-      sl->busy = false;
-      sl->last_used = ++S->clock;
-      if (!sl->ready) { // creation failed: give the memory back
-        S->bytes -= sl->bytes;
-        S->slots.erase(std::find(S->slots.begin(), S->slots.end(), sl));
-        delete sl;
-      }
-      S->active--;
-      S->done.push_back(gres[k]);
-      S->st.completed++;
-    }
-    S->cv_done.notify_all();
-    S->cv_work.notify_all();
   }
 }
 

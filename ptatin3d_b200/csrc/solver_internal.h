@@ -4,6 +4,7 @@
 #include <stddef.h>
 
 #include <atomic>
+#include <functional>
 #include <stdint.h>
 
 #ifndef P3D_GROUP_MAX
@@ -126,6 +127,28 @@ void solver_set_cancel_flag(p3d_solver *s, const std::atomic<int> *flag);
 // nullptr) per member: P3D_OK, P3D_ERR_NOCONV, _BREAKDOWN or _CANCELLED.
 int solver_group_solve(p3d_solver *const *solvers, int K, double *const *u, double *const *p,
                        struct p3d_solve_stats *stats, int *status);
+// A rolling group: members join at the start of a restart cycle and leave as
+// soon as they finish, the others going on.  A member is a solver (set up,
+// right-hand side set) with device arrays u, p (initial guess in, solution
+// out) and a caller's tag.
+struct GroupMember {
+  p3d_solver *solver = nullptr;
+  double *u = nullptr, *p = nullptr;
+  void *tag = nullptr;
+};
+struct GroupHooks {
+  // start of every restart cycle: writes up to `room` new members to `add`
+  // and returns their count (nullptr: no one joins)
+  std::function<int(int room, GroupMember *add)> admit;
+  // a member left (its u, p written; stats filled): P3D_OK, P3D_ERR_NOCONV,
+  // _BREAKDOWN, _CANCELLED, or P3D_ERR_ARG when it could not join
+  std::function<void(const GroupMember &m, int status, const struct p3d_solve_stats &st)> leave;
+};
+// runs until no member is left and none joins; the members' solvers must
+// share the mesh and options (checked; a mismatching joiner leaves with
+// P3D_ERR_ARG).  Returns P3D_OK or a CUDA failure (after which every member
+// still in the group has left with that status).
+int solver_group_run(const GroupMember *first, int K, int max_members, GroupHooks &hooks);
 
 // dense_inverse.cu (coarse-grid operator, in place, blocked Gauss-Jordan)
 size_t dense_inverse_scratch(int n);

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "p3d_b200.h"
@@ -1032,67 +1033,190 @@ static int g_norms2(Group &g, int slot, double *const *v, double *out)
 }
 
 struct MemberState {
+  GroupMember m;
   std::vector<double> H, cs, sn, gv, y;
-  double r0 = -1.0, tol = 0.0, rnorm = 0.0;
-  int its = 0;
-  bool conv = false, done = false;
+  double r0 = -1.0, tol = 0.0, rnorm = 0.0, t_join = 0.0;
+  int its = 0, gmax = 1; // gmax: the largest membership seen
+  bool conv = false;
   int status = P3D_OK;
 };
 
-// x += sum_{i<j} y_i Z_i for the members listed (coefficients uploaded to hdev)
-static int g_update_x(Group &g, const std::vector<int> &idx, std::vector<MemberState> &ms, int j, int msize)
+// why solver s cannot share a group with ref (nullptr: it can)
+static const char *group_mismatch(const p3d_solver *ref, const p3d_solver *s)
 {
-  if (idx.empty() || j == 0) return P3D_OK;
+  if (s->device != ref->device || s->mesh.mx != ref->mesh.mx || s->mesh.my != ref->mesh.my ||
+      s->mesh.mz != ref->mesh.mz || s->mesh.dirichlet != ref->mesh.dirichlet)
+    return "differs in device or mesh";
+  if (s->o.nlevels != ref->o.nlevels || s->o.cheb_its != ref->o.cheb_its || s->o.mg_precision != ref->o.mg_precision ||
+      s->o.restart != ref->o.restart || s->o.max_it != ref->o.max_it || s->o.coarse_op != ref->o.coarse_op)
+    return "differs in solver options";
+  if (s->o.inner_its > 0 || s->o.inner_rtol > 0.0 || s->lv.size() < 2)
+    return "needs one V-cycle per outer iteration and >= 2 levels";
+  if (!s->setup_done || !s->rhs_set) return "not set up or without right-hand side";
+  return nullptr;
+}
+
+// x += sum_{i<j} y_i Z_i for the members given (coefficients uploaded to hdev)
+static int g_update_x(cudaStream_t st, const std::vector<MemberState *> &mem, int j, int msize)
+{
+  if (mem.empty() || j == 0) return P3D_OK;
   MGroup M;
   memset(&M, 0, sizeof M);
   int K = 0;
-  for (int k : idx) {
-    p3d_solver *s = g.m[k];
-    MemberState &st = ms[k];
+  for (MemberState *q : mem) {
+    p3d_solver *s = q->m.solver;
     for (int i = j - 1; i >= 0; i--) {
-      double acc = st.gv[i];
-      for (int c = i + 1; c < j; c++) acc -= st.H[(size_t)i * msize + c] * st.y[c];
-      st.y[i] = acc / st.H[(size_t)i * msize + i];
+      double acc = q->gv[i];
+      for (int c = i + 1; c < j; c++) acc -= q->H[(size_t)i * msize + c] * q->y[c];
+      q->y[i] = acc / q->H[(size_t)i * msize + i];
     }
-    CU(cudaMemcpyAsync(s->hdev, st.y.data(), j * 8, cudaMemcpyHostToDevice, g.st), "h2d y");
+    CU(cudaMemcpyAsync(s->hdev, q->y.data(), j * 8, cudaMemcpyHostToDevice, st), "h2d y");
     M.V[K] = s->Zptr;
     M.w[K] = s->xsol;
     M.out[K] = s->hdev;
     K++;
   }
-  vg_maxpy(M, K, g.m[0]->N, j, 1.0, g.st);
-  return cuda_check(cudaStreamSynchronize(g.st), "x update"); // y (host) must outlive the copy
+  vg_maxpy(M, K, mem[0]->m.solver->N, j, 1.0, st);
+  return cuda_check(cudaStreamSynchronize(st), "x update"); // y (host) must outlive the copy
 }
 
-// lock-step FGMRES(m) of the members; their xsol hold the initial guesses
-static int group_fgmres(Group &all, std::vector<MemberState> &ms)
+// members leaving: true residual |b - A x|, solution to (u, p), stats, hook
+static int g_leave(cudaStream_t st, const std::vector<MemberState *> &out, GroupHooks &hooks)
 {
-  const int msize = all.m[0]->o.restart, max_it = all.m[0]->o.max_it;
-  const size_t N = all.m[0]->N;
-  for (int k = 0; k < all.K; k++) {
-    ms[k].H.assign((size_t)(msize + 1) * msize, 0.0);
-    ms[k].cs.assign(msize, 0.0); ms[k].sn.assign(msize, 0.0);
-    ms[k].gv.assign(msize + 1, 0.0); ms[k].y.assign(msize, 0.0);
-    // the scratch slot of the basis pointers names the member's w (norms)
-    double *w = all.m[k]->w;
-    CU(cudaMemcpyAsync(all.m[k]->Vptr + all.m[k]->hs, &w, sizeof(double *), cudaMemcpyHostToDevice, all.st), "ptr");
+  if (out.empty()) return P3D_OK;
+  Group gl;
+  gl.st = st;
+  double *x[P3D_GROUP_MAX], *w[P3D_GROUP_MAX];
+  for (MemberState *q : out) {
+    gl.m[gl.K] = q->m.solver;
+    x[gl.K] = q->m.solver->xsol;
+    w[gl.K] = q->m.solver->w;
+    gl.K++;
   }
-  CU(cudaStreamSynchronize(all.st), "sync");
-  std::vector<int> act; // indices into all.m of the members still solving
-  for (int k = 0; k < all.K; k++) act.push_back(k);
-  int rc = P3D_OK;
+  const size_t N = gl.m[0]->N;
+  CK(g_stokes_op(gl, x, w));
+  VGroup<double> V;
+  memset(&V, 0, sizeof V);
+  for (int k = 0; k < gl.K; k++) { V.v[0][k] = gl.m[k]->bvec; V.v[1][k] = w[k]; V.v[2][k] = w[k]; }
+  vg_residual<double>(V, gl.K, N, st);
+  double rt[P3D_GROUP_MAX];
+  CK(g_norms2(gl, gl.m[0]->hs, w, rt));
+  for (int k = 0; k < gl.K; k++) {
+    p3d_solver *s = gl.m[k];
+    CU(cudaMemcpyAsync(out[k]->m.u, s->xsol, s->nu * 8, cudaMemcpyDeviceToDevice, st), "u out");
+    CU(cudaMemcpyAsync(out[k]->m.p, s->xsol + s->nu, s->np * 8, cudaMemcpyDeviceToDevice, st), "p out");
+  }
+  CU(cudaStreamSynchronize(st), "member out");
+  const double t = now_ms();
+  for (int k = 0; k < gl.K; k++) {
+    p3d_solver *s = gl.m[k];
+    MemberState &q = *out[k];
+    p3d_solve_stats ss;
+    memset(&ss, 0, sizeof ss);
+    ss.iterations = q.its;
+    ss.r0 = q.r0;
+    ss.rfinal = rt[k];
+    ss.converged = q.status == P3D_OK && (q.conv || rt[k] <= std::max(s->o.rtol * q.r0, s->o.atol) * 1.0000001);
+    ss.setup_ms = s->setup_ms;
+    ss.solve_ms = t - q.t_join;
+    ss.lmax_fine = s->lv.back().lmax;
+    ss.coarse_dofs = s->nc;
+    ss.group_members = q.gmax;
+    const int sk = q.status != P3D_OK ? q.status : (ss.converged ? P3D_OK : P3D_ERR_NOCONV);
+    if (hooks.leave) hooks.leave(q.m, sk, ss);
+  }
+  return P3D_OK;
+}
+
+int solver_group_run(const GroupMember *first, int K0, int max_members, GroupHooks &hooks)
+{
+  if (!first || K0 < 1 || K0 > P3D_GROUP_MAX || !first[0].solver)
+    return set_error(P3D_ERR_ARG, "group run: bad arguments");
+  max_members = std::max(1, std::min(max_members, P3D_GROUP_MAX));
+  const p3d_solver *ref = first[0].solver;
+  const int msize = ref->o.restart, max_it = ref->o.max_it;
+  const size_t N = ref->N;
+  cudaSetDevice(ref->device);
+  cudaStream_t st = nullptr;
+  CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "group stream");
+  std::vector<std::unique_ptr<MemberState>> act; // members in the group's order
   Group g;
-  g.st = all.st;
+  g.st = st;
+  bool dirty = true;
   auto rebuild = [&]() -> int {
     g_release_graph(g);
     g.K = (int)act.size();
-    for (int i = 0; i < g.K; i++) g.m[i] = all.m[act[i]];
-    if (!g.K) return P3D_OK;
-    return g_capture(g);
+    for (int i = 0; i < g.K; i++) {
+      g.m[i] = act[i]->m.solver;
+      act[i]->gmax = std::max(act[i]->gmax, g.K);
+    }
+    dirty = false;
+    return g.K ? g_capture(g) : P3D_OK;
   };
-  int its = 0;
-  if ((rc = rebuild())) return rc;
-  while (!act.empty() && its < max_it) {
+  p3d_solve_stats none;
+  memset(&none, 0, sizeof none);
+  auto join = [&](const GroupMember &gm) -> int {
+    const char *why = gm.solver && gm.u && gm.p ? group_mismatch(ref, gm.solver) : "null member";
+    if (!why)
+      for (auto &q : act)
+        if (q->m.solver == gm.solver) why = "solver already in the group";
+    if (why) {
+      set_error(P3D_ERR_ARG, "group member: %s", why);
+      if (hooks.leave) hooks.leave(gm, P3D_ERR_ARG, none);
+      return P3D_OK;
+    }
+    p3d_solver *s = gm.solver;
+    CU(cudaStreamSynchronize(s->st), "member sync"); // its set-up and right-hand side first
+    auto q = std::make_unique<MemberState>();
+    q->m = gm;
+    q->H.assign((size_t)(msize + 1) * msize, 0.0);
+    q->cs.assign(msize, 0.0);
+    q->sn.assign(msize, 0.0);
+    q->gv.assign(msize + 1, 0.0);
+    q->y.assign(msize, 0.0);
+    q->t_join = now_ms();
+    // the scratch slot of the basis pointers names the member's w (norms)
+    double *w = s->w;
+    CU(cudaMemcpyAsync(s->Vptr + s->hs, &w, sizeof(double *), cudaMemcpyHostToDevice, st), "ptr");
+    CU(cudaMemcpyAsync(s->xsol, gm.u, s->nu * 8, cudaMemcpyDeviceToDevice, st), "x u");
+    CU(cudaMemcpyAsync(s->xsol + s->nu, gm.p, s->np * 8, cudaMemcpyDeviceToDevice, st), "x p");
+    act.push_back(std::move(q));
+    dirty = true;
+    return P3D_OK;
+  };
+  // members at positions `idx` of act leave (their x final)
+  auto leave = [&](const std::vector<int> &idx) -> int {
+    std::vector<MemberState *> out;
+    for (int i : idx) out.push_back(act[i].get());
+    const int rc = g_leave(st, out, hooks);
+    std::vector<std::unique_ptr<MemberState>> keep;
+    for (int i = 0; i < (int)act.size(); i++)
+      if (std::find(idx.begin(), idx.end(), i) == idx.end()) keep.push_back(std::move(act[i]));
+    act = std::move(keep);
+    dirty = true;
+    return rc;
+  };
+  int rc = P3D_OK;
+  bool started = false;
+  GroupMember add[P3D_GROUP_MAX];
+  for (;;) {
+    // admissions at the start of a restart cycle
+    if (!started) {
+      for (int k = 0; k < K0 && !rc; k++) {
+        if ((int)act.size() >= max_members) {
+          set_error(P3D_ERR_ARG, "group member: the group is full");
+          if (hooks.leave) hooks.leave(first[k], P3D_ERR_ARG, none);
+          continue;
+        }
+        rc = join(first[k]);
+      }
+      started = true;
+    } else if (hooks.admit && (int)act.size() < max_members) {
+      const int n = hooks.admit(max_members - (int)act.size(), add);
+      for (int k = 0; k < n && !rc; k++) rc = join(add[k]);
+    }
+    if (rc || act.empty()) break;
+    if (dirty && (rc = rebuild())) break;
     // r = b - A x into V_0 of every member, |r|
     double *x[P3D_GROUP_MAX], *w[P3D_GROUP_MAX], *v0[P3D_GROUP_MAX];
     for (int i = 0; i < g.K; i++) { x[i] = g.m[i]->xsol; w[i] = g.m[i]->w; v0[i] = g.m[i]->V; }
@@ -1100,49 +1224,55 @@ static int group_fgmres(Group &all, std::vector<MemberState> &ms)
     VGroup<double> V;
     memset(&V, 0, sizeof V);
     for (int i = 0; i < g.K; i++) { V.v[0][i] = g.m[i]->bvec; V.v[1][i] = w[i]; V.v[2][i] = v0[i]; }
-    vg_residual<double>(V, g.K, N, g.st);
+    vg_residual<double>(V, g.K, N, st);
     double beta[P3D_GROUP_MAX];
     if ((rc = g_norms2(g, 0, v0, beta))) break;
-    std::vector<int> leave;
+    std::vector<int> out;
     for (int i = 0; i < g.K; i++) {
-      MemberState &st = ms[act[i]];
-      if (st.r0 < 0) st.r0 = beta[i];
-      st.rnorm = beta[i];
-      st.tol = std::max(g.m[i]->o.rtol * st.r0, g.m[i]->o.atol);
-      if (!std::isfinite(beta[i])) { st.status = set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual"); leave.push_back(i); }
-      else if (beta[i] <= st.tol) { st.conv = true; leave.push_back(i); }
+      MemberState &q = *act[i];
+      if (q.r0 < 0) q.r0 = beta[i];
+      q.rnorm = beta[i];
+      q.tol = std::max(g.m[i]->o.rtol * q.r0, g.m[i]->o.atol);
+      if (!std::isfinite(beta[i])) {
+        q.status = set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual");
+        out.push_back(i);
+      } else if (beta[i] <= q.tol) {
+        q.conv = true;
+        out.push_back(i);
+      } else if (q.its >= max_it) {
+        out.push_back(i); // iteration limit: not converged
+      } else if (g.m[i]->cancel && g.m[i]->cancel->load(std::memory_order_relaxed)) {
+        q.status = P3D_ERR_CANCELLED;
+        out.push_back(i);
+      }
     }
-    if (!leave.empty()) {
-      std::vector<int> keep;
-      for (int i = 0; i < g.K; i++)
-        if (std::find(leave.begin(), leave.end(), i) == leave.end()) keep.push_back(act[i]);
-      act = keep;
-      if ((rc = rebuild())) break;
-      continue; // recompute the residual pointers for the smaller group
+    if (!out.empty()) {
+      if ((rc = leave(out))) break;
+      continue; // admissions, then the residuals of the new membership
     }
     for (int i = 0; i < g.K; i++) {
       V.v[0][i] = v0[i]; V.v[1][i] = v0[i]; V.s[0][i] = 1.0 / beta[i]; V.s[1][i] = 0.0;
-      MemberState &st = ms[act[i]];
-      std::fill(st.gv.begin(), st.gv.end(), 0.0);
-      st.gv[0] = beta[i];
+      MemberState &q = *act[i];
+      std::fill(q.gv.begin(), q.gv.end(), 0.0);
+      q.gv[0] = beta[i];
     }
-    vg_axpby<double>(V, g.K, N, g.st); // V_0 /= beta
+    vg_axpby<double>(V, g.K, N, st); // V_0 /= beta
     int j = 0;
-    bool cycle_end = false;
-    for (; j < msize && its < max_it && !cycle_end; j++, its++) {
+    for (; j < msize && !act.empty(); j++) {
       // z_j = PC v_j (grouped graph), w = A z_j
       for (int i = 0; i < g.K; i++) {
         V.v[0][i] = g.m[i]->V + (size_t)j * N; V.v[1][i] = g.m[i]->pc_in; V.s[0][i] = 1.0; V.s[1][i] = 0.0;
       }
-      vg_axpby<double>(V, g.K, N, g.st);
-      if ((rc = cuda_check(cudaGraphLaunch(g.gexec, g.st), "grouped pc graph"))) break;
+      vg_axpby<double>(V, g.K, N, st);
+      if ((rc = cuda_check(cudaGraphLaunch(g.gexec, st), "grouped pc graph"))) break;
       count_launch(1);
       double *zj[P3D_GROUP_MAX];
       for (int i = 0; i < g.K; i++) {
         zj[i] = g.m[i]->Z + (size_t)j * N;
         V.v[0][i] = g.m[i]->pc_out; V.v[1][i] = zj[i];
       }
-      vg_axpby<double>(V, g.K, N, g.st);
+      vg_axpby<double>(V, g.K, N, st);
+      for (int i = 0; i < g.K; i++) w[i] = g.m[i]->w;
       if ((rc = g_stokes_op(g, zj, w))) break;
       // classical Gram-Schmidt, first pass with |w|^2; second pass where needed
       MGroup M;
@@ -1151,21 +1281,19 @@ static int group_fgmres(Group &all, std::vector<MemberState> &ms)
         p3d_solver *s = g.m[i];
         M.V[i] = s->Vptr; M.w[i] = w[i]; M.out[i] = s->hdev; M.self_out[i] = s->hdev + j + 1; M.part[i] = s->part;
       }
-      vg_mdot(M, g.K, N, j + 1, g.st);
-      vg_maxpy(M, g.K, N, j + 1, -1.0, g.st);
-      for (int i = 0; i < g.K; i++)
-        if ((rc = cuda_check(cudaMemcpyAsync(g.m[i]->hhost, g.m[i]->hdev, (j + 2) * 8, cudaMemcpyDeviceToHost, g.st), "d2h")))
-          break;
-      if (rc) break;
-      if ((rc = cuda_check(cudaStreamSynchronize(g.st), "sync"))) break;
+      vg_mdot(M, g.K, N, j + 1, st);
+      vg_maxpy(M, g.K, N, j + 1, -1.0, st);
+      for (int i = 0; i < g.K && !rc; i++)
+        rc = cuda_check(cudaMemcpyAsync(g.m[i]->hhost, g.m[i]->hdev, (j + 2) * 8, cudaMemcpyDeviceToHost, st), "d2h");
+      if (rc || (rc = cuda_check(cudaStreamSynchronize(st), "sync"))) break;
       double hn[P3D_GROUP_MAX];
       bool second[P3D_GROUP_MAX];
       int nsecond = 0;
       for (int i = 0; i < g.K; i++) {
-        MemberState &st = ms[act[i]];
+        MemberState &q = *act[i];
         double hh = 0.0;
         for (int c = 0; c <= j; c++) {
-          st.H[(size_t)c * msize + j] = g.m[i]->hhost[c];
+          q.H[(size_t)c * msize + j] = g.m[i]->hhost[c];
           hh += g.m[i]->hhost[c] * g.m[i]->hhost[c];
         }
         const double wb2 = g.m[i]->hhost[j + 1];
@@ -1179,7 +1307,7 @@ static int group_fgmres(Group &all, std::vector<MemberState> &ms)
         int K2 = 0;
         double *w2[P3D_GROUP_MAX];
         Group g2; // the members that need the second pass
-        g2.st = g.st;
+        g2.st = st;
         for (int i = 0; i < g.K; i++)
           if (second[i]) {
             p3d_solver *s = g.m[i];
@@ -1188,171 +1316,124 @@ static int group_fgmres(Group &all, std::vector<MemberState> &ms)
             K2++;
           }
         g2.K = K2;
-        vg_mdot(M2, K2, N, j + 1, g.st);
-        vg_maxpy(M2, K2, N, j + 1, -1.0, g.st);
-        for (int q = 0; q < K2; q++)
-          if ((rc = cuda_check(cudaMemcpyAsync(g2.m[q]->hhost + g2.m[q]->hs, g2.m[q]->hdev + g2.m[q]->hs, (j + 1) * 8,
-                                               cudaMemcpyDeviceToHost, g.st), "d2h")))
-            break;
+        vg_mdot(M2, K2, N, j + 1, st);
+        vg_maxpy(M2, K2, N, j + 1, -1.0, st);
+        for (int q = 0; q < K2 && !rc; q++)
+          rc = cuda_check(cudaMemcpyAsync(g2.m[q]->hhost + g2.m[q]->hs, g2.m[q]->hdev + g2.m[q]->hs, (j + 1) * 8,
+                                          cudaMemcpyDeviceToHost, st), "d2h");
         if (rc) break;
         double n2[P3D_GROUP_MAX];
         if ((rc = g_norms2(g2, g2.m[0]->hs, w2, n2))) break; // synchronizes
         for (int i = 0, q = 0; i < g.K; i++)
           if (second[i]) {
-            MemberState &st = ms[act[i]];
-            for (int c = 0; c <= j; c++) st.H[(size_t)c * msize + j] += g.m[i]->hhost[g.m[i]->hs + c];
+            MemberState &ms = *act[i];
+            for (int c = 0; c <= j; c++) ms.H[(size_t)c * msize + j] += g.m[i]->hhost[g.m[i]->hs + c];
             hn[i] = n2[q++];
           }
       }
       // v_{j+1} = w / hn, Givens rotations, residual estimates
-      std::vector<int> fin; // members whose cycle ends here
+      std::vector<int> fin; // members whose solve ends here
       for (int i = 0; i < g.K; i++) {
-        MemberState &st = ms[act[i]];
-        std::vector<double> &H = st.H;
+        MemberState &q = *act[i];
+        std::vector<double> &H = q.H;
         H[(size_t)(j + 1) * msize + j] = hn[i];
         V.v[0][i] = w[i]; V.v[1][i] = g.m[i]->V + (size_t)(j + 1) * N; V.s[0][i] = hn[i] > 0 ? 1.0 / hn[i] : 0.0;
         V.s[1][i] = 0.0;
         for (int c = 0; c < j; c++) {
           const double a = H[(size_t)c * msize + j], b = H[(size_t)(c + 1) * msize + j];
-          H[(size_t)c * msize + j] = st.cs[c] * a + st.sn[c] * b;
-          H[(size_t)(c + 1) * msize + j] = -st.sn[c] * a + st.cs[c] * b;
+          H[(size_t)c * msize + j] = q.cs[c] * a + q.sn[c] * b;
+          H[(size_t)(c + 1) * msize + j] = -q.sn[c] * a + q.cs[c] * b;
         }
         const double a = H[(size_t)j * msize + j], b = H[(size_t)(j + 1) * msize + j];
         const double rr = std::hypot(a, b);
-        st.cs[j] = rr > 0 ? a / rr : 1.0;
-        st.sn[j] = rr > 0 ? b / rr : 0.0;
+        q.cs[j] = rr > 0 ? a / rr : 1.0;
+        q.sn[j] = rr > 0 ? b / rr : 0.0;
         H[(size_t)j * msize + j] = rr;
         H[(size_t)(j + 1) * msize + j] = 0.0;
-        st.gv[j + 1] = -st.sn[j] * st.gv[j];
-        st.gv[j] = st.cs[j] * st.gv[j];
-        st.rnorm = std::fabs(st.gv[j + 1]);
-        st.its++;
-        if (!std::isfinite(st.rnorm)) {
-          st.status = set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual estimate");
+        q.gv[j + 1] = -q.sn[j] * q.gv[j];
+        q.gv[j] = q.cs[j] * q.gv[j];
+        q.rnorm = std::fabs(q.gv[j + 1]);
+        q.its++;
+        if (!std::isfinite(q.rnorm)) {
+          q.status = set_error(P3D_ERR_BREAKDOWN, "FGMRES: non-finite residual estimate");
           fin.push_back(i);
-        } else if (st.rnorm <= st.tol || hn[i] == 0.0) {
-          st.conv = st.rnorm <= st.tol;
+        } else if (q.rnorm <= q.tol || hn[i] == 0.0) {
+          q.conv = q.rnorm <= q.tol;
+          fin.push_back(i);
+        } else if (q.its >= max_it) {
           fin.push_back(i);
         } else if (g.m[i]->cancel && g.m[i]->cancel->load(std::memory_order_relaxed)) {
-          st.status = P3D_ERR_CANCELLED; // keeps the iterate reached
+          q.status = P3D_ERR_CANCELLED; // keeps the iterate reached
           fin.push_back(i);
         }
       }
-      vg_axpby<double>(V, g.K, N, g.st);
+      vg_axpby<double>(V, g.K, N, st);
       if (!fin.empty()) {
-        // finished members: x += Z y over their j + 1 directions, then they leave
-        // (a member that broke down keeps its iterate)
-        Group gf;
-        gf.st = g.st;
-        std::vector<MemberState> fs;
-        std::vector<int> upd;
-        for (int i : fin) {
-          if (ms[act[i]].status == P3D_OK || ms[act[i]].status == P3D_ERR_CANCELLED) upd.push_back(gf.K);
-          gf.m[gf.K++] = g.m[i];
-          fs.push_back(ms[act[i]]);
-        }
-        if ((rc = g_update_x(gf, upd, fs, j + 1, msize))) break;
-        for (int q = 0; q < (int)fin.size(); q++) {
-          ms[act[fin[q]]] = fs[q];
-          ms[act[fin[q]]].done = true;
-        }
-        std::vector<int> keep;
-        for (int i = 0; i < g.K; i++)
-          if (std::find(fin.begin(), fin.end(), i) == fin.end()) keep.push_back(act[i]);
-        act = keep;
-        if (act.empty()) { j++; its++; break; }
+        // finished members: x += Z y over their j + 1 directions, then they
+        // leave (a member that broke down keeps its iterate)
+        std::vector<MemberState *> upd;
+        for (int i : fin)
+          if (act[i]->status == P3D_OK || act[i]->status == P3D_ERR_CANCELLED) upd.push_back(act[i].get());
+        if ((rc = g_update_x(st, upd, j + 1, msize))) break;
+        if ((rc = leave(fin))) break;
+        if (act.empty()) break;
         if ((rc = rebuild())) break;
-        for (int i = 0; i < g.K; i++) w[i] = g.m[i]->w;
       }
     }
     if (rc) break;
-    if (act.empty()) break; // every member left during the cycle (its update is done)
-    // end of the cycle (restart or iteration limit): x += Z y for the rest
-    std::vector<int> idx;
-    for (int i = 0; i < g.K; i++) idx.push_back(i);
-    std::vector<MemberState> cur;
-    for (int i = 0; i < g.K; i++) cur.push_back(ms[act[i]]);
-    if ((rc = g_update_x(g, idx, cur, j, msize))) break;
-    for (int i = 0; i < g.K; i++) ms[act[i]] = cur[i];
+    if (act.empty()) continue; // every member left during the cycle: admissions
+    // end of the cycle (restart): x += Z y for the rest
+    std::vector<MemberState *> all;
+    for (auto &q : act) all.push_back(q.get());
+    if ((rc = g_update_x(st, all, j, msize))) break;
   }
   g_release_graph(g);
+  if (rc) {
+    // a CUDA failure: the members still in the group leave with it
+    for (auto &q : act)
+      if (hooks.leave) hooks.leave(q->m, rc, none);
+    act.clear();
+  }
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
   return rc;
 }
 
 int solver_group_solve(p3d_solver *const *solvers, int K, double *const *u, double *const *p, p3d_solve_stats *stats,
                        int *status)
 {
-  if (!solvers || !u || !p || K < 1 || K > P3D_GROUP_MAX) return set_error(P3D_ERR_ARG, "group solve: bad arguments");
-  p3d_solver *s0 = solvers[0];
+  if (!solvers || !u || !p || !stats || K < 1 || K > P3D_GROUP_MAX)
+    return set_error(P3D_ERR_ARG, "group solve: bad arguments");
   for (int k = 0; k < K; k++) {
     p3d_solver *s = solvers[k];
     if (!s || !u[k] || !p[k]) return set_error(P3D_ERR_ARG, "group solve: null member %d", k);
-    if (!s->setup_done || !s->rhs_set) return set_error(P3D_ERR_STATE, "group solve: member %d before setup / rhs", k);
-    if (s->device != s0->device || s->mesh.mx != s0->mesh.mx || s->mesh.my != s0->mesh.my || s->mesh.mz != s0->mesh.mz ||
-        s->mesh.dirichlet != s0->mesh.dirichlet || s->o.nlevels != s0->o.nlevels || s->o.cheb_its != s0->o.cheb_its ||
-        s->o.mg_precision != s0->o.mg_precision || s->o.restart != s0->o.restart || s->o.max_it != s0->o.max_it ||
-        s->o.coarse_op != s0->o.coarse_op)
-      return set_error(P3D_ERR_ARG, "group solve: member %d differs in mesh or options", k);
-    if (s->o.inner_its > 0 || s->o.inner_rtol > 0.0 || s->lv.size() < 2)
-      return set_error(P3D_ERR_ARG, "group solve: members need one V-cycle per outer iteration and >= 2 levels");
+    if (const char *why = group_mismatch(solvers[0], s)) return set_error(P3D_ERR_ARG, "group solve: member %d %s", k, why);
     for (int q = 0; q < k; q++)
       if (solvers[q] == s) return set_error(P3D_ERR_ARG, "group solve: solver %d given twice", k);
   }
-  cudaSetDevice(s0->device);
-  const double t0 = now_ms();
-  Group all;
-  all.K = K;
-  all.st = s0->st;
-  for (int k = 0; k < K; k++) all.m[k] = solvers[k];
-  // order the members' own streams before the group's
-  for (int k = 1; k < K; k++) CU(cudaStreamSynchronize(solvers[k]->st), "member sync");
+  GroupMember mem[P3D_GROUP_MAX];
+  int sk[P3D_GROUP_MAX];
   for (int k = 0; k < K; k++) {
-    p3d_solver *s = solvers[k];
-    CU(cudaMemcpyAsync(s->xsol, u[k], s->nu * 8, cudaMemcpyDeviceToDevice, all.st), "x u");
-    CU(cudaMemcpyAsync(s->xsol + s->nu, p[k], s->np * 8, cudaMemcpyDeviceToDevice, all.st), "x p");
+    mem[k].solver = solvers[k];
+    mem[k].u = u[k];
+    mem[k].p = p[k];
+    mem[k].tag = reinterpret_cast<void *>((intptr_t)k);
+    memset(&stats[k], 0, sizeof stats[k]);
+    sk[k] = P3D_ERR_CUDA;
   }
-  std::vector<MemberState> ms(K);
-  int rc = group_fgmres(all, ms);
-  // true residuals and the solutions out
-  if (!rc) {
-    double *x[P3D_GROUP_MAX], *w[P3D_GROUP_MAX];
-    for (int k = 0; k < K; k++) { x[k] = solvers[k]->xsol; w[k] = solvers[k]->w; }
-    rc = g_stokes_op(all, x, w);
-    if (!rc) {
-      VGroup<double> V;
-      memset(&V, 0, sizeof V);
-      for (int k = 0; k < K; k++) { V.v[0][k] = solvers[k]->bvec; V.v[1][k] = w[k]; V.v[2][k] = w[k]; }
-      vg_residual<double>(V, K, s0->N, all.st);
-      double rt[P3D_GROUP_MAX];
-      rc = g_norms2(all, s0->hs, w, rt);
-      for (int k = 0; !rc && k < K; k++) {
-        p3d_solver *s = solvers[k];
-        p3d_solve_stats &st = stats[k];
-        memset(&st, 0, sizeof st);
-        st.iterations = ms[k].its;
-        st.r0 = ms[k].r0;
-        st.rfinal = rt[k];
-        st.converged = ms[k].status == P3D_OK &&
-                       (ms[k].conv || rt[k] <= std::max(s->o.rtol * ms[k].r0, s->o.atol) * 1.0000001);
-        st.setup_ms = s->setup_ms;
-        st.lmax_fine = s->lv.back().lmax;
-        st.coarse_dofs = s->nc;
-        rc = cuda_check(cudaMemcpyAsync(u[k], s->xsol, s->nu * 8, cudaMemcpyDeviceToDevice, all.st), "u out");
-        if (!rc) rc = cuda_check(cudaMemcpyAsync(p[k], s->xsol + s->nu, s->np * 8, cudaMemcpyDeviceToDevice, all.st), "p out");
-      }
-      if (!rc) rc = cuda_check(cudaStreamSynchronize(all.st), "group solve sync");
-    }
-  }
-  const double dt = now_ms() - t0;
-  for (int k = 0; k < K; k++) stats[k].solve_ms = dt;
-  if (rc) return rc;
+  GroupHooks h;
+  h.leave = [&](const GroupMember &m, int s, const p3d_solve_stats &st) {
+    const int k = (int)reinterpret_cast<intptr_t>(m.tag);
+    stats[k] = st;
+    sk[k] = s;
+  };
+  const int rc = solver_group_run(mem, K, K, h);
   int worst = P3D_OK;
   for (int k = 0; k < K; k++) {
-    const int sk = ms[k].status != P3D_OK ? ms[k].status : (stats[k].converged ? P3D_OK : P3D_ERR_NOCONV);
-    if (status) status[k] = sk;
-    if (sk != P3D_OK && (worst == P3D_OK || worst == P3D_ERR_NOCONV)) worst = sk;
+    if (status) status[k] = sk[k];
+    if (sk[k] != P3D_OK && (worst == P3D_OK || worst == P3D_ERR_NOCONV)) worst = sk[k];
   }
-  return worst;
+  return rc ? rc : worst;
 }
 
 } // namespace p3d
@@ -1633,6 +1714,7 @@ int solver_solve_nowait(p3d_solver *s, double *u, double *p, p3d_solve_stats *st
   local.setup_ms = s->setup_ms;
   local.lmax_fine = s->lv.back().lmax;
   local.coarse_dofs = s->nc;
+  local.group_members = 1;
   if (stats) *stats = local;
   if (rc) return rc;
   if (cancelled) return set_error(P3D_ERR_CANCELLED, "solve cancelled after %d iterations", local.iterations);

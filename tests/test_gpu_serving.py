@@ -121,3 +121,39 @@ def test_grouped_requests_match_their_solo_solves(cuda):
         assert abs(r["iterations"] - alone[t]["iterations"]) <= max(2, 0.05 * alone[t]["iterations"])
         assert rel(r["u"], alone[t]["u"]) <= 1e-7
         assert rel(r["p"], alone[t]["p"]) <= 1e-6
+
+
+
+def test_requests_join_a_running_group_and_leave_when_done(cuda):
+    """With one worker, requests of the running request's shape that arrive
+    while it solves join its group at a restart boundary instead of waiting
+    for it; the easy ones leave, with their results posted, while the hard
+    one goes on; every result equals the request solved on its own."""
+    import time
+    hard = request(16, 6, 1e3, 41)
+    easy = [request(16, 1, 10.0, 42 + t) for t in range(3)]
+    kw = dict(rtol=1e-10, max_it=3000)
+    alone = {}
+    with StokesServer(hbm_budget=8 << 30, max_active=1, group_max=1) as S:
+        for t, arr in enumerate([hard] + easy):
+            submit(S, 16, arr, t, **kw)
+            alone[t] = S.wait_all()[0]
+    assert all(r["ok"] for r in alone.values())
+    assert alone[0]["iterations"] > 4 * max(alone[t]["iterations"] for t in (1, 2, 3))
+    with StokesServer(hbm_budget=8 << 30, max_active=1, group_max=8) as S:
+        submit(S, 16, hard, 0, **kw)
+        time.sleep(alone[0]["run_ms"] / 1000 / 5)  # a fifth of the hard solve's own time
+        for t in (1, 2, 3):
+            submit(S, 16, easy[t - 1], t, **kw)
+        done = S.wait_all()
+        st = S.stats()
+    res = {r["tag"]: r for r in done}
+    assert [r["tag"] for r in done][-1] == 0  # the easy ones were posted first
+    assert st["grouped"] >= 3 and st["groups"] == 1, st
+    for t in range(4):
+        r, a = res[t], alone[t]
+        assert r["ok"], (t, r["status"])
+        assert abs(r["iterations"] - a["iterations"]) <= max(2, 0.05 * a["iterations"]), (t, r["iterations"], a["iterations"])
+        assert rel(r["u"], a["u"]) <= 1e-6 and rel(r["p"], a["p"]) <= 1e-5
+    # the easy ones did not wait for the hard one: each took about its own solve time
+    assert max(res[t]["latency_ms"] for t in (1, 2, 3)) < 0.8 * res[0]["latency_ms"]
