@@ -472,7 +472,7 @@ def serving_stream(n, seed=7, rate_per_s=200.0):
     return out, arrivals - arrivals[0]
 
 
-def serve_leg(device, n, max_active=8, group_max=8):
+def serve_leg(device, n, max_active=8, group_max=8, group_elements=16384):
     """Served stream (mixed precision, rtol 1e-6) against the same solves run
     one after another with the plain FP64 solver."""
     import torch
@@ -485,7 +485,8 @@ def serve_leg(device, n, max_active=8, group_max=8):
     reqs, arrivals = serving_stream(n)
     opts = dict(rtol=1e-6, max_it=1000, schur_eta=SCHUR_ETA_GEOMEAN)
     # served: continuous admission, concurrent solves
-    S = StokesServer(device=device, hbm_budget=64 << 30, max_active=max_active, group_max=group_max)
+    S = StokesServer(device=device, hbm_budget=64 << 30, max_active=max_active, group_max=group_max,
+                     group_elements=group_elements)
     for r in reqs[:6]:  # warm the pool shapes (setup of each shape once)
         S.submit((r["m"],) * 3, bits, r["coords"], r["eta"], r["rho"], nlevels=max_levels(r["m"]),
                  mg_precision=PREC_F32, **opts)
@@ -528,7 +529,8 @@ def serve_leg(device, n, max_active=8, group_max=8):
     return {"workload": f"{n} independent Stokes solves, m^3 elements with m uniform in {list(SERVE_SIZES)}, 1-12 "
                         "sinkers r=0.1, eta contrast log-uniform [1e2,1e5], Poisson arrivals 200/s; mixed precision, "
                         "rtol 1e-6, max 1000 FGMRES iterations",
-            "requests": n, "max_active": max_active, "group_max": group_max, "converged": n_ok,
+            "requests": n, "max_active": max_active, "group_max": group_max, "group_elements": group_elements,
+            "converged": n_ok,
             "converged_solves_per_s": n_ok / served_s,
             "p50_latency_ms_converged": float(np.percentile(lat_ok, 50)),
             "p99_latency_ms_converged": float(np.percentile(lat_ok, 99)),
@@ -725,7 +727,8 @@ def run_b200(args):
                 solve["layered_64"] = {"failed": str(exc)}
     serving = None
     if rank == 0 and args.serve_requests > 0:
-        serving = serve_leg(local, args.serve_requests, group_max=args.serve_group_max)
+        serving = serve_leg(local, args.serve_requests, group_max=args.serve_group_max,
+                            group_elements=args.serve_group_elements)
     markers = None
     if rank == 0 and not args.no_markers:
         try:
@@ -911,6 +914,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=256, help="requests of the served-stream leg (0: skip)")
     ap.add_argument("--serve-group-max", type=int, default=8,
                     help="queued same-shape requests the server solves as one group (1: no grouping)")
+    ap.add_argument("--serve-group-elements", type=int, default=16384,
+                    help="largest mesh (elements) the server solves in groups")
     ap.add_argument("--no-markers", action="store_true", help="skip the marker-projection leg")
     ap.add_argument("--slabs", action="store_true", help="run the multi-GPU z-slab path on a single rank")
     ap.add_argument("--size", type=int, default=96, help="elements per direction")

@@ -409,6 +409,11 @@ int p3d_server_create(int device, int64_t hbm_budget_bytes, int32_t max_active, 
  * request on its own.  Requests with an inner velocity solve or one level are
  * always solved alone. */
 int p3d_server_set_group_max(p3d_server *server, int32_t group_max);
+/* Requests whose mesh has more than max_elements elements (default 16384,
+ * i.e. 25^3) are solved alone: grouping pays where the launches of one
+ * solve cannot fill the device (small meshes) and costs the memory of every
+ * member at once.  0 groups nothing. */
+int p3d_server_set_group_elements(p3d_server *server, int64_t max_elements);
 /* Non-blocking.  The request's host arrays must stay valid until its result
  * has been returned by p3d_server_poll. */
 int p3d_server_submit(p3d_server *server, const p3d_request *request);

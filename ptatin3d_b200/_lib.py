@@ -122,6 +122,7 @@ _SIGS = {
     "p3d_op_set_host_register": ([C.c_void_p, C.c_int], C.c_int),
     "p3d_server_cancel": ([C.c_void_p, C.c_int64], C.c_int),
     "p3d_server_set_group_max": ([C.c_void_p, C.c_int32], C.c_int),
+    "p3d_server_set_group_elements": ([C.c_void_p, C.c_int64], C.c_int),
     "p3d_solver_solve_grouped": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                   C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
     "p3d_a11_mult_grouped": ([C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32,

@@ -172,6 +172,7 @@ struct p3d_server {
   int64_t budget = 0;
   int max_active = 1;
   int group_max = 8; // requests of one shape solved together by one worker
+  int64_t group_elements = 16384; // larger meshes are solved alone
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Pending> queue;
@@ -350,11 +351,13 @@ static void worker(p3d_server *S)
     Job *first = take_job(S, jobs, head, slot, fresh);
     const int gmax = std::min(S->group_max, P3D_GROUP_MAX);
     std::vector<Job *> batch{first};
-    if (gmax > 1 && groupable(head.req)) gather(S, head.req, gmax - 1, jobs, batch, evict);
+    const bool group = gmax > 1 && groupable(head.req) &&
+                       (int64_t)head.req.mx * head.req.my * head.req.mz <= S->group_elements;
+    if (group) gather(S, head.req, gmax - 1, jobs, batch, evict);
     S->cv_work.notify_all(); // the next request may fit as well
     lk.unlock();
     release(evict);
-    if (gmax == 1 || !groupable(head.req)) {
+    if (!group) {
       // solved alone
       p3d_solve_stats st;
       memset(&st, 0, sizeof st);
@@ -453,6 +456,14 @@ int p3d_server_set_group_max(p3d_server *S, int32_t group_max)
     return set_error(P3D_ERR_ARG, "server_set_group_max: 1..%d", P3D_GROUP_MAX);
   std::lock_guard<std::mutex> g(S->mu);
   S->group_max = group_max;
+  return P3D_OK;
+}
+
+int p3d_server_set_group_elements(p3d_server *S, int64_t max_elements)
+{
+  if (!S || max_elements < 0) return set_error(P3D_ERR_ARG, "server_set_group_elements: bad arguments");
+  std::lock_guard<std::mutex> g(S->mu);
+  S->group_elements = max_elements;
   return P3D_OK;
 }
 
