@@ -341,12 +341,15 @@ int p3d_solver_solve(p3d_solver *s, double *u_dev, double *p_dev, p3d_solve_stat
  * members, the block preconditioner of all members one captured graph (no
  * counterpart in the reference, which solves one system per process).  Each
  * member keeps its own Krylov basis, step lengths and stopping test; a member
- * that converges or breaks down leaves the group and the others go on.
- * Members need one V-cycle per outer iteration (inner_its = 0, inner_rtol =
- * 0) and at least 2 levels.  u[i], p[i]: device initial guesses in, solutions
- * out; stats[i] per member; status[i] (may be NULL): P3D_OK, P3D_ERR_NOCONV
- * or P3D_ERR_BREAKDOWN per member.  Returns P3D_OK when every member
- * converged, else a member's failure status. */
+ * that converges, breaks down or reaches max_it leaves the group (its u, p
+ * written) and the others go on.  Members need one V-cycle per outer
+ * iteration (inner_its = 0, inner_rtol = 0) and at least 2 levels.  u[i],
+ * p[i]: device initial guesses in, solutions out; stats[i] per member
+ * (solve_ms from the start to the member's own exit; group_members the
+ * largest group it shared launches with); status[i] (may be NULL): P3D_OK,
+ * P3D_ERR_NOCONV, P3D_ERR_BREAKDOWN or P3D_ERR_CANCELLED per member.
+ * Returns P3D_OK when every member converged, else a member's failure
+ * status. */
 int p3d_solver_solve_grouped(p3d_solver *const solvers[], int32_t k, double *const u[], double *const p[],
                              p3d_solve_stats stats[], int32_t status[]);
 /* One application of the block preconditioner (testing / external Krylov). */
