@@ -902,6 +902,50 @@ def profile_solve(spec):
     return 0
 
 
+def profile_group(spec):
+    """K solves of one shape, first one after another and then as one grouped
+    solve (p3d_solver_solve_grouped), for profiling their launches: spec =
+    "m,K,iterations,precision".  Each member is a unit cube with its own 4
+    sinkers of radius 0.1 (viscosity contrast 1e3, density +1 %), free slip
+    walls and base, free surface top, Chebyshev(3)/Jacobi, Galerkin levels
+    down to 2^3 elements or fewer, geometric-mean Schur weighting; every solve
+    stops after `iterations` FGMRES iterations.  Prints the wall times, no
+    JSON (not a benchmark number)."""
+    import torch
+
+    from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
+    from ptatin3d_b200 import mesh as M
+    from ptatin3d_b200.solver import StokesSolver, max_levels, solve_grouped
+    m, K, its, prec = (int(v) for v in spec.split(","))
+    bits = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
+    c = M.uniform_coords(m, m, m)
+    qp = M.qp_coords(c, m, m, m)
+    solvers = []
+    for s in range(K):
+        cen, r = M.random_sinkers(4, s + 1, 0.1)
+        S = StokesSolver(m, m, m, bits, nlevels=max_levels(m), rtol=1e-14, max_it=its,
+                         mg_precision=PREC_F32 if prec == 32 else PREC_F64, schur_eta=SCHUR_ETA_GEOMEAN)
+        S.setup(c, M.sinker_eta(qp, cen, r, 1.0, 1e3))
+        S.set_rhs_body_force(M.sinker_density(qp, cen, r, 1.0, 1.01))
+        solvers.append(S)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for S in solvers:
+        S.solve(raise_on_noconv=False)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res = solve_grouped(solvers)
+    torch.cuda.synchronize()
+    t_grp = time.perf_counter() - t0
+    n_its = sum(r[2]["iterations"] for r in res)
+    print(f"{K} solves of {m}^3, {its} iterations each: one after another {t_seq * 1e3:.1f} ms, grouped "
+          f"{t_grp * 1e3:.1f} ms ({n_its} member iterations, {t_grp / n_its * 1e3:.3f} ms each)")
+    for S in solvers:
+        S.destroy()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -922,9 +966,13 @@ def main():
     ap.add_argument("--workload", default="deformed", choices=["deformed", "layered"])
     ap.add_argument("--profile-solve", default=None, metavar="M,ITS,PREC",
                     help="run one short solve for profiling its launches, print one line, no benchmark")
+    ap.add_argument("--profile-group", default=None, metavar="M,K,ITS,PREC",
+                    help="run K same-shape solves one after another, then grouped, for profiling; no benchmark")
     args = ap.parse_args()
     if args.profile_solve:
         return profile_solve(args.profile_solve)
+    if args.profile_group:
+        return profile_group(args.profile_group)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)
