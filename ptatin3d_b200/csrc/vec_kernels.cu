@@ -18,6 +18,15 @@ static int vgrid(size_t n)
   if (g > cap) g = cap;
   return g < 1 ? 1 : (int)g;
 }
+// blocks of a multi-dot launch (per member): about 8 entries per thread, at
+// most P3D_MDOT_BLOCKS.  Short vectors take few blocks, so that the last
+// block's pass over the partials and the ticket traffic stay small.
+static int mdot_blocks(size_t n)
+{
+  size_t g = (n + 2047) / 2048;
+  if (g > P3D_MDOT_BLOCKS) g = P3D_MDOT_BLOCKS;
+  return g < 1 ? 1 : (int)g;
+}
 
 #define GS_LOOP(i, n) for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (n); i += (size_t)gridDim.x * blockDim.x)
 
@@ -492,7 +501,7 @@ void vg_mdot(const MGroup &G, int K, size_t n, int k, cudaStream_t s)
 {
   for (int j0 = 0; j0 < k; j0 += P3D_MDOT_CHUNK) {
     const int kc = k - j0 < P3D_MDOT_CHUNK ? k - j0 : P3D_MDOT_CHUNK;
-    const dim3 grid(P3D_MDOT_BLOCKS, K);
+    const dim3 grid(mdot_blocks(n), K);
     switch (kc) {
     case 1: kg_mdot_partial<1><<<grid, 256, 0, s>>>(G, n, j0); break;
     case 2: kg_mdot_partial<2><<<grid, 256, 0, s>>>(G, n, j0); break;
@@ -592,7 +601,7 @@ static void mdot_chunk(size_t n, const T *const *V_dev, const T *w, double *part
 {
   // part holds P3D_MDOT_BLOCKS * (P3D_MDOT_CHUNK + 1) partials, then the ticket counter
   unsigned int *ticket = reinterpret_cast<unsigned int *>(part + (size_t)P3D_MDOT_BLOCKS * (P3D_MDOT_CHUNK + 1));
-  k_mdot_partial<T, KC><<<P3D_MDOT_BLOCKS, 256, 0, s>>>(n, V_dev, w, part, ticket, out, self_out);
+  k_mdot_partial<T, KC><<<mdot_blocks(n), 256, 0, s>>>(n, V_dev, w, part, ticket, out, self_out);
   count_launch(1);
 }
 template <typename T>
