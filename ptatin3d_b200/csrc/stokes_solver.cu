@@ -976,18 +976,33 @@ static void g_release_graph(Group &g)
   g.graph = nullptr;
 }
 
-// capture the grouped preconditioner of the current members (after one eager run)
+// capture the grouped preconditioner of the current members.  The first
+// capture of a group follows one eager run (kernel attributes are set outside
+// a capture).  A later capture (the membership changed) has the same
+// sequence of kernels, only with other grids and arguments, so it updates the
+// executable graph in place; a new one is instantiated only if that fails.
 static int g_capture(Group &g)
 {
-  g_release_graph(g);
-  CK(g_apply_pc(g));
-  CU(cudaStreamSynchronize(g.st), "grouped pc warm");
+  if (!g.gexec) {
+    CK(g_apply_pc(g));
+    CU(cudaStreamSynchronize(g.st), "grouped pc warm");
+  }
   CU(cudaStreamBeginCapture(g.st, cudaStreamCaptureModeThreadLocal), "begin capture");
   int rc = g_apply_pc(g);
   cudaGraph_t gr = nullptr;
   cudaError_t e = cudaStreamEndCapture(g.st, &gr);
   if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
   CU(e, "end capture");
+  if (g.gexec) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(g.gexec, gr, &info) == cudaSuccess) {
+      if (g.graph) cudaGraphDestroy(g.graph);
+      g.graph = gr;
+      return P3D_OK;
+    }
+    cudaGetLastError(); // the update was refused: instantiate anew
+    g_release_graph(g);
+  }
   g.graph = gr;
   return cuda_check(cudaGraphInstantiate(&g.gexec, gr, 0), "graph instantiate");
 }
@@ -1144,7 +1159,6 @@ int solver_group_run(const GroupMember *first, int K0, int max_members, GroupHoo
   g.st = st;
   bool dirty = true;
   auto rebuild = [&]() -> int {
-    g_release_graph(g);
     g.K = (int)act.size();
     for (int i = 0; i < g.K; i++) {
       g.m[i] = act[i]->m.solver;
