@@ -306,6 +306,10 @@ static int gather(p3d_server *S, const p3d_request &ref, int room, std::deque<st
   return n;
 }
 
+// how long a request of another shape may wait at the head of the queue
+// before running groups stop taking joiners
+constexpr double JOIN_HOLD_MS = 100.0;
+
 static void worker(p3d_server *S)
 {
   cudaSetDevice(S->device);
@@ -402,7 +406,12 @@ static void worker(p3d_server *S)
       std::vector<Slot *> ev;
       {
         std::lock_guard<std::mutex> g(S->mu);
-        gather(S, head.req, room, jobs, got, ev);
+        // fairness: while a request of another shape has waited at the head
+        // of the queue for longer than JOIN_HOLD_MS, the group takes no
+        // joiners, so that it drains and its worker can take that request
+        const bool held = !S->queue.empty() && !same_group(S->queue.front().req, head.req) &&
+                          wall_ms() - S->queue.front().t_submit > JOIN_HOLD_MS;
+        if (!held) gather(S, head.req, room, jobs, got, ev);
       }
       release(ev);
       return got.empty() ? 0 : ready_members(got, add);

@@ -157,3 +157,33 @@ def test_requests_join_a_running_group_and_leave_when_done(cuda):
         assert rel(r["u"], a["u"]) <= 1e-6 and rel(r["p"], a["p"]) <= 1e-5
     # the easy ones did not wait for the hard one: each took about its own solve time
     assert max(res[t]["latency_ms"] for t in (1, 2, 3)) < 0.8 * res[0]["latency_ms"]
+
+
+def test_running_groups_stop_taking_joiners_while_another_shape_waits(cuda):
+    """Fairness between shapes: with one worker busy on a 24^3 request, a
+    12^3 request waits at the head of the queue.  A second 24^3 request that
+    arrives after that wait has passed 100 ms does not join the running
+    group (which would keep the worker for another whole solve), so the 12^3
+    request is served before it."""
+    import time
+    kw = dict(rtol=1e-14, max_it=1000)  # runs to max_it: a fixed, long solve
+    a1, a2 = request(24, 6, 1e4, 51), request(24, 6, 1e4, 52)
+    b = request(12, 1, 10.0, 53)
+    with StokesServer(hbm_budget=8 << 30, max_active=1, group_max=8) as S:
+        submit(S, 24, a1, 1, **kw)
+        submit(S, 24, a1, 0, **kw)  # same shape: joins 1 at once (the head is of its shape)
+        time.sleep(0.05)
+        submit(S, 12, b, 2, rtol=1e-9)
+        time.sleep(0.2)  # the 12^3 request has now waited 200 ms at the head
+        submit(S, 24, a2, 3, **kw)
+        done = S.wait_all()
+        st = S.stats()
+    order = [r["tag"] for r in done]
+    res = {r["tag"]: r for r in done}
+    assert res[2]["ok"], res[2]["status"]
+    assert res[1]["iterations"] == 1000 and res[3]["iterations"] == 1000
+    # the first group was still running when the second 24^3 request arrived
+    assert min(res[0]["latency_ms"], res[1]["latency_ms"]) > 300, (res[0]["latency_ms"], res[1]["latency_ms"])
+    assert order.index(2) < order.index(3), order
+    assert res[2]["latency_ms"] < res[3]["latency_ms"]
+    assert st["grouped"] == 2 and st["groups"] == 1, st  # 0 and 1 shared launches, 3 did not join
