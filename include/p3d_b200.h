@@ -408,17 +408,21 @@ int p3d_server_create(int device, int64_t hbm_budget_bytes, int32_t max_active, 
  * p3d_solver_solve_grouped: one launch per kernel for all of them).  Queued
  * requests of the group's shape join it at the start of a restart cycle; a
  * member leaves, and its result is posted, as soon as it converges, fails,
- * is cancelled or reaches max_it, while the others go on.  While a request
- * of another shape has waited at the head of the queue for more than 100 ms,
- * running groups take no joiners (they drain and free their workers).  1
- * solves every request on its own.  Requests with an inner velocity solve or
- * one level are always solved alone. */
+ * is cancelled or reaches max_it, while the others go on.  A request joins
+ * a group ahead of queued requests of other shapes only if none of them
+ * arrived more than the overtake bound before it (default 2000 ms,
+ * p3d_server_set_group_overtake_ms), so groups cannot keep a worker from
+ * the other shapes indefinitely.  1 solves every request on its own.
+ * Requests with an inner velocity solve or one level are always solved
+ * alone. */
 int p3d_server_set_group_max(p3d_server *server, int32_t group_max);
 /* Requests whose mesh has more than max_elements elements (default 16384,
  * i.e. 25^3) are solved alone: grouping pays where the launches of one
  * solve cannot fill the device (small meshes) and costs the memory of every
  * member at once.  0 groups nothing. */
 int p3d_server_set_group_elements(p3d_server *server, int64_t max_elements);
+/* The overtake bound of the rolling groups in milliseconds (>= 0). */
+int p3d_server_set_group_overtake_ms(p3d_server *server, int32_t ms);
 /* Non-blocking.  The request's host arrays must stay valid until its result
  * has been returned by p3d_server_poll. */
 int p3d_server_submit(p3d_server *server, const p3d_request *request);

@@ -123,6 +123,7 @@ _SIGS = {
     "p3d_server_cancel": ([C.c_void_p, C.c_int64], C.c_int),
     "p3d_server_set_group_max": ([C.c_void_p, C.c_int32], C.c_int),
     "p3d_server_set_group_elements": ([C.c_void_p, C.c_int64], C.c_int),
+    "p3d_server_set_group_overtake_ms": ([C.c_void_p, C.c_int32], C.c_int),
     "p3d_solver_solve_grouped": ([C.POINTER(C.c_void_p), C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                   C.c_void_p, C.POINTER(C.c_int32)], C.c_int),
     "p3d_a11_mult_grouped": ([C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int32,

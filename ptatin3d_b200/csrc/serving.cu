@@ -173,6 +173,7 @@ struct p3d_server {
   int max_active = 1;
   int group_max = 8; // requests of one shape solved together by one worker
   int64_t group_elements = 16384; // larger meshes are solved alone
+  double overtake_ms = 2000.0;     // see gather()
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Pending> queue;
@@ -291,11 +292,16 @@ static int gather(p3d_server *S, const p3d_request &ref, int room, std::deque<st
                   std::vector<Job *> &got, std::vector<Slot *> &evict)
 {
   int n = 0;
+  double t_other = -1.0; // arrival of the oldest queued request of another shape
   for (auto it = S->queue.begin(); it != S->queue.end() && n < room;) {
     if (!same_group(it->req, ref)) {
+      if (t_other < 0) t_other = it->t_submit;
       ++it;
       continue;
     }
+    // fairness: no request overtakes one of another shape that arrived more
+    // than overtake_ms before it (the queue is in arrival order)
+    if (t_other >= 0 && it->t_submit - t_other > S->overtake_ms) break;
     bool f = false, big = false;
     Slot *sl = admit_request(S, it->req, evict, f, big);
     if (!sl) break; // no slot or memory for more now
@@ -305,10 +311,6 @@ static int gather(p3d_server *S, const p3d_request &ref, int room, std::deque<st
   }
   return n;
 }
-
-// how long a request of another shape may wait at the head of the queue
-// before running groups stop taking joiners
-constexpr double JOIN_HOLD_MS = 100.0;
 
 static void worker(p3d_server *S)
 {
@@ -406,12 +408,7 @@ static void worker(p3d_server *S)
       std::vector<Slot *> ev;
       {
         std::lock_guard<std::mutex> g(S->mu);
-        // fairness: while a request of another shape has waited at the head
-        // of the queue for longer than JOIN_HOLD_MS, the group takes no
-        // joiners, so that it drains and its worker can take that request
-        const bool held = !S->queue.empty() && !same_group(S->queue.front().req, head.req) &&
-                          wall_ms() - S->queue.front().t_submit > JOIN_HOLD_MS;
-        if (!held) gather(S, head.req, room, jobs, got, ev);
+        gather(S, head.req, room, jobs, got, ev);
       }
       release(ev);
       return got.empty() ? 0 : ready_members(got, add);
@@ -465,6 +462,14 @@ int p3d_server_set_group_max(p3d_server *S, int32_t group_max)
     return set_error(P3D_ERR_ARG, "server_set_group_max: 1..%d", P3D_GROUP_MAX);
   std::lock_guard<std::mutex> g(S->mu);
   S->group_max = group_max;
+  return P3D_OK;
+}
+
+int p3d_server_set_group_overtake_ms(p3d_server *S, int32_t ms)
+{
+  if (!S || ms < 0) return set_error(P3D_ERR_ARG, "server_set_group_overtake_ms: bad arguments");
+  std::lock_guard<std::mutex> g(S->mu);
+  S->overtake_ms = ms;
   return P3D_OK;
 }
 

@@ -20,17 +20,20 @@ from .solver import default_opts
 
 class StokesServer:
     def __init__(self, device: int = 0, hbm_budget: int = 16 << 30, max_active: int = 4, group_max: int = 8,
-                 group_elements: int = 16384):
+                 group_elements: int = 16384, group_overtake_ms: int = 2000):
         """group_max: requests of one shape solved together in a rolling
         group (shared launches; later arrivals join at restart boundaries,
         members leave when done); 1 solves every request on its own.
-        group_elements: meshes with more elements are solved alone."""
+        group_elements: meshes with more elements are solved alone.
+        group_overtake_ms: a request is grouped ahead of queued requests of
+        other shapes only if none of them arrived that much earlier."""
         import torch  # noqa: F401  (the server shares the process's CUDA context)
         h = C.c_void_p()
         check(lib().p3d_server_create(int(device), int(hbm_budget), int(max_active), C.byref(h)))
         self.h = h
         check(lib().p3d_server_set_group_max(h, int(group_max)))
         check(lib().p3d_server_set_group_elements(h, int(group_elements)))
+        check(lib().p3d_server_set_group_overtake_ms(h, int(group_overtake_ms)))
         self._live = {}
         self._tags = itertools.count()
 

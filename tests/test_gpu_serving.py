@@ -159,22 +159,22 @@ def test_requests_join_a_running_group_and_leave_when_done(cuda):
     assert max(res[t]["latency_ms"] for t in (1, 2, 3)) < 0.8 * res[0]["latency_ms"]
 
 
-def test_running_groups_stop_taking_joiners_while_another_shape_waits(cuda):
-    """Fairness between shapes: with one worker busy on a 24^3 request, a
-    12^3 request waits at the head of the queue.  A second 24^3 request that
-    arrives after that wait has passed 100 ms does not join the running
-    group (which would keep the worker for another whole solve), so the 12^3
-    request is served before it."""
+def test_groups_do_not_overtake_long_waiting_requests_of_other_shapes(cuda):
+    """Fairness between shapes: with one worker busy on a group of 24^3
+    requests, a 12^3 request waits in the queue.  A later 24^3 request that
+    arrives more than the overtake bound (100 ms here) after it does not join
+    the running group (which would keep the worker for another whole solve),
+    so the 12^3 request is served before it."""
     import time
     kw = dict(rtol=1e-14, max_it=1000)  # runs to max_it: a fixed, long solve
     a1, a2 = request(24, 6, 1e4, 51), request(24, 6, 1e4, 52)
     b = request(12, 1, 10.0, 53)
-    with StokesServer(hbm_budget=8 << 30, max_active=1, group_max=8) as S:
+    with StokesServer(hbm_budget=8 << 30, max_active=1, group_max=8, group_overtake_ms=100) as S:
         submit(S, 24, a1, 1, **kw)
         submit(S, 24, a1, 0, **kw)  # same shape: joins 1 at once (the head is of its shape)
         time.sleep(0.05)
         submit(S, 12, b, 2, rtol=1e-9)
-        time.sleep(0.2)  # the 12^3 request has now waited 200 ms at the head
+        time.sleep(0.2)  # 200 ms after the 12^3 request
         submit(S, 24, a2, 3, **kw)
         done = S.wait_all()
         st = S.stats()
