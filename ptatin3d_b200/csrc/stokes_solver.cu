@@ -1145,15 +1145,33 @@ static int g_leave(cudaStream_t st, const std::vector<MemberState *> &out, Group
 
 int solver_group_run(const GroupMember *first, int K0, int max_members, GroupHooks &hooks)
 {
-  if (!first || K0 < 1 || K0 > P3D_GROUP_MAX || !first[0].solver)
-    return set_error(P3D_ERR_ARG, "group run: bad arguments");
+  if (!first || K0 < 1 || K0 > P3D_GROUP_MAX) return set_error(P3D_ERR_ARG, "group run: bad arguments");
   max_members = std::max(1, std::min(max_members, P3D_GROUP_MAX));
-  const p3d_solver *ref = first[0].solver;
+  const p3d_solver *ref = nullptr; // the shape and options every member must share
+  for (int k = 0; k < K0 && !ref; k++) ref = first[k].solver;
+  if (!ref) {
+    p3d_solve_stats z;
+    memset(&z, 0, sizeof z);
+    const int rc0 = set_error(P3D_ERR_ARG, "group run: no solver given");
+    for (int k = 0; k < K0; k++)
+      if (hooks.leave) hooks.leave(first[k], rc0, z);
+    return rc0;
+  }
   const int msize = ref->o.restart, max_it = ref->o.max_it;
   const size_t N = ref->N;
   cudaSetDevice(ref->device);
+  p3d_solve_stats none;
+  memset(&none, 0, sizeof none);
+  // every member handed to the run leaves exactly once, failures included
+  auto leave_all = [&](const GroupMember *m, int n, int status) {
+    for (int k = 0; k < n; k++)
+      if (hooks.leave) hooks.leave(m[k], status, none);
+  };
   cudaStream_t st = nullptr;
-  CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "group stream");
+  if (int rc0 = cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "group stream")) {
+    leave_all(first, K0, rc0);
+    return rc0;
+  }
   std::vector<std::unique_ptr<MemberState>> act; // members in the group's order
   Group g;
   g.st = st;
@@ -1167,8 +1185,6 @@ int solver_group_run(const GroupMember *first, int K0, int max_members, GroupHoo
     dirty = false;
     return g.K ? g_capture(g) : P3D_OK;
   };
-  p3d_solve_stats none;
-  memset(&none, 0, sizeof none);
   auto join = [&](const GroupMember &gm) -> int {
     const char *why = gm.solver && gm.u && gm.p ? group_mismatch(ref, gm.solver) : "null member";
     if (!why)
@@ -1180,7 +1196,6 @@ int solver_group_run(const GroupMember *first, int K0, int max_members, GroupHoo
       return P3D_OK;
     }
     p3d_solver *s = gm.solver;
-    CU(cudaStreamSynchronize(s->st), "member sync"); // its set-up and right-hand side first
     auto q = std::make_unique<MemberState>();
     q->m = gm;
     q->H.assign((size_t)(msize + 1) * msize, 0.0);
@@ -1189,11 +1204,17 @@ int solver_group_run(const GroupMember *first, int K0, int max_members, GroupHoo
     q->gv.assign(msize + 1, 0.0);
     q->y.assign(msize, 0.0);
     q->t_join = now_ms();
-    // the scratch slot of the basis pointers names the member's w (norms)
+    // its set-up and right-hand side first; the scratch slot of the basis
+    // pointers names the member's w (norms)
     double *w = s->w;
-    CU(cudaMemcpyAsync(s->Vptr + s->hs, &w, sizeof(double *), cudaMemcpyHostToDevice, st), "ptr");
-    CU(cudaMemcpyAsync(s->xsol, gm.u, s->nu * 8, cudaMemcpyDeviceToDevice, st), "x u");
-    CU(cudaMemcpyAsync(s->xsol + s->nu, gm.p, s->np * 8, cudaMemcpyDeviceToDevice, st), "x p");
+    int rc = cuda_check(cudaStreamSynchronize(s->st), "member sync");
+    if (!rc) rc = cuda_check(cudaMemcpyAsync(s->Vptr + s->hs, &w, sizeof(double *), cudaMemcpyHostToDevice, st), "ptr");
+    if (!rc) rc = cuda_check(cudaMemcpyAsync(s->xsol, gm.u, s->nu * 8, cudaMemcpyDeviceToDevice, st), "x u");
+    if (!rc) rc = cuda_check(cudaMemcpyAsync(s->xsol + s->nu, gm.p, s->np * 8, cudaMemcpyDeviceToDevice, st), "x p");
+    if (rc) {
+      if (hooks.leave) hooks.leave(gm, rc, none);
+      return rc;
+    }
     act.push_back(std::move(q));
     dirty = true;
     return P3D_OK;
@@ -1203,6 +1224,7 @@ int solver_group_run(const GroupMember *first, int K0, int max_members, GroupHoo
     std::vector<MemberState *> out;
     for (int i : idx) out.push_back(act[i].get());
     const int rc = g_leave(st, out, hooks);
+    if (rc) return rc; // none of them has left: the failure path below lets them go
     std::vector<std::unique_ptr<MemberState>> keep;
     for (int i = 0; i < (int)act.size(); i++)
       if (std::find(idx.begin(), idx.end(), i) == idx.end()) keep.push_back(std::move(act[i]));
@@ -1216,18 +1238,23 @@ int solver_group_run(const GroupMember *first, int K0, int max_members, GroupHoo
   for (;;) {
     // admissions at the start of a restart cycle
     if (!started) {
-      for (int k = 0; k < K0 && !rc; k++) {
-        if ((int)act.size() >= max_members) {
+      for (int k = 0; k < K0; k++) {
+        if (rc) {
+          leave_all(first + k, 1, rc);
+        } else if ((int)act.size() >= max_members) {
           set_error(P3D_ERR_ARG, "group member: the group is full");
-          if (hooks.leave) hooks.leave(first[k], P3D_ERR_ARG, none);
-          continue;
+          leave_all(first + k, 1, P3D_ERR_ARG);
+        } else {
+          rc = join(first[k]);
         }
-        rc = join(first[k]);
       }
       started = true;
     } else if (hooks.admit && (int)act.size() < max_members) {
       const int n = hooks.admit(max_members - (int)act.size(), add);
-      for (int k = 0; k < n && !rc; k++) rc = join(add[k]);
+      for (int k = 0; k < n; k++) {
+        if (rc) leave_all(add + k, 1, rc);
+        else rc = join(add[k]);
+      }
     }
     if (rc || act.empty()) break;
     if (dirty && (rc = rebuild())) break;
