@@ -1,4 +1,4 @@
-"""Slab-partitioned CPU MatMult of the reference kernel (CPU BASELINE ONLY; the
+"""Slab-partitioned CPU MatMult of the reference kernel (CPU baseline only; the
 product never imports it).
 
 P processes, one per host core, each apply the reference's own
