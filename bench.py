@@ -729,6 +729,12 @@ def run_b200(args):
     if rank == 0 and args.serve_requests > 0:
         serving = serve_leg(local, args.serve_requests, group_max=args.serve_group_max,
                             group_elements=args.serve_group_elements)
+    grouped = None
+    if rank == 0 and args.serve_requests > 0:
+        try:
+            grouped = grouped_leg(local)
+        except Exception as exc:  # reported, not required
+            grouped = {"failed": str(exc)}
     markers = None
     if rank == 0 and not args.no_markers:
         try:
@@ -763,6 +769,7 @@ def run_b200(args):
                              "TFLOP/s": REF_FLOPS_PER_EL * m ** 3 / (kern_ms * 1e-3) / 1e12},
                 "solve": solve,
                 "serving": serving,
+                "grouped_solves": grouped,
                 "markers": markers}
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -902,28 +909,26 @@ def profile_solve(spec):
     return 0
 
 
-def profile_group(spec):
+def grouped_solves(m, K, its, prec, device=0):
     """K solves of one shape, first one after another and then as one grouped
-    solve (p3d_solver_solve_grouped), for profiling their launches: spec =
-    "m,K,iterations,precision".  Each member is a unit cube with its own 4
-    sinkers of radius 0.1 (viscosity contrast 1e3, density +1 %), free slip
+    solve (p3d_solver_solve_grouped).  Each member is a unit cube with its own
+    4 sinkers of radius 0.1 (viscosity contrast 1e3, density +1 %), free slip
     walls and base, free surface top, Chebyshev(3)/Jacobi, Galerkin levels
     down to 2^3 elements or fewer, geometric-mean Schur weighting; every solve
-    stops after `iterations` FGMRES iterations.  Prints the wall times, no
-    JSON (not a benchmark number)."""
+    stops after `its` FGMRES iterations.  Returns (one-after-another ms,
+    grouped ms, member iterations)."""
     import torch
 
     from ptatin3d_b200 import PREC_F32, PREC_F64, SCHUR_ETA_GEOMEAN
     from ptatin3d_b200 import mesh as M
     from ptatin3d_b200.solver import StokesSolver, max_levels, solve_grouped
-    m, K, its, prec = (int(v) for v in spec.split(","))
     bits = M.FREE_SLIP & ~M.bc_bit(M.FACE_KMAX, 2)
     c = M.uniform_coords(m, m, m)
     qp = M.qp_coords(c, m, m, m)
     solvers = []
     for s in range(K):
         cen, r = M.random_sinkers(4, s + 1, 0.1)
-        S = StokesSolver(m, m, m, bits, nlevels=max_levels(m), rtol=1e-14, max_it=its,
+        S = StokesSolver(m, m, m, bits, device=device, nlevels=max_levels(m), rtol=1e-14, max_it=its,
                          mg_precision=PREC_F32 if prec == 32 else PREC_F64, schur_eta=SCHUR_ETA_GEOMEAN)
         S.setup(c, M.sinker_eta(qp, cen, r, 1.0, 1e3))
         S.set_rhs_body_force(M.sinker_density(qp, cen, r, 1.0, 1.01))
@@ -939,11 +944,32 @@ def profile_group(spec):
     torch.cuda.synchronize()
     t_grp = time.perf_counter() - t0
     n_its = sum(r[2]["iterations"] for r in res)
-    print(f"{K} solves of {m}^3, {its} iterations each: one after another {t_seq * 1e3:.1f} ms, grouped "
-          f"{t_grp * 1e3:.1f} ms ({n_its} member iterations, {t_grp / n_its * 1e3:.3f} ms each)")
     for S in solvers:
         S.destroy()
+    return t_seq * 1e3, t_grp * 1e3, n_its
+
+
+def profile_group(spec):
+    """grouped_solves for profiling their launches: spec = "m,K,iterations,
+    precision".  Prints the wall times, no JSON (not a benchmark number)."""
+    m, K, its, prec = (int(v) for v in spec.split(","))
+    t_seq, t_grp, n_its = grouped_solves(m, K, its, prec)
+    print(f"{K} solves of {m}^3, {its} iterations each: one after another {t_seq:.1f} ms, grouped "
+          f"{t_grp:.1f} ms ({n_its} member iterations, {t_grp / n_its:.3f} ms each)")
     return 0
+
+
+def grouped_leg(device):
+    """Shared launches: 8 same-shape small solves (mixed precision, 30 FGMRES
+    iterations each) one after another and as one grouped solve."""
+    out = {"workload": "8 same-shape Stokes solves (unit cube, 4 sinkers each, contrast 1e3), mixed precision, "
+                       "30 FGMRES iterations each: one after another vs p3d_solver_solve_grouped"}
+    for m in (8, 16):
+        grouped_solves(m, 8, 3, 32, device)  # warm-up (graphs, pools)
+        t_seq, t_grp, n_its = grouped_solves(m, 8, 30, 32, device)
+        out[f"m{m}"] = {"one_after_another_ms": t_seq, "grouped_ms": t_grp, "member_iterations": n_its,
+                        "speedup": t_seq / t_grp}
+    return out
 
 
 def main():
